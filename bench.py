@@ -1,0 +1,419 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 sparse hot path (one JSON line on rank 0).
+
+Headline: FP64 CSR SpMV (segmented-sum form) throughput in GB/s on the
+irregular-row workload -- 4,000,000 rows, power-law row lengths (exponent
+2.1, clipped to [1, 20000]), uniform sorted columns, N(0,1) values,
+x ~ U[-1,1] seed 0 -- with algorithmic bytes per SpMV
+  nnz*(8 + 4) + (n+1)*4 + n*8 (x) + n*8 (y).
+A step is one SpMV over the whole matrix.  The matrix (~0.4 GB) is larger
+than L2, so no L2 flush is done between steps; x (32 MB) may stay in L2.
+
+Also reported (N == 1 only): the same SpMV on the 2D/3D Laplacians, the
+IC(0)-PCG time to a 1e-10 true residual on the RCM-ordered 128^3 3D
+Laplacian in FP64 vs mixed precision, the reference's OpenMP CPU path timed
+on this host, and clocks sampled during the timed region.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+For N > 1 (torchrun, one rank per GPU) every rank runs its own replica of
+the workload (the solve path does not shard; weak scaling) and the time is
+the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "SpMV GB/s vs ~8 TB/s HBM; IC(0)-PCG time to 1e-10 resid, mixed vs FP64"
+WORKLOAD = "powerlaw_spmv_fp64_segsum"
+
+
+def spmv_bytes(n, nnz, vbytes=8, xbytes=8, beta=False):
+    return nnz * (vbytes + 4) + (n + 1) * 4 + n * xbytes + n * xbytes * (2 if beta else 1)
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel_key):
+    """Per-launch DRAM bytes recorded from an ncu capture, if committed."""
+    f = ROOT / "profiles" / "traffic.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == kernel_key:
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML in a thread."""
+
+    def __init__(self, index=0, period=0.002):
+        self.period, self.samples, self.reasons = period, [], set()
+        self.ok = False
+        try:
+            import pynvml as N
+            N.nvmlInit()
+            self.N = N
+            self.h = N.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = N.nvmlDeviceGetMaxClockInfo(self.h, N.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:
+            self.max_mhz = None
+        self._stop = threading.Event()
+
+    def _run(self):
+        N = self.N
+        names = {
+            "gpu_idle": N.nvmlClocksEventReasonGpuIdle,
+            "sw_power_cap": N.nvmlClocksEventReasonSwPowerCap,
+            "hw_slowdown": N.nvmlClocksEventReasonHwSlowdown,
+            "hw_thermal_slowdown": N.nvmlClocksEventReasonHwThermalSlowdown,
+            "sw_thermal_slowdown": N.nvmlClocksEventReasonSwThermalSlowdown,
+            "hw_power_brake": N.nvmlClocksEventReasonHwPowerBrakeSlowdown,
+        }
+        while not self._stop.is_set():
+            try:
+                self.samples.append(N.nvmlDeviceGetClockInfo(self.h, N.NVML_CLOCK_SM))
+                r = N.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for k, v in names.items():
+                    if r & v:
+                        self.reasons.add(k)
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def __enter__(self):
+        if self.ok:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self.ok:
+            self._stop.set()
+            self.t.join()
+
+    def summary(self):
+        if not self.ok or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unavailable"]}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons - {"gpu_idle"}), "samples": len(self.samples)}
+
+
+def powerlaw_workload():
+    from linearalgebra_b200 import gen
+    n, ai, aj, av = gen.powerlaw(4_000_000, seed=0)
+    x = gen.uniform_vector(n, 0)
+    return n, ai, aj, av, x
+
+
+def cpu_reference_spmv(n, ai, aj, av, x, budget_s=10.0, max_reps=100):
+    """The reference's own SegSumSPMV (compiled in place, oracle/_ref) with
+    all host threads: median seconds per SpMV over a bounded sample."""
+    import oracle
+    rf = oracle.ref()
+    kind = "reference"
+    if rf is None:
+        raise RuntimeError("oracle/_ref/libla_ref.so is missing (build() compiles it)")
+    P = oracle.ptr
+    T = rf.la_ref_max_threads()
+    h = rf.la_ref_segsum_create(T, n, 0, P(ai), P(aj), P(av))
+    y = np.zeros(n)
+    rf.la_ref_segsum_apply(h, n, 0, P(ai), P(aj), P(av), P(x), P(y), 1.0, 0.0)  # warm
+    times = []
+    t_end = time.perf_counter() + budget_s
+    while len(times) < max_reps and (time.perf_counter() < t_end or len(times) < 3):
+        t0 = time.perf_counter()
+        rf.la_ref_segsum_apply(h, n, 0, P(ai), P(aj), P(av), P(x), P(y), 1.0, 0.0)
+        times.append(time.perf_counter() - t0)
+    rf.la_ref_segsum_destroy(h)
+    return statistics.median(times), T, len(times), kind
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's OpenMP SegSumSPMV on the host."""
+    if rank != 0:
+        return
+    n, ai, aj, av, x = powerlaw_workload()
+    nnz = int(ai[-1])
+    byt = spmv_bytes(n, nnz)
+    import oracle
+    rf = oracle.ref()
+    P = oracle.ptr
+    T = rf.la_ref_max_threads()
+    h = rf.la_ref_segsum_create(T, n, 0, P(ai), P(aj), P(av))
+    y = np.zeros(n)
+    for _ in range(args.warmup):
+        rf.la_ref_segsum_apply(h, n, 0, P(ai), P(aj), P(av), P(x), P(y), 1.0, 0.0)
+    steps = args.steps if args.steps_given else 30
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        rf.la_ref_segsum_apply(h, n, 0, P(ai), P(aj), P(av), P(x), P(y), 1.0, 0.0)
+    dt = time.perf_counter() - t0
+    rf.la_ref_segsum_destroy(h)
+    v = steps * byt / dt / 1e9
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "GB/s",
+        "n_gpus": world, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": dt / steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "rows": n, "nnz": nnz, "bytes_per_step": byt,
+                   "l2": "matrix larger than L2; no flush", "parallelism": "host OpenMP"},
+        "cpu_baseline": {"value": v, "unit": "GB/s", "cores": T, "kind": "reference",
+                         "sample": f"{steps} full SegSumSPMV calls on the same matrix"},
+        "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def time_device_spmv(la, torch, plan, xd, yd, steps, warmup, alpha=1.0, beta=0.0):
+    for _ in range(warmup):
+        plan(xd, yd, alpha, beta)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        plan(xd, yd, alpha, beta)
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3
+
+
+def extras(la, torch, peak):
+    """Single-GPU extras: Laplacian SpMV rooflines and the PCG comparison."""
+    from linearalgebra_b200 import gen
+    out = {"spmv": [], "pcg": None}
+    for label, t in (("C1_lap2d_512", gen.laplacian_2d(512)), ("C3_lap3d_128", gen.laplacian_3d(128))):
+        n, ai, aj, av = t
+        nnz = int(ai[-1])
+        A = la.CSR(n, n, 0, ai, aj, av, keep_f32=True)
+        x = gen.uniform_vector(n, 0)
+        for kind, kid in (("segsum", la.api.LA_SPMV_SEGSUM), ("albus", la.api.LA_SPMV_ALBUS)):
+            plan = la.SPMV(A, kid)
+            for dt, tdt, vb in (("f64", torch.float64, 8), ("f32", torch.float32, 4)):
+                xd = torch.as_tensor(x).to("cuda", tdt)
+                yd = torch.empty(n, dtype=tdt, device="cuda")
+                # flush L2 between reps for the L2-resident 2D case
+                flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+                times = []
+                for _ in range(30):
+                    flush.fill_(1)
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record()
+                    plan(xd, yd)
+                    e1.record()
+                    torch.cuda.synchronize()
+                    times.append(e0.elapsed_time(e1) / 1e3)
+                t = statistics.median(times[5:])
+                b = spmv_bytes(n, nnz, vb, vb)
+                out["spmv"].append({"config": label, "form": kind, "dtype": dt, "n": n, "nnz": nnz,
+                                    "bytes": b, "us": t * 1e6, "GB/s": b / t / 1e9,
+                                    "frac_of_measured_hbm": b / t / 1e9 / peak,
+                                    "frac_of_8TBs": b / t / 8e12, "l2": "flushed"})
+                del flush
+    # IC(0)-PCG on the RCM-ordered 128^3 Laplacian, FP64 vs mixed
+    n, ai, aj, av = gen.laplacian_3d(128)
+    t0 = time.perf_counter()
+    iperm, perm = la.SerialCM(n, 0, ai, aj)
+    b_ai, b_aj, b_av = la.Permute(n, 0, ai, aj, av, iperm, perm)
+    ua, uj, uv = gen.upper_with_diag(n, b_ai, b_aj, b_av)
+    f = la.ICCLevelNumeric0(n, 0, ua, uj, uv)
+    A = la.CSR(n, n, 0, b_ai, b_aj, b_av, keep_f32=True)
+    s64 = la.PCG(A, ua, uj, f)
+    s32 = la.PCG(A, ua, uj, f, mixed=True)
+    setup_s = time.perf_counter() - t0
+    bvec = gen.uniform_vector(n, 0)
+    bd = torch.as_tensor(bvec).to("cuda")
+    x64 = torch.empty(n, dtype=torch.float64, device="cuda")
+    x32 = torch.empty(n, dtype=torch.float64, device="cuda")
+    s64.solve(bd, x64)  # warm-up
+    s32.solve(bd, x32)
+    r64 = s64.solve(bd, x64)
+    r32 = s32.solve(bd, x32)
+    err = float(torch.linalg.norm(x32 - x64) / torch.linalg.norm(x64))
+    out["pcg"] = {"config": "C3_lap3d_128_rcm", "n": n, "nnz": int(ai[-1]), "rtol": 1e-10,
+                  "levels": 382, "setup_s_host": setup_s,
+                  "fp64": {"iterations": r64.iterations, "ms": r64.solve_ms,
+                           "rel_residual": r64.rel_residual},
+                  "mixed": {"inner_iterations": r32.iterations, "outer": r32.outer_iterations,
+                            "ms": r32.solve_ms, "rel_residual": r32.rel_residual,
+                            "rel_err_vs_fp64": err},
+                  "speedup_mixed_vs_fp64": r64.solve_ms / r32.solve_ms}
+    return out, (b_ai, b_aj, b_av, ua, uj, f, bvec, r64)
+
+
+def cpu_pcg(mats):
+    import oracle
+    rf = oracle.ref()
+    b_ai, b_aj, b_av, ua, uj, f, bvec, _ = mats
+    n = len(b_ai) - 1
+    P = oracle.ptr
+    T = rf.la_ref_max_threads()
+    h = rf.la_ref_pcg_create(T, n, 0, P(b_ai), P(b_aj), P(b_av), P(ua), P(uj), P(f))
+    x = np.zeros(n)
+    rel = np.zeros(1)
+    t0 = time.perf_counter()
+    it = rf.la_ref_pcg_solve(h, P(bvec), P(x), 1e-10, 5000, P(rel))
+    dt = time.perf_counter() - t0
+    rf.la_ref_pcg_destroy(h)
+    return {"kind": "reference kernels (ParallelSPMV + OptimizedTriangularSolve<Barrier>) "
+                    "composed into PCG; MKL PCG driver absent",
+            "cores": T, "iterations": it, "s": dt, "rel_residual": float(rel[0])}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--no-cpu-pcg", action="store_true")
+    args = ap.parse_args()
+    args.steps_given = args.steps is not None
+    if args.steps is None:
+        args.steps = 1000
+    args.warmup = max(args.warmup, 3)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    import linearalgebra_b200 as la
+
+    peak, peak_kind = measured_peak()
+    n, ai, aj, av, x = powerlaw_workload()
+    nnz = int(ai[-1])
+    byt = spmv_bytes(n, nnz)
+    A = la.CSR(n, n, 0, ai, aj, av)
+    plan = la.SPMV(A, la.api.LA_SPMV_SEGSUM)
+    xd = torch.as_tensor(x).to("cuda")
+    yd = torch.empty(n, dtype=torch.float64, device="cuda")
+    for _ in range(args.warmup):
+        plan(xd, yd)
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with sampler:
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(args.steps):
+            plan(xd, yd)
+        e1.record()
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+    t = e0.elapsed_time(e1) / 1e3
+    if pg:
+        tt = torch.tensor([t], device="cuda")
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        t = float(tt.item())
+    value = world * args.steps * byt / t / 1e9
+    launch_s = t / args.steps
+
+    # end to end through the reference-facing host-pointer call: pinned host
+    # x in, y out, every step
+    hx = torch.as_tensor(x).pin_memory()
+    hy = torch.empty(n, dtype=torch.float64).pin_memory()
+    hxn, hyn = hx.numpy(), hy.numpy()
+    e2e_steps = max(10, min(args.steps, 200))
+    for _ in range(3):
+        plan(hxn, hyn)
+    if pg:
+        pg.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        plan(hxn, hyn)
+    te = time.perf_counter() - t0
+    if pg:
+        tt = torch.tensor([te], device="cuda")
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        te = float(tt.item())
+    e2e = world * e2e_steps * byt / te / 1e9
+    ok = np.allclose(hyn, yd.cpu().numpy(), rtol=1e-12, atol=1e-12)
+
+    result = {
+        "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator standing in for the reference's "
+                "downloaded matrices)",
+        "config": {"workload": WORKLOAD, "rows": n, "nnz": nnz, "bytes_per_step": byt,
+                   "row_lengths": "ceil(Pareto(2.1)) clipped to [1, 20000]",
+                   "l2": "inputs larger than L2 (matrix %.2f GB); no flush" % (byt / 1e9),
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "roofline": {"bound": "hbm", "achieved": byt / launch_s / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": byt / launch_s / 1e9 / peak,
+                     "peak_kind": peak_kind, "kernel": "spmv_tile_kernel<SegSum, f64>",
+                     "traffic": profiled_traffic("spmv_tile_kernel_segsum_f64_powerlaw4M")},
+        "e2e": {"value": e2e, "unit": "GB/s", "h2d_bytes_per_step": n * 8,
+                "d2h_bytes_per_step": n * 8, "steps": e2e_steps,
+                "api": "SPMV.__call__ host arrays -> la_spmv_host", "matches_device": bool(ok)},
+        "gpu_launches": args.steps,
+        "clocks": sampler.summary(),
+    }
+    if rank == 0 and world == 1:
+        try:
+            sec, T, reps, kind = cpu_reference_spmv(n, ai, aj, av, x)
+            result["cpu_baseline"] = {"value": byt / sec / 1e9, "unit": "GB/s", "cores": T,
+                                      "kind": kind,
+                                      "sample": f"{reps} full SegSumSPMV calls (median)"}
+        except Exception as ex:  # reported, never silently replaced
+            result["cpu_baseline"] = {"value": None, "unit": "GB/s", "cores": None,
+                                      "kind": "reference", "sample": f"failed: {ex}"}
+        if not args.no_extras:
+            ex, mats = extras(la, torch, peak)
+            result["extras"] = ex
+            if not args.no_cpu_pcg:
+                try:
+                    ex["pcg"]["cpu_reference"] = cpu_pcg(mats)
+                except Exception as e:
+                    ex["pcg"]["cpu_reference"] = {"error": str(e)}
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

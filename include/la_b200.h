@@ -1,0 +1,238 @@
+/* la_b200.h -- C-ABI of the B200-native sparse hot path.
+ *
+ * Drop-in replacement, for one NVIDIA B200 (sm_100a), of the sparse hot
+ * path of miaodi/linearAlgebra: CSR SpMV in its segmented-sum and ALBUS
+ * forms, the level-scheduled triangular solves that apply IC(0)/ILU(0)
+ * factors, the IC(0)-preconditioned CG built on them, and hand-written
+ * adjoints.  Every entry point below names the reference interface it
+ * replaces (path:line within the reference project).
+ *
+ * Conventions (those of the reference, sparse_mat_op/spmv.hpp:16-19):
+ *  - CSR with int32 row pointers `ai[n+1]` and column indices `aj[nnz]`,
+ *    index base 0 or 1 (ai[0] == base), values double (LA_F64) or float
+ *    (LA_F32);
+ *  - SpMV computes y = alpha * A * x + beta * y (the reference names the
+ *    input b and the output x); when beta == 0, y is not read;
+ *  - the caller owns every array passed in; handles own device copies;
+ *  - a handle is used from one stream and one host thread at a time, as the
+ *    reference objects are (their operator() mutates scratch);
+ *  - pointers passed to the `_host` entry points are host memory; all other
+ *    vector pointers are device memory;
+ *  - every call returns an la_status; la_last_error_string() describes the
+ *    last failure of the calling thread.
+ * No function here falls back to the CPU: without a usable CUDA device the
+ * device entry points return LA_ERR_NO_DEVICE.
+ */
+#ifndef LA_B200_H
+#define LA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  LA_OK = 0,
+  LA_ERR_INVALID_ARG = 1,
+  LA_ERR_BAD_CSR = 2,       /* fails ValidCSR (matrix_utils.hpp:985-1014) */
+  LA_ERR_CUDA = 3,          /* a CUDA runtime call failed */
+  LA_ERR_TIMEOUT = 4,       /* a bounded device wait gave up */
+  LA_ERR_BREAKDOWN = 5,     /* IC pivot < 0 (precond.hpp:684-685) */
+  LA_ERR_NOT_CONVERGED = 6, /* iteration limit reached */
+  LA_ERR_NO_DEVICE = 7,     /* no usable sm_100 device */
+  LA_ERR_ALLOC = 8
+} la_status;
+
+typedef enum { LA_F64 = 0, LA_F32 = 1 } la_dtype;
+
+typedef enum {
+  LA_SPMV_SEGSUM = 0, /* SegSumSPMV, sparse_mat_op/spmv.hpp:59-185 */
+  LA_SPMV_ALBUS = 1   /* ALBUSSPMV,  sparse_mat_op/spmv.hpp:186-300 */
+} la_spmv_kind;
+
+typedef enum { LA_LOWER = 0, LA_UPPER = 1 } la_uplo; /* TriangularMatrix L/U,
+                                                        matrix_utils.hpp:581 */
+
+typedef struct la_csr_s *la_csr_t;
+typedef struct la_spmv_plan_s *la_spmv_plan_t;
+typedef struct la_trsv_plan_s *la_trsv_plan_t;
+typedef struct la_pcg_s *la_pcg_t;
+typedef void *la_stream_t; /* a cudaStream_t; NULL is the legacy stream */
+
+/* ---------------------------------------------------------------- misc */
+const char *la_last_error_string(void);
+/* Library version string. */
+const char *la_version(void);
+/* Number of SMs of the current device (0 if none); a liveness probe. */
+la_status la_device_sm_count(int *sms);
+
+/* ---------------------------------------------------------- CSR handle */
+/* Device copy of a CSR matrix (the reference's CSRMatrix* containers,
+ * matrix_utils.hpp:37-103).  ai/aj/av are HOST arrays; the structure is
+ * validated with ValidCSR semantics (matrix_utils.hpp:985-1014: ai[0] ==
+ * base, rows sorted, no duplicates, columns in range) before upload.
+ * `flags` bit 0 (LA_CSR_KEEP_F32): also keep an FP32 copy of FP64 values,
+ * used by the mixed-precision solver. */
+#define LA_CSR_KEEP_F32 1
+la_status la_csr_create(int n, int ncols, int base, const int *ai,
+                        const int *aj, const void *av, la_dtype dtype,
+                        int flags, la_csr_t *out);
+/* Same, from DEVICE arrays (copied; no validation beyond sizes). */
+la_status la_csr_create_device(int n, int ncols, int nnz, int base,
+                               const int *d_ai, const int *d_aj,
+                               const void *d_av, la_dtype dtype, int flags,
+                               la_csr_t *out);
+/* Replace the values (same pattern); av is host memory if on_device == 0. */
+la_status la_csr_update_values(la_csr_t A, const void *av, int on_device);
+la_status la_csr_info(la_csr_t A, int *n, int *ncols, int *nnz, int *base,
+                      la_dtype *dtype);
+la_status la_csr_destroy(la_csr_t A);
+
+/* ---------------------------------------------------------------- SpMV */
+/* Plan = the reference's preprocess() (SegSumSPMV::preprocess,
+ * spmv.hpp:68-77; ALBUSSPMV::preprocess, spmv.hpp:195-228): the nnz are cut
+ * into equal tiles and the start row of every tile is found by binary
+ * search, once.  Scratch for cross-tile partial rows is owned by the plan. */
+la_status la_spmv_plan_create(la_csr_t A, la_spmv_kind kind,
+                              la_spmv_plan_t *out);
+/* y = alpha*A*x + beta*y on the device (SegSumSPMV::operator(),
+ * spmv.hpp:79-177; ALBUSSPMV::operator(), spmv.hpp:230-293; SPMV<>
+ * adapter, spmv.hpp:326-330).  x, y device arrays of `vdtype`: LA_F64 needs
+ * an FP64 matrix; LA_F32 vectors use the FP32 values (an FP32 matrix or the
+ * LA_CSR_KEEP_F32 copy) and accumulate in FP32. */
+la_status la_spmv(la_spmv_plan_t plan, double alpha, const void *x,
+                  double beta, void *y, la_dtype vdtype, la_stream_t stream);
+/* Host-pointer form of the same call: x (n doubles) is copied in, y copied
+ * in when beta != 0 and out always; synchronous.  This is the path the
+ * C++ drop-in classes (include/la_b200.hpp) take for host vectors. */
+la_status la_spmv_host(la_spmv_plan_t plan, double alpha, const double *x,
+                       double beta, double *y);
+la_status la_spmv_plan_destroy(la_spmv_plan_t plan);
+
+/* Adjoints of y = A x (no reference counterpart; the reference has none).
+ * la_spmv_transpose: out = alpha * A^T g + beta * out (dL/dx), through a
+ * transposed copy of A built once per plan on first use (the role
+ * ForwardSubstitutionT plays for triangles, triangle_solve.hpp:87-98).
+ * la_sddmm_pattern: dv[k] = alpha * g[row(k)] * x[col(k)] over the stored
+ * pattern (dL/dvalues).  FP64 only. */
+la_status la_spmv_transpose(la_spmv_plan_t plan, double alpha, const double *g,
+                            double beta, double *out, la_stream_t stream);
+la_status la_sddmm_pattern(la_spmv_plan_t plan, double alpha, const double *g,
+                           const double *x, double *dv, la_stream_t stream);
+
+/* ------------------------------------------------------- host analysis */
+/* TopologicalSort2<L|U> (matrix_utils.hpp:637-675), bit-identical output:
+ * iperm[n] (values i + base, ordered by level then row) and zero-based
+ * prefix[levels + 1] (caller provides n + 1 ints).  Returns the level
+ * count in *levels. */
+la_status la_topological_sort2(la_uplo uplo, int n, int base, const int *ai,
+                               const int *aj, int *iperm, int *prefix,
+                               int *levels);
+/* SerialCM reverse Cuthill-McKee (reordering/Reordering.cpp:37-136),
+ * bit-identical iperm/perm (values carry the base). */
+la_status la_rcm(int n, int base, const int *ai, const int *aj, int *iperm,
+                 int *perm);
+/* permute (matrix_utils.hpp:429-472): B(i,:) = A(iperm[i],:), columns mapped
+ * through perm (may be NULL: rows only, permuteRow :474-480) and re-sorted. */
+la_status la_permute(int n, int base, const int *ai, const int *aj,
+                     const double *av, const int *iperm, const int *perm,
+                     int *p_ai, int *p_aj, double *p_av);
+/* ParallelTranspose2 (matrix_utils.hpp:311-390). av/t_av may be NULL. */
+la_status la_transpose(int rows, int cols, int base, const int *ai,
+                       const int *aj, const double *av, int *t_ai, int *t_aj,
+                       double *t_av);
+/* SplitLDU (matrix_utils.hpp:720-803); outputs sized nnz / n + 1 / n. */
+la_status la_split_ldu(int n, int base, const int *ai, const int *aj,
+                       const double *av, int *l_ai, int *l_aj, double *l_av,
+                       double *d, int *u_ai, int *u_aj, double *u_av,
+                       int *lnnz, int *unnz);
+/* SplitTriangle<L|U> (matrix_utils.hpp:805-879), incl. the diagonal. */
+la_status la_split_triangle(la_uplo uplo, int n, int base, const int *ai,
+                            const int *aj, const double *av, int *t_ai,
+                            int *t_aj, double *t_av, int *tnnz);
+/* ValidCSR (matrix_utils.hpp:985-1014): LA_OK or LA_ERR_BAD_CSR. */
+la_status la_valid_csr(int rows, int cols, int base, const int *ai,
+                       const int *aj);
+/* IC(0) numeric factor, ICCLevel0SymSymbolic + ICCLevelNumeric
+ * (precond.hpp:13-37, 615-693): u_* is the upper triangle of an SPD matrix
+ * with the diagonal first in each row; icc_av (same pattern) receives U
+ * with A ~= U^T U.  omega shifts the diagonal by (1 + omega).
+ * LA_ERR_BREAKDOWN on a negative pivot. */
+la_status la_icc0(int n, int base, const int *u_ai, const int *u_aj,
+                  const double *u_av, double omega, double *icc_av);
+/* incomplete_cholesky_k_2::numeric_factorize shift-retry loop
+ * (mkl_wrapper/incomplete_cholesky.cpp:315-342): on breakdown retry with
+ * shift = max(2 * shift, 1e-3), at most 20 restarts.  *shift_used gets the
+ * final shift. */
+la_status la_icc0_shifted(int n, int base, const int *u_ai, const int *u_aj,
+                          const double *u_av, double *icc_av,
+                          double *shift_used);
+
+/* ------------------------------------------------- triangular solves */
+/* OptimizedTriangularSolve<Barrier, L|U>::analysis (triangle_solve.hpp:
+ * 157-159, triangle_solve.tpp:17-113): levels by TopologicalSort2 on the
+ * host, rows stored in execution (level) order, uploaded once.  ai/aj/av:
+ * HOST CSR of the STRICT triangle; diag: host array of n values or NULL
+ * (unit diagonal).  `dtype` selects FP64 or FP32 storage (FP32 values and
+ * FP32 vectors in la_trsv).  The persistent solve kernel walks the levels
+ * with per-row readiness (no launch per level) and bounded waits. */
+la_status la_trsv_analysis(la_uplo uplo, int n, int base, const int *ai,
+                           const int *aj, const double *av,
+                           const double *diag, la_dtype dtype,
+                           la_trsv_plan_t *out);
+/* x = T^-1 b (triangle_solve.tpp:115-155 operator()/BarrierOp): b, x device
+ * arrays of the plan's dtype; b and x must not alias.  LA_ERR_TIMEOUT if a
+ * dependency wait exceeded its bound (x is then undefined). */
+la_status la_trsv(la_trsv_plan_t plan, const void *b, void *x,
+                  la_stream_t stream);
+/* Asynchronous form of la_trsv: launches and returns without waiting; a
+ * timeout is recorded in the plan and reported by la_trsv_status. */
+la_status la_trsv_launch(la_trsv_plan_t plan, const void *b, void *x,
+                         la_stream_t stream);
+/* Synchronises `stream` and returns LA_ERR_TIMEOUT if any launch of this
+ * plan since the last status check gave up on a wait (then clears it). */
+la_status la_trsv_status(la_trsv_plan_t plan, la_stream_t stream);
+/* Host-pointer form (synchronous). */
+la_status la_trsv_host(la_trsv_plan_t plan, const double *b, double *x);
+/* Level structure of the plan: *levels, and if non-NULL iperm[n] /
+ * prefix[levels + 1] exactly as TopologicalSort2 returns them. */
+la_status la_trsv_levels(la_trsv_plan_t plan, int *levels, int *iperm,
+                         int *prefix);
+la_status la_trsv_plan_destroy(la_trsv_plan_t plan);
+
+/* ---------------------------------------------------------- IC(0)-PCG */
+/* Solver state for A x = b with the IC(0) preconditioner U^T U; the role of
+ * mkl_pcg_solver + incomplete_cholesky_k_2 (mkl_wrapper/mkl_solver.cpp:
+ * 150-251, mkl_wrapper/incomplete_cholesky.cpp:21-29, 286-342).
+ * A: FP64 CSR handle (full symmetric storage).  u_ai/u_aj/icc_av: HOST IC
+ * factor U (upper, diagonal first, as la_icc0 returns).  mode LA_PCG_FP64:
+ * everything FP64.  mode LA_PCG_MIXED: FP64 outer iterative refinement
+ * (r = b - A x with FP64 A, FP64 update) around an inner PCG whose SpMV and
+ * triangular solves read FP32 A / FP32 factors and accumulate in FP32,
+ * with FP64 dot products and norms. */
+typedef enum { LA_PCG_FP64 = 0, LA_PCG_MIXED = 1 } la_pcg_mode;
+typedef struct {
+  int iterations;        /* total (inner) PCG iterations */
+  int outer_iterations;  /* refinement steps (1 for FP64) */
+  double rel_residual;   /* true ||b - A x|| / ||b|| in FP64 at exit */
+  double solve_ms;       /* device time of the solve, CUDA events */
+} la_pcg_info;
+la_status la_pcg_create(la_csr_t A, const int *u_ai, const int *u_aj,
+                        const double *icc_av, la_pcg_mode mode,
+                        la_pcg_t *out);
+/* Solve to ||b - A x|| / ||b|| < rtol (the reference's user stopping test,
+ * mkl_solver.cpp:211-225), x0 = 0.  b, x: device FP64 arrays.
+ * LA_ERR_NOT_CONVERGED if maxit is reached (x holds the last iterate). */
+la_status la_pcg_solve(la_pcg_t s, const double *b, double *x, double rtol,
+                       int maxit, la_pcg_info *info, la_stream_t stream);
+/* Host-pointer form (synchronous): b, x host arrays of n doubles. */
+la_status la_pcg_solve_host(la_pcg_t s, const double *b, double *x,
+                            double rtol, int maxit, la_pcg_info *info);
+la_status la_pcg_destroy(la_pcg_t s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LA_B200_H */

@@ -1,0 +1,390 @@
+"""Python mirror of the reference's hot-path interface over the C-ABI.
+
+Names, argument order and meaning follow the reference's C++ API
+(sparse_mat_op/spmv.hpp, triangle_solve.hpp, matrix_utils.hpp,
+precond.hpp, reordering/Reordering.cpp):
+
+* ``SegSumSPMV`` / ``ALBUSSPMV``: ``preprocess(size, base, ai, aj, av)`` then
+  ``spmv(size, base, ai, aj, av, b, x, alpha, beta)`` computing
+  x = alpha*A*b + beta*x (spmv.hpp:68-82, 195-233).  ``preprocess`` uploads
+  the matrix and builds the tile plan once; later calls must pass the same
+  matrix (as the reference's preprocessed state assumes).  ``b`` / ``x`` may
+  be numpy arrays (host path: copied in and out) or CUDA torch tensors
+  (device path, on the current stream).
+* ``SPMV(csr, kind)``: the ``SPMV<CSR, Impl>`` adapter (spmv.hpp:310-334).
+* ``OptimizedTriangularSolve(uplo)``: ``analysis(rows, base, ai, aj, av,
+  diag=None)`` then ``solve(b, x)`` (triangle_solve.hpp:149-171).
+* ``TopologicalSort2``, ``SplitLDU``, ``SplitTriangle``, ``Transpose``,
+  ``Permute``, ``ValidCSR``, ``ICCLevelNumeric0``, ``SerialCM``: the host
+  preprocessing steps, bit-identical to the reference's.
+* ``PCG``: IC(0)-preconditioned CG (FP64 or mixed precision).
+
+Everything computes on the GPU through liblab200.so; nothing falls back to
+the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import (LA_CSR_KEEP_F32, LA_F32, LA_F64, LA_LOWER, LA_PCG_FP64,
+                   LA_PCG_MIXED, LA_SPMV_ALBUS, LA_SPMV_SEGSUM, LA_UPPER,
+                   LAError, PcgInfo, call)
+
+__all__ = [
+    "CSR", "SPMV", "SegSumSPMV", "ALBUSSPMV", "OptimizedTriangularSolve",
+    "TopologicalSort2", "SplitLDU", "SplitTriangle", "Transpose", "Permute",
+    "ValidCSR", "ICCLevelNumeric0", "ICCShifted", "SerialCM", "PCG", "LAError",
+    "spmv_transpose", "sddmm_pattern",
+]
+
+
+def _i32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _ptr(a) -> C.c_void_p:
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return C.c_void_p(a.ctypes.data)
+    return C.c_void_p(a.data_ptr())  # torch tensor
+
+
+def _stream(t) -> C.c_void_p:
+    import torch
+    return C.c_void_p(torch.cuda.current_stream(t.device).cuda_stream)
+
+
+def _is_device(a) -> bool:
+    return not isinstance(a, np.ndarray) and getattr(a, "is_cuda", False)
+
+
+# ------------------------------------------------------------------ CSR
+class CSR:
+    """Device copy of a CSR matrix (host arrays are validated and copied)."""
+
+    def __init__(self, n, ncols, base, ai, aj, av, dtype=np.float64,
+                 keep_f32=False):
+        ai, aj = _i32(ai), _i32(aj)
+        av = np.ascontiguousarray(av, dtype=dtype)
+        self.n, self.ncols, self.base = int(n), int(ncols), int(base)
+        self.nnz = int(ai[n] - base)
+        self.dtype = np.dtype(dtype)
+        h = C.c_void_p()
+        call("la_csr_create", self.n, self.ncols, self.base, _ptr(ai), _ptr(aj),
+             _ptr(av), LA_F64 if self.dtype == np.float64 else LA_F32,
+             LA_CSR_KEEP_F32 if keep_f32 else 0, C.byref(h))
+        self.h = h
+        self.host = (ai, aj, av)
+
+    def update_values(self, av):
+        if _is_device(av):
+            call("la_csr_update_values", self.h, _ptr(av), 1)
+        else:
+            av = np.ascontiguousarray(av, dtype=self.dtype)
+            call("la_csr_update_values", self.h, _ptr(av), 0)
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value:
+            _lib.lib().la_csr_destroy(h)
+            self.h = None
+
+
+class SPMV:
+    """``SPMV<CSR, Impl>`` (spmv.hpp:310-334): y = alpha*A*x + beta*y."""
+
+    def __init__(self, A: CSR, kind: int = LA_SPMV_SEGSUM):
+        self.A = A
+        h = C.c_void_p()
+        call("la_spmv_plan_create", A.h, int(kind), C.byref(h))
+        self.h = h
+
+    def __call__(self, b, x, alpha=1.0, beta=0.0):
+        """x = alpha*A*b + beta*x; b/x numpy (host path) or CUDA tensors."""
+        if _is_device(b):
+            import torch
+            vd = LA_F64 if b.dtype == torch.float64 else LA_F32
+            call("la_spmv", self.h, float(alpha), _ptr(b), float(beta), _ptr(x),
+                 vd, _stream(b))
+        else:
+            if not (isinstance(x, np.ndarray) and x.dtype == np.float64
+                    and x.flags.c_contiguous):
+                raise TypeError("host x must be a C-contiguous float64 array")
+            b = _f64(b)
+            call("la_spmv_host", self.h, float(alpha), _ptr(b), float(beta),
+                 _ptr(x))
+        return x
+
+    def transpose(self, g, out, alpha=1.0, beta=0.0):
+        """out = alpha*A^T g + beta*out (device FP64 tensors)."""
+        call("la_spmv_transpose", self.h, float(alpha), _ptr(g), float(beta),
+             _ptr(out), _stream(g))
+        return out
+
+    def sddmm(self, g, x, dv, alpha=1.0):
+        """dv[k] = alpha*g[row(k)]*x[col(k)] (device FP64 tensors)."""
+        call("la_sddmm_pattern", self.h, float(alpha), _ptr(g), _ptr(x),
+             _ptr(dv), _stream(g))
+        return dv
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value:
+            _lib.lib().la_spmv_plan_destroy(h)
+            self.h = None
+
+
+def spmv_transpose(plan: SPMV, g, out, alpha=1.0, beta=0.0):
+    return plan.transpose(g, out, alpha, beta)
+
+
+def sddmm_pattern(plan: SPMV, g, x, dv, alpha=1.0):
+    return plan.sddmm(g, x, dv, alpha)
+
+
+class SegSumSPMV:
+    """``SegSumSPMV`` (spmv.hpp:59-185) on the GPU."""
+
+    KIND = LA_SPMV_SEGSUM
+
+    def __init__(self, num_threads: int | None = None):
+        self._nthreads = num_threads  # kept for API parity; the GPU ignores it
+        self._plan = None
+        self._key = None
+
+    def setNumThreads(self, num_threads: int):
+        self._nthreads = num_threads
+
+    def preprocess(self, size, base, ai, aj, av):
+        ai, aj, av = _i32(ai), _i32(aj), _f64(av)
+        ncols = int(aj.max()) + 1 - base if aj.size else size
+        ncols = max(ncols, size)
+        self._A = CSR(size, ncols, base, ai, aj, av)
+        self._plan = SPMV(self._A, self.KIND)
+        self._key = (int(size), int(base))
+
+    def __call__(self, size, base, ai, aj, av, b, x, alpha=1.0, beta=0.0):
+        if self._plan is None or self._key != (int(size), int(base)):
+            self.preprocess(size, base, ai, aj, av)
+        return self._plan(b, x, alpha, beta)
+
+
+class ALBUSSPMV(SegSumSPMV):
+    """``ALBUSSPMV`` (spmv.hpp:186-300) on the GPU."""
+
+    KIND = LA_SPMV_ALBUS
+
+
+# ----------------------------------------------------------- triangular
+class OptimizedTriangularSolve:
+    """``OptimizedTriangularSolve<Barrier, L|U>`` (triangle_solve.hpp:149-208)."""
+
+    def __init__(self, uplo: str = "L", num_threads: int | None = None,
+                 dtype=np.float64):
+        self.uplo = LA_LOWER if uplo in ("L", 0, LA_LOWER) else LA_UPPER
+        self._nthreads = num_threads
+        self.dtype = np.dtype(dtype)
+        self.h = None
+
+    def analysis(self, rows, base, ai, aj, av, diag=None):
+        ai, aj, av = _i32(ai), _i32(aj), _f64(av)
+        d = None if diag is None else _f64(diag)
+        h = C.c_void_p()
+        call("la_trsv_analysis", self.uplo, int(rows), int(base), _ptr(ai),
+             _ptr(aj), _ptr(av), _ptr(d),
+             LA_F64 if self.dtype == np.float64 else LA_F32, C.byref(h))
+        self.h = h
+        self.n = int(rows)
+        return self
+
+    def levels(self):
+        lv = C.c_int()
+        call("la_trsv_levels", self.h, C.byref(lv), None, None)
+        iperm = np.empty(self.n, np.int32)
+        prefix = np.empty(lv.value + 1, np.int32)
+        call("la_trsv_levels", self.h, C.byref(lv), _ptr(iperm), _ptr(prefix))
+        return lv.value, iperm, prefix
+
+    def __call__(self, b, x):
+        if _is_device(b):
+            call("la_trsv", self.h, _ptr(b), _ptr(x), _stream(b))
+        else:
+            b = _f64(b)
+            call("la_trsv_host", self.h, _ptr(b), _ptr(x))
+        return x
+
+    def launch(self, b, x):
+        """Asynchronous device solve; errors surface in status()."""
+        call("la_trsv_launch", self.h, _ptr(b), _ptr(x), _stream(b))
+        return x
+
+    def status(self, t):
+        call("la_trsv_status", self.h, _stream(t))
+
+    def get_num_threads(self):
+        return self._nthreads
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value:
+            _lib.lib().la_trsv_plan_destroy(h)
+            self.h = None
+
+
+# --------------------------------------------------------- host analysis
+def TopologicalSort2(uplo, nodes, base, ai, aj):
+    """Level sets (matrix_utils.hpp:637-675): returns (levels, iperm, prefix)."""
+    ai, aj = _i32(ai), _i32(aj)
+    iperm = np.empty(nodes, np.int32)
+    prefix = np.empty(nodes + 1, np.int32)
+    lv = C.c_int()
+    call("la_topological_sort2", LA_LOWER if uplo in ("L", 0) else LA_UPPER,
+         int(nodes), int(base), _ptr(ai), _ptr(aj), _ptr(iperm), _ptr(prefix),
+         C.byref(lv))
+    return lv.value, iperm, prefix[: lv.value + 1].copy()
+
+
+def SerialCM(n, base, ai, aj):
+    """Reverse Cuthill-McKee (reordering/Reordering.cpp:37-136): (iperm, perm)."""
+    ai, aj = _i32(ai), _i32(aj)
+    iperm = np.empty(n, np.int32)
+    perm = np.empty(n, np.int32)
+    call("la_rcm", int(n), int(base), _ptr(ai), _ptr(aj), _ptr(iperm), _ptr(perm))
+    return iperm, perm
+
+
+def Permute(n, base, ai, aj, av, iperm, perm=None):
+    """matrix_utils.hpp:429-480: B(i,:) = A(iperm[i],:), columns via perm."""
+    ai, aj, av, iperm = _i32(ai), _i32(aj), _f64(av), _i32(iperm)
+    perm = None if perm is None else _i32(perm)
+    nnz = int(ai[n] - base)
+    p_ai = np.empty(n + 1, np.int32)
+    p_aj = np.empty(max(nnz, 1), np.int32)
+    p_av = np.empty(max(nnz, 1), np.float64)
+    call("la_permute", int(n), int(base), _ptr(ai), _ptr(aj), _ptr(av),
+         _ptr(iperm), _ptr(perm), _ptr(p_ai), _ptr(p_aj), _ptr(p_av))
+    return p_ai, p_aj[:nnz], p_av[:nnz]
+
+
+def Transpose(rows, cols, base, ai, aj, av=None):
+    """ParallelTranspose2 (matrix_utils.hpp:311-390)."""
+    ai, aj = _i32(ai), _i32(aj)
+    avp = None if av is None else _f64(av)
+    nnz = int(ai[rows] - base)
+    t_ai = np.empty(cols + 1, np.int32)
+    t_aj = np.empty(max(nnz, 1), np.int32)
+    t_av = None if av is None else np.empty(max(nnz, 1), np.float64)
+    call("la_transpose", int(rows), int(cols), int(base), _ptr(ai), _ptr(aj),
+         _ptr(avp), _ptr(t_ai), _ptr(t_aj), _ptr(t_av))
+    return t_ai, t_aj[:nnz], (None if t_av is None else t_av[:nnz])
+
+
+def SplitLDU(n, base, ai, aj, av):
+    """SplitLDU (matrix_utils.hpp:720-803): ((L), D, (U)) as CSR triples."""
+    ai, aj, av = _i32(ai), _i32(aj), _f64(av)
+    nnz = max(int(ai[n] - base), 1)
+    l_ai, u_ai = np.empty(n + 1, np.int32), np.empty(n + 1, np.int32)
+    l_aj, u_aj = np.empty(nnz, np.int32), np.empty(nnz, np.int32)
+    l_av, u_av = np.empty(nnz, np.float64), np.empty(nnz, np.float64)
+    d = np.empty(n, np.float64)
+    ln, un = C.c_int(), C.c_int()
+    call("la_split_ldu", int(n), int(base), _ptr(ai), _ptr(aj), _ptr(av),
+         _ptr(l_ai), _ptr(l_aj), _ptr(l_av), _ptr(d), _ptr(u_ai), _ptr(u_aj),
+         _ptr(u_av), C.byref(ln), C.byref(un))
+    return ((l_ai, l_aj[: ln.value].copy(), l_av[: ln.value].copy()), d,
+            (u_ai, u_aj[: un.value].copy(), u_av[: un.value].copy()))
+
+
+def SplitTriangle(uplo, n, base, ai, aj, av):
+    """SplitTriangle<L|U> (matrix_utils.hpp:805-879), diagonal included."""
+    ai, aj, av = _i32(ai), _i32(aj), _f64(av)
+    nnz = max(int(ai[n] - base), 1)
+    t_ai, t_aj, t_av = (np.empty(n + 1, np.int32), np.empty(nnz, np.int32),
+                        np.empty(nnz, np.float64))
+    tn = C.c_int()
+    call("la_split_triangle", LA_LOWER if uplo in ("L", 0) else LA_UPPER,
+         int(n), int(base), _ptr(ai), _ptr(aj), _ptr(av), _ptr(t_ai),
+         _ptr(t_aj), _ptr(t_av), C.byref(tn))
+    return t_ai, t_aj[: tn.value].copy(), t_av[: tn.value].copy()
+
+
+def ValidCSR(rows, cols, base, ai, aj) -> bool:
+    """ValidCSR (matrix_utils.hpp:985-1014)."""
+    ai, aj = _i32(ai), _i32(aj)
+    st = call("la_valid_csr", int(rows), int(cols), int(base), _ptr(ai),
+              _ptr(aj), ok=(0, 2))
+    return st == 0
+
+
+def ICCLevelNumeric0(n, base, u_ai, u_aj, u_av, omega=0.0):
+    """IC(0) factor (precond.hpp:13-37, 615-693) of the upper triangle.
+
+    Returns the factor values; raises LAError(LA_ERR_BREAKDOWN) on a
+    negative pivot, the reference's ``false`` return.
+    """
+    u_ai, u_aj, u_av = _i32(u_ai), _i32(u_aj), _f64(u_av)
+    out = np.empty_like(u_av)
+    call("la_icc0", int(n), int(base), _ptr(u_ai), _ptr(u_aj), _ptr(u_av),
+         float(omega), _ptr(out))
+    return out
+
+
+def ICCShifted(n, base, u_ai, u_aj, u_av):
+    """IC(0) with the reference's shift-retry loop; returns (values, shift)."""
+    u_ai, u_aj, u_av = _i32(u_ai), _i32(u_aj), _f64(u_av)
+    out = np.empty_like(u_av)
+    sh = C.c_double()
+    call("la_icc0_shifted", int(n), int(base), _ptr(u_ai), _ptr(u_aj),
+         _ptr(u_av), _ptr(out), C.byref(sh))
+    return out, sh.value
+
+
+# ------------------------------------------------------------------- PCG
+@dataclass
+class PCGResult:
+    iterations: int
+    outer_iterations: int
+    rel_residual: float
+    solve_ms: float
+    status: str
+
+
+class PCG:
+    """IC(0)-PCG (mkl_solver.cpp:150-251 + incomplete_cholesky.cpp:21-29)."""
+
+    def __init__(self, A: CSR, u_ai, u_aj, icc_av, mixed: bool = False):
+        self.A = A
+        u_ai, u_aj, icc_av = _i32(u_ai), _i32(u_aj), _f64(icc_av)
+        h = C.c_void_p()
+        call("la_pcg_create", A.h, _ptr(u_ai), _ptr(u_aj), _ptr(icc_av),
+             LA_PCG_MIXED if mixed else LA_PCG_FP64, C.byref(h))
+        self.h = h
+
+    def solve(self, b, x, rtol=1e-10, maxit=10000, allow_not_converged=False):
+        info = PcgInfo()
+        ok = (0, 6) if allow_not_converged else (0,)
+        if _is_device(b):
+            st = call("la_pcg_solve", self.h, _ptr(b), _ptr(x), float(rtol),
+                      int(maxit), C.byref(info), _stream(b), ok=ok)
+        else:
+            b = _f64(b)
+            st = call("la_pcg_solve_host", self.h, _ptr(b), _ptr(x),
+                      float(rtol), int(maxit), C.byref(info), ok=ok)
+        return PCGResult(info.iterations, info.outer_iterations,
+                         info.rel_residual, info.solve_ms,
+                         _lib.STATUS_NAMES.get(st, str(st)))
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value:
+            _lib.lib().la_pcg_destroy(h)
+            self.h = None

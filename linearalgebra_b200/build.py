@@ -1,0 +1,83 @@
+"""Build the CUDA library in-tree: linearalgebra_b200/liblab200.so.
+
+Every source under csrc/ is compiled by nvcc for sm_100a only
+(-gencode arch=compute_100a,code=sm_100a) with -lineinfo, objects go to
+linearalgebra_b200/_build/, and the shared library is linked next to this
+file so that it travels with the source tree.  The CUDA runtime is linked
+statically; torch (used by the tests for device memory) keeps its own.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+CSRC = PKG / "csrc"
+OUT = PKG / "liblab200.so"
+BUILD = PKG / "_build"
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = [
+    "-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr",
+    "-Xcompiler", "-fPIC,-O3", "-Xptxas", "-O3",
+] + ARCH
+
+
+def nvcc() -> str:
+    cand = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(cand).exists():
+        raise RuntimeError("nvcc not found")
+    return cand
+
+
+def _sources() -> list[Path]:
+    return sorted(list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cpp")))
+
+
+def _compile(src: Path, verbose_ptxas: bool) -> Path:
+    obj = BUILD / (src.name + ".o")
+    cmd = [nvcc(), *NVCC_FLAGS, "-c", str(src), "-o", str(obj)]
+    if src.suffix == ".cpp":
+        cmd[1:1] = ["-x", "cu"]
+    if verbose_ptxas:
+        cmd += ["-Xptxas", "-v"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {src.name}:\n{res.stdout}\n{res.stderr}")
+    if verbose_ptxas and res.stderr:
+        sys.stderr.write(res.stderr)
+    return obj
+
+
+def _stale() -> bool:
+    if not OUT.exists():
+        return True
+    t = OUT.stat().st_mtime
+    deps = _sources() + list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + \
+        [PKG.parent / "include" / "la_b200.h", Path(__file__)]
+    return any(p.stat().st_mtime > t for p in deps)
+
+
+def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
+    """Compile (if stale) and return the path of liblab200.so."""
+    if not force and not _stale():
+        return OUT
+    BUILD.mkdir(exist_ok=True)
+    srcs = _sources()
+    with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 2)) as ex:
+        objs = list(ex.map(lambda s: _compile(s, verbose_ptxas), srcs))
+    tmp = OUT.with_suffix(".so.tmp")
+    cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs)]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")
+    os.replace(tmp, OUT)
+    return OUT
+
+
+if __name__ == "__main__":
+    p = build(force="--force" in sys.argv, verbose_ptxas="-v" in sys.argv)
+    print(p)

@@ -1,0 +1,86 @@
+// la_device.cuh -- device helpers shared by the kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace la {
+namespace dev {
+
+// Streaming loads for matrix data read once per call: non-coherent path,
+// no L1 allocation (x and y keep the L1/L2 room).
+__device__ __forceinline__ int4 ld_stream(const int4 *p) {
+  int4 r;
+  asm("ld.global.nc.L1::no_allocate.v4.s32 {%0,%1,%2,%3}, [%4];"
+      : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+      : "l"(p));
+  return r;
+}
+__device__ __forceinline__ double2 ld_stream(const double2 *p) {
+  double2 r;
+  asm("ld.global.nc.L1::no_allocate.v2.f64 {%0,%1}, [%2];"
+      : "=d"(r.x), "=d"(r.y)
+      : "l"(p));
+  return r;
+}
+__device__ __forceinline__ float4 ld_stream(const float4 *p) {
+  float4 r;
+  asm("ld.global.nc.L1::no_allocate.v4.f32 {%0,%1,%2,%3}, [%4];"
+      : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
+      : "l"(p));
+  return r;
+}
+template <typename T> __device__ __forceinline__ T ld_stream(const T *p) {
+  return __ldg(p);
+}
+
+// Device-scope relaxed accesses (bypass the non-coherent L1) used for data
+// exchanged between CTAs of one kernel.
+__device__ __forceinline__ double ld_relaxed(const double *p) {
+  double v;
+  asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ float ld_relaxed(const float *p) {
+  float v;
+  asm volatile("ld.relaxed.gpu.global.f32 %0, [%1];" : "=f"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed(double *p, double v) {
+  asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed(float *p, float v) {
+  asm volatile("st.relaxed.gpu.global.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+}
+__device__ __forceinline__ int ld_relaxed(const int *p) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Segmented-sum pair: f = "a segment boundary occurred", v = running sum
+// since the last boundary.  combine(a, b) = (a.f | b.f, b.f ? b.v : a.v+b.v).
+template <typename ACC> struct SegPair {
+  int f;
+  ACC v;
+};
+
+// Inclusive warp-level segmented scan.
+template <typename ACC>
+__device__ __forceinline__ SegPair<ACC> warp_seg_scan_incl(SegPair<ACC> a) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int f = __shfl_up_sync(0xffffffffu, a.f, d);
+    const ACC v = __shfl_up_sync(0xffffffffu, a.v, d);
+    if (lane >= d) {
+      if (!a.f)
+        a.v = v + a.v;
+      a.f |= f;
+    }
+  }
+  return a;
+}
+
+} // namespace dev
+} // namespace la

@@ -1,0 +1,380 @@
+// la_host.cpp -- host-side preprocessing of the sparse hot path.
+//
+// These run once per matrix on the host, as in the reference, and their
+// integer outputs (level sets, permutations, split patterns) must be
+// bit-identical to the reference's; floating-point outputs (IC(0) values)
+// follow the reference's operation order so they are bit-identical too.
+// Each function cites the reference routine it restates.
+
+#include "la_internal.h"
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+namespace la {
+
+// matrix_utils.hpp:985-1014 ValidCSR.
+bool valid_csr(int rows, int cols, int base, const int *ai, const int *aj,
+               std::string *why) {
+  auto fail = [&](const char *m, long r) {
+    if (why) {
+      char buf[128];
+      std::snprintf(buf, sizeof buf, "%s (row %ld)", m, r);
+      *why = buf;
+    }
+    return false;
+  };
+  if (rows < 0 || cols < 0)
+    return fail("negative dimension", -1);
+  if (ai[0] != base)
+    return fail("ai[0] is not equal to base", 0);
+  for (int i = 0; i < rows; i++) {
+    if (ai[i + 1] < ai[i])
+      return fail("ai is not monotonically increasing", i);
+    const int *b = aj + (ai[i] - base), *e = aj + (ai[i + 1] - base);
+    for (const int *p = b; p + 1 < e; p++) {
+      if (p[1] < p[0])
+        return fail("unsorted row", i);
+      if (p[1] == p[0])
+        return fail("duplicate entry in row", i);
+    }
+    if (e > b && (b[0] < base || e[-1] >= cols + base))
+      return fail("column index out of range in row", i);
+  }
+  return true;
+}
+
+// matrix_utils.hpp:637-675 TopologicalSort2.  depth(i) = max over stored
+// entries j of depth(j) + 1, rows visited ascending (L) or descending (U);
+// iperm lists rows by (level, ascending row) with values i + base; prefix is
+// zero-based with levels + 1 entries.
+int topological_sort2(int uplo, int n, int base, const int *ai, const int *aj,
+                      int *iperm, int *prefix) {
+  std::vector<int> depth(n, 0);
+  int levels = 0;
+  for (int k = 0; k < n; k++) {
+    const int i = uplo == LA_LOWER ? k : n - 1 - k;
+    int d = depth[i];
+    for (int j = ai[i] - base; j < ai[i + 1] - base; j++)
+      d = std::max(d, depth[aj[j] - base] + 1);
+    depth[i] = d;
+    levels = std::max(levels, d + 1);
+  }
+  std::fill(prefix, prefix + levels + 1, 0);
+  for (int i = 0; i < n; i++)
+    prefix[depth[i] + 1]++;
+  for (int l = 0; l < levels; l++)
+    prefix[l + 1] += prefix[l];
+  std::vector<int> cursor(prefix, prefix + levels);
+  for (int i = 0; i < n; i++)
+    iperm[cursor[depth[i]]++] = i + base;
+  return levels;
+}
+
+// matrix_utils.hpp:311-390 ParallelTranspose2 (same arrays as the serial
+// form :195-225): a counting sort by column, stable in the source row.
+void transpose(int rows, int cols, int base, const int *ai, const int *aj,
+               const double *av, int *t_ai, int *t_aj, double *t_av) {
+  const int nnz = ai[rows] - base;
+  std::vector<int> pos(cols + 1, 0);
+  for (int k = 0; k < nnz; k++)
+    pos[aj[k] - base + 1]++;
+  std::partial_sum(pos.begin(), pos.end(), pos.begin());
+  for (int c = 0; c <= cols; c++)
+    t_ai[c] = pos[c] + base;
+  const bool vals = av && t_av;
+  for (int i = 0; i < rows; i++)
+    for (int k = ai[i] - base; k < ai[i + 1] - base; k++) {
+      const int q = pos[aj[k] - base]++;
+      t_aj[q] = i + base;
+      if (vals)
+        t_av[q] = av[k];
+    }
+}
+
+// matrix_utils.hpp:429-472 permute / :474-480 permuteRow: row i of the
+// result is row iperm[i] of A, columns renamed through perm (if given) and
+// each row re-sorted by column (the reference's insertion sort is stable
+// for distinct columns, so any sort of distinct keys gives its order).
+void permute(int n, int base, const int *ai, const int *aj, const double *av,
+             const int *iperm, const int *perm, int *p_ai, int *p_aj,
+             double *p_av) {
+  p_ai[0] = base;
+  for (int i = 0; i < n; i++) {
+    const int src = iperm ? iperm[i] - base : i;
+    p_ai[i + 1] = p_ai[i] + (ai[src + 1] - ai[src]);
+  }
+  std::vector<std::pair<int, double>> row;
+  for (int i = 0; i < n; i++) {
+    const int src = iperm ? iperm[i] - base : i;
+    const int o = p_ai[i] - base, s = ai[src] - base, len = ai[src + 1] - ai[src];
+    if (!perm) {
+      std::memcpy(p_aj + o, aj + s, sizeof(int) * len);
+      std::memcpy(p_av + o, av + s, sizeof(double) * len);
+      continue;
+    }
+    row.resize(len);
+    for (int q = 0; q < len; q++)
+      row[q] = {perm[aj[s + q] - base], av[s + q]};
+    std::sort(row.begin(), row.end(),
+              [](const auto &a, const auto &b) { return a.first < b.first; });
+    for (int q = 0; q < len; q++) {
+      p_aj[o + q] = row[q].first;
+      p_av[o + q] = row[q].second;
+    }
+  }
+}
+
+// matrix_utils.hpp:720-803 SplitLDU: strict lower, diagonal (0 when
+// missing), strict upper; entries keep their column order.
+void split_ldu(int n, int base, const int *ai, const int *aj, const double *av,
+               int *l_ai, int *l_aj, double *l_av, double *d, int *u_ai,
+               int *u_aj, double *u_av, int *lnnz, int *unnz) {
+  int lp = 0, up = 0;
+  l_ai[0] = base;
+  u_ai[0] = base;
+  for (int i = 0; i < n; i++) {
+    d[i] = 0;
+    for (int k = ai[i] - base; k < ai[i + 1] - base; k++) {
+      const int c = aj[k] - base;
+      if (c < i) {
+        l_aj[lp] = aj[k];
+        l_av[lp++] = av[k];
+      } else if (c > i) {
+        u_aj[up] = aj[k];
+        u_av[up++] = av[k];
+      } else {
+        d[i] = av[k];
+      }
+    }
+    l_ai[i + 1] = lp + base;
+    u_ai[i + 1] = up + base;
+  }
+  *lnnz = lp;
+  *unnz = up;
+}
+
+// matrix_utils.hpp:805-879 SplitTriangle<L|U>: the triangle incl. diagonal.
+int split_triangle(int uplo, int n, int base, const int *ai, const int *aj,
+                   const double *av, int *t_ai, int *t_aj, double *t_av) {
+  int p = 0;
+  t_ai[0] = base;
+  for (int i = 0; i < n; i++) {
+    for (int k = ai[i] - base; k < ai[i + 1] - base; k++) {
+      const int c = aj[k] - base;
+      if (uplo == LA_UPPER ? c >= i : c <= i) {
+        t_aj[p] = aj[k];
+        t_av[p++] = av[k];
+      }
+    }
+    t_ai[i + 1] = p + base;
+  }
+  return p;
+}
+
+// precond.hpp:615-693 ICCLevelNumeric on the IC(0) pattern (the upper
+// triangle with the diagonal first in each row; precond.hpp:13-37).
+//
+// Up-looking factorisation.  Row j of U starts as row j of A with the
+// diagonal scaled by (1 + omega).  The earlier rows k that hold an entry in
+// column j are found through per-column lists threaded through `next`:
+// after row k is finished (and each time one of its entries is consumed),
+// k is pushed on the list of the column of its next unconsumed entry, with
+// `cursor[k]` pointing at that entry.  The lists are LIFO, and the updates
+// are applied in list order, which is the reference's order; each update
+// subtracts U_kj * U_k,c from the matching entries c of row j.  Finally the
+// pivot p is checked (p < 0: breakdown) and U_jj = sqrt(p), U_jc /= U_jj.
+bool icc0(int n, int base, const int *u_ai, const int *u_aj, const double *u_av,
+          double omega, double *icc_av) {
+  constexpr int kEnd = INT_MAX;
+  std::vector<int> next(n, kEnd), cursor(n, 0);
+  for (int j = 0; j < n; j++) {
+    const int rs = u_ai[j] - base, re = u_ai[j + 1] - base;
+    icc_av[rs] = u_av[rs] * (1.0 + omega);
+    std::memcpy(icc_av + rs + 1, u_av + rs + 1, sizeof(double) * (re - rs - 1));
+    for (int k = next[j]; k < j;) {
+      int ck = cursor[k]++;
+      const int ke = u_ai[k + 1] - base;
+      const int after = next[k];
+      if (ck + 1 < ke) { // push k on the list of its next column
+        const int c = u_aj[ck + 1] - base;
+        next[k] = next[c];
+        next[c] = k;
+      }
+      const double ukj = icc_av[ck];
+      for (int p = rs; ck < ke && p < re;) {
+        if (u_aj[ck] == u_aj[p])
+          icc_av[p++] -= ukj * icc_av[ck++];
+        else if (u_aj[ck] < u_aj[p])
+          ck++;
+        else
+          p++;
+      }
+      k = after;
+    }
+    if (re - rs > 1) {
+      const int c = u_aj[rs + 1] - base;
+      next[j] = next[c];
+      next[c] = j;
+      cursor[j] = rs + 1;
+    }
+    if (icc_av[rs] < 0)
+      return false;
+    const double piv = std::sqrt(icc_av[rs]);
+    icc_av[rs] = piv;
+    for (int p = rs + 1; p < re; p++)
+      icc_av[p] /= piv;
+  }
+  return true;
+}
+
+// reordering/Reordering.cpp:37-136 SerialCM (reverse Cuthill-McKee).
+//
+// Components: the reference's union-find links toward the larger index, so
+// each component's root is its largest node; components are visited in
+// ascending root order and their members in ascending index order
+// (reordering/UnionFind.cpp:83-129, 217-293).  Components of one or two
+// nodes are emitted as is.  Otherwise a pseudo-peripheral source is chosen
+// as the reference executes PseudoDiameter (reordering/Reordering.h:72-136):
+// start at the first node of minimum degree; BFS from it; greedily take up
+// to five last-level candidates by (degree, index), setting the degree of
+// each candidate and of its neighbours to INT_MAX (a persistent change that
+// later breaks the CM ties); BFS from the first candidate -- deeper: it
+// becomes the source and the search repeats; otherwise the search stops.
+// The CM sweep visits the ordering level by level and appends, for each
+// node, its unvisited neighbours of the next BFS level sorted by (degree,
+// index).  The complete ordering is reversed; perm is its inverse.
+namespace {
+struct Bfs {
+  const int *ai, *aj;
+  int base;
+  std::vector<int> level, queue;
+  // BFS from src over its component; returns the level count.
+  int run(int n, int src) {
+    level.assign(n, -1);
+    queue.clear();
+    queue.push_back(src);
+    level[src] = 0;
+    for (size_t h = 0; h < queue.size(); h++) {
+      const int u = queue[h];
+      for (int k = ai[u] - base; k < ai[u + 1] - base; k++) {
+        const int v = aj[k] - base;
+        if (level[v] < 0) {
+          level[v] = level[u] + 1;
+          queue.push_back(v);
+        }
+      }
+    }
+    return level[queue.back()] + 1;
+  }
+};
+} // namespace
+
+void rcm(int n, int base, const int *ai, const int *aj, int *iperm, int *perm) {
+  std::vector<int> deg(n);
+  for (int i = 0; i < n; i++)
+    deg[i] = ai[i + 1] - ai[i];
+  Bfs bfs{ai, aj, base, {}, {}};
+
+  // components, ordered by their largest node; members ascending
+  std::vector<int> comp(n, -1), comp_max;
+  for (int i = 0; i < n; i++) {
+    if (comp[i] >= 0)
+      continue;
+    const int id = (int)comp_max.size();
+    bfs.run(n, i);
+    int mx = i;
+    for (int v : bfs.queue) {
+      comp[v] = id;
+      mx = std::max(mx, v);
+    }
+    comp_max.push_back(mx);
+  }
+  const int ncomp = (int)comp_max.size();
+  std::vector<int> rank(ncomp), start(ncomp + 1, 0), members(n);
+  {
+    int r = 0;
+    for (int i = 0; i < n; i++)
+      if (comp_max[comp[i]] == i)
+        rank[comp[i]] = r++;
+    for (int i = 0; i < n; i++)
+      start[rank[comp[i]] + 1]++;
+    std::partial_sum(start.begin(), start.end(), start.begin());
+    std::vector<int> fill(start.begin(), start.end() - 1);
+    for (int i = 0; i < n; i++)
+      members[fill[rank[comp[i]]]++] = i;
+  }
+
+  std::vector<int> children;
+  for (int c = 0; c < ncomp; c++) {
+    const int off = start[c], size = start[c + 1] - start[c];
+    if (size <= 2) {
+      for (int q = 0; q < size; q++)
+        iperm[off + q] = members[off + q] + base;
+      continue;
+    }
+    int src = members[off];
+    for (int q = off; q < off + size; q++)
+      if (deg[members[q]] < deg[src])
+        src = members[q];
+    for (;;) {
+      const int height = bfs.run(n, src);
+      std::vector<int> last;
+      for (int v : bfs.queue)
+        if (bfs.level[v] == height - 1)
+          last.push_back(v);
+      int first = -1;
+      for (int chosen = 0; chosen < 5; chosen++) {
+        int sel = -1;
+        for (int v : last)
+          if (deg[v] != INT_MAX &&
+              (sel < 0 || deg[v] < deg[sel] || (deg[v] == deg[sel] && v < sel)))
+            sel = v;
+        if (sel < 0)
+          break;
+        if (first < 0)
+          first = sel;
+        deg[sel] = INT_MAX;
+        for (int k = ai[sel] - base; k < ai[sel + 1] - base; k++)
+          deg[aj[k] - base] = INT_MAX;
+      }
+      if (first < 0 || bfs.run(n, first) <= height)
+        break;
+      src = first;
+    }
+    // Cuthill-McKee sweep
+    const int height = bfs.run(n, src);
+    std::vector<int> lstart(height + 1, 0);
+    for (int q = off; q < off + size; q++)
+      lstart[bfs.level[members[q]] + 1]++;
+    std::partial_sum(lstart.begin(), lstart.end(), lstart.begin());
+    int e = off;
+    iperm[e++] = src + base;
+    auto by_deg = [&](int a, int b) {
+      return deg[a] != deg[b] ? deg[a] < deg[b] : a < b;
+    };
+    for (int l = 0; l < height; l++)
+      for (int r = lstart[l]; r < lstart[l + 1]; r++) {
+        const int u = iperm[off + r] - base;
+        children.clear();
+        for (int k = ai[u] - base; k < ai[u + 1] - base; k++) {
+          const int v = aj[k] - base;
+          if (bfs.level[v] == l + 1) {
+            children.push_back(v);
+            bfs.level[v] = -1;
+          }
+        }
+        std::sort(children.begin(), children.end(), by_deg);
+        for (int v : children)
+          iperm[e++] = v + base;
+      }
+  }
+  std::reverse(iperm, iperm + n);
+  for (int i = 0; i < n; i++)
+    perm[iperm[i] - base] = i + base;
+}
+
+} // namespace la

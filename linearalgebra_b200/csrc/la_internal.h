@@ -1,0 +1,135 @@
+// la_internal.h -- shared internals of the B200 sparse hot path library.
+#pragma once
+
+#include "../../include/la_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+namespace la {
+
+// Thread-local last error message (la_last_error_string).
+void set_error(const char *fmt, ...);
+const char *get_error();
+
+#define LA_CUDA_TRY(expr)                                                      \
+  do {                                                                         \
+    cudaError_t _e = (expr);                                                   \
+    if (_e != cudaSuccess) {                                                   \
+      ::la::set_error("%s failed: %s (%s:%d)", #expr, cudaGetErrorString(_e),  \
+                      __FILE__, __LINE__);                                     \
+      return LA_ERR_CUDA;                                                      \
+    }                                                                          \
+  } while (0)
+
+#define LA_TRY(expr)                                                           \
+  do {                                                                         \
+    la_status _s = (expr);                                                     \
+    if (_s != LA_OK)                                                           \
+      return _s;                                                               \
+  } while (0)
+
+#define LA_CHECK_ARG(cond, msg)                                                \
+  do {                                                                         \
+    if (!(cond)) {                                                             \
+      ::la::set_error("invalid argument: %s", msg);                            \
+      return LA_ERR_INVALID_ARG;                                               \
+    }                                                                          \
+  } while (0)
+
+// Returns LA_OK if a CUDA device of compute capability 10.x is current.
+la_status require_device();
+int sm_count();
+
+// Device buffer with RAII release.
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  ~DevBuf() { release(); }
+  la_status alloc(size_t b);
+  la_status upload(const void *host, size_t b);
+  void release();
+  template <typename T> T *as() const { return static_cast<T *>(p); }
+};
+
+// ------------------------------------------------------------ host algos
+// (la_host.cpp) -- restatements of the reference's host-side steps.
+bool valid_csr(int rows, int cols, int base, const int *ai, const int *aj,
+               std::string *why);
+int topological_sort2(int uplo, int n, int base, const int *ai, const int *aj,
+                      int *iperm, int *prefix);
+void transpose(int rows, int cols, int base, const int *ai, const int *aj,
+               const double *av, int *t_ai, int *t_aj, double *t_av);
+void permute(int n, int base, const int *ai, const int *aj, const double *av,
+             const int *iperm, const int *perm, int *p_ai, int *p_aj,
+             double *p_av);
+void split_ldu(int n, int base, const int *ai, const int *aj, const double *av,
+               int *l_ai, int *l_aj, double *l_av, double *d, int *u_ai,
+               int *u_aj, double *u_av, int *lnnz, int *unnz);
+int split_triangle(int uplo, int n, int base, const int *ai, const int *aj,
+                   const double *av, int *t_ai, int *t_aj, double *t_av);
+bool icc0(int n, int base, const int *u_ai, const int *u_aj, const double *u_av,
+          double omega, double *icc_av);
+void rcm(int n, int base, const int *ai, const int *aj, int *iperm, int *perm);
+
+} // namespace la
+
+// ----------------------------------------------------------------- handles
+struct la_csr_s {
+  int n = 0, ncols = 0, nnz = 0, base = 0;
+  la_dtype dtype = LA_F64;
+  la::DevBuf ai, aj, av, av32; // av32: FP32 copy of FP64 values (optional)
+  std::vector<int> h_ai;       // host copy of the row pointers (plans)
+  const void *values(la_dtype vd) const;
+};
+
+struct la_spmv_plan_s {
+  la_csr_t A = nullptr;
+  la_spmv_kind kind = LA_SPMV_SEGSUM;
+  int ntiles = 0;
+  la::DevBuf tile_row;  // int[ntiles + 1]: row holding each tile's first nz
+  la::DevBuf head_slot; // int[ntiles]: first tile sharing this tile's row
+  la::DevBuf slot_cnt;  // int[ntiles + 1]: contributors per merge slot
+  la::DevBuf part;      // double[2 * ntiles]: head / tail partial sums
+  la::DevBuf arrive;    // unsigned[ntiles + 1]: arrival counters (self-reset)
+  // lazily built transpose for the adjoint
+  la_csr_t At = nullptr;
+  la_spmv_plan_t Atplan = nullptr;
+  // host staging for la_spmv_host
+  la::DevBuf hx, hy;
+};
+
+struct la_trsv_plan_s {
+  int n = 0, nnz = 0, levels = 0, base = 0;
+  la_uplo uplo = LA_LOWER;
+  la_dtype dtype = LA_F64;
+  bool unit = true;
+  std::vector<int> h_iperm, h_prefix;
+  // execution-ordered strict triangle: row p of the plan is original row
+  // exec_row[p]; columns keep the original numbering.
+  la::DevBuf ai, aj, av, diag, exec_row, chunk_start, err;
+  int nchunks = 0;
+  int grid = 0;
+  la::DevBuf hb, hx; // staging for the host form
+};
+
+struct la_pcg_s {
+  la_csr_t A = nullptr;
+  la_pcg_mode mode = LA_PCG_FP64;
+  int n = 0;
+  la_spmv_plan_t Ap = nullptr;
+  la_trsv_plan_t L = nullptr, U = nullptr;
+  la::DevBuf r, z, p, q, t;        // FP64 work vectors
+  la::DevBuf r32, z32, p32, q32, t32, d32; // FP32 inner vectors (mixed)
+  la::DevBuf scal, partials, ticket;
+  la::DevBuf hb, hx;
+  int dot_blocks = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};

@@ -1,0 +1,410 @@
+// la_pcg.cu -- IC(0)-preconditioned CG on one B200, FP64 and mixed.
+//
+// Reference: the reference's intended solve sequence (execs/linearSolve.cpp:
+// 118-135): an IC(0) factor U of the SPD matrix (A ~= U^T U,
+// incomplete_cholesky_k_2, mkl_wrapper/incomplete_cholesky.cpp:286-342),
+// MKL's RCI PCG (mkl_wrapper/mkl_solver.cpp:150-251) with the preconditioner
+// applied as trsv(U^T) then trsv(U) (incomplete_cholesky.cpp:21-29) and the
+// user stopping test ||A x - b|| / ||b|| < rel_tol (mkl_solver.cpp:211-225).
+// MKL is replaced by this file's loop over the library's own kernels: the
+// nnz-balanced SpMV (la_spmv.cu), the persistent level-scheduled triangular
+// solves (la_trsv.cu) and deterministic FP64 dot products below.
+//
+// Stopping: the recurrence residual is watched every iteration; once it is
+// below rtol the true residual b - A x is formed in FP64 and the solve stops
+// only if that is below rtol too (the reference's test, evaluated where it
+// can change the outcome instead of after every iteration).
+//
+// Mixed mode: FP64 iterative refinement.  r = b - A x with the FP64 matrix,
+// then an inner PCG on A d = r / ||r|| whose SpMV and triangular solves read
+// FP32 values and FP32 vectors and accumulate in FP32, with FP64 dot
+// products and scalars; x += ||r|| d in FP64.  The inner solve stops at a
+// relative residual of kInnerTol.
+
+#include "la_device.cuh"
+#include "la_internal.h"
+
+#include <cmath>
+
+namespace la {
+
+la_status spmv_launch(la_spmv_plan_t P, double alpha, const void *x,
+                      double beta, void *y, const void *yin, la_dtype vd,
+                      cudaStream_t st);
+la_status trsv_launch(la_trsv_plan_t P, const void *b, void *x,
+                      cudaStream_t st);
+la_status trsv_check(la_trsv_plan_t P, cudaStream_t st);
+la_status trsv_build(la_trsv_plan_t P, const int *ai, const int *aj,
+                     const double *av, const double *diag);
+la_status spmv_plan_build(la_spmv_plan_t P);
+
+namespace {
+
+constexpr int kDotThreads = 512;
+constexpr double kInnerTol = 1e-5;
+
+// Scalar slots in device memory.
+enum { S_RZ = 0, S_PQ, S_RR, S_ALPHA, S_BETA, S_DOT, S_COUNT };
+
+// Deterministic FP64 dot with a fused finaliser: every block writes its
+// partial sum, the last block to finish (atomic ticket after a fence) adds
+// the partials in block order and applies `op`.
+enum DotOp { OP_STORE = 0, OP_ALPHA = 1, OP_BETA = 2 };
+
+template <typename XA, typename XB>
+__global__ void __launch_bounds__(kDotThreads)
+    dot_kernel(const int n, const XA *__restrict__ a, const XB *__restrict__ b,
+               double *partials, unsigned *ticket, double *scal, const int op) {
+  __shared__ double red[kDotThreads / 32];
+  __shared__ bool last;
+  double s = 0.0;
+  for (int i = blockIdx.x * kDotThreads + threadIdx.x; i < n;
+       i += gridDim.x * kDotThreads)
+    s += double(a[i]) * double(b[i]);
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1)
+    s += __shfl_down_sync(0xffffffffu, s, d);
+  if ((threadIdx.x & 31) == 0)
+    red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < kDotThreads / 32; w++)
+      t += red[w];
+    partials[blockIdx.x] = t;
+    __threadfence();
+    last = atomicAdd(ticket, 1u) + 1u == gridDim.x;
+  }
+  __syncthreads();
+  if (!last || threadIdx.x != 0)
+    return;
+  __threadfence();
+  double t = 0.0;
+  for (int k = 0; k < (int)gridDim.x; k++)
+    t += __ldcg(partials + k);
+  *ticket = 0u;
+  scal[S_DOT] = t;
+  if (op == OP_ALPHA) { // alpha = (r, z) / (p, A p)
+    scal[S_PQ] = t;
+    scal[S_ALPHA] = scal[S_RZ] / t;
+  } else if (op == OP_BETA) { // beta = (r, z)_new / (r, z)_old
+    scal[S_BETA] = t / scal[S_RZ];
+    scal[S_RZ] = t;
+  }
+}
+
+// x += alpha p; r -= alpha q (alpha from device memory).
+template <typename X>
+__global__ void xr_update_kernel(const int n, X *x, X *r, const X *p,
+                                 const X *q, const double *scal) {
+  const double al = scal[S_ALPHA];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
+    x[i] = X(double(x[i]) + al * double(p[i]));
+    r[i] = X(double(r[i]) - al * double(q[i]));
+  }
+}
+
+// p = z + beta p
+template <typename X>
+__global__ void p_update_kernel(const int n, X *p, const X *z,
+                                const double *scal) {
+  const double be = scal[S_BETA];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x)
+    p[i] = X(double(z[i]) + be * double(p[i]));
+}
+
+// out = X(scale * in)
+template <typename XO, typename XI>
+__global__ void scale_copy_kernel(const int n, XO *out, const XI *in,
+                                  const double scale) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x)
+    out[i] = XO(scale * double(in[i]));
+}
+
+// x += scale * d
+__global__ void refine_kernel(const int n, double *x, const float *d,
+                              const double scale) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x)
+    x[i] += scale * double(d[i]);
+}
+
+__global__ void zero_kernel(const int n, double *x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x)
+    x[i] = 0.0;
+}
+
+} // namespace
+} // namespace la
+
+
+
+namespace la {
+namespace {
+
+int vec_grid(int n) { return std::max(1, std::min((n + 255) / 256, 8 * sm_count())); }
+
+template <typename XA, typename XB>
+la_status dot(la_pcg_t S, const XA *a, const XB *b, int op, cudaStream_t st) {
+  dot_kernel<XA, XB><<<S->dot_blocks, kDotThreads, 0, st>>>(
+      S->n, a, b, S->partials.as<double>(), S->ticket.as<unsigned>(),
+      S->scal.as<double>(), op);
+  LA_CUDA_TRY(cudaGetLastError());
+  return LA_OK;
+}
+
+la_status read_scalar(la_pcg_t S, int slot, double *v, cudaStream_t st) {
+  LA_CUDA_TRY(cudaMemcpyAsync(v, S->scal.as<double>() + slot, sizeof(double),
+                              cudaMemcpyDeviceToHost, st));
+  LA_CUDA_TRY(cudaStreamSynchronize(st));
+  return LA_OK;
+}
+
+// True relative residual ||b - A x|| / bnorm in FP64 (uses t).
+la_status true_residual(la_pcg_t S, const double *b, const double *x,
+                        double bnorm, double *rel, cudaStream_t st) {
+  LA_TRY(spmv_launch(S->Ap, -1.0, x, 1.0, S->t.p, b, LA_F64, st));
+  LA_TRY(dot(S, S->t.as<double>(), S->t.as<double>(), OP_STORE, st));
+  double tt;
+  LA_TRY(read_scalar(S, S_DOT, &tt, st));
+  *rel = std::sqrt(tt) / bnorm;
+  return LA_OK;
+}
+
+// One preconditioned CG run on A y = rhs from y = 0 with vectors of type X.
+// Stops when ||r|| <= tol * ||rhs|| (recurrence residual), or, when
+// `b_true` is given (FP64 mode), when additionally the true residual of y
+// against b_true is below tol.  Returns the iteration count in *iters.
+template <typename X>
+la_status pcg_run(la_pcg_t S, const X *rhs, X *y, X *r, X *z, X *p, X *q,
+                  X *t, la_dtype vd, double tol, int maxit, const double *b_true,
+                  double bnorm_true, int *iters, double *rel_out,
+                  cudaStream_t st) {
+  const int n = S->n, g = vec_grid(n);
+  *iters = 0;
+  LA_CUDA_TRY(cudaMemsetAsync(y, 0, sizeof(X) * n, st));
+  LA_CUDA_TRY(cudaMemcpyAsync(r, rhs, sizeof(X) * n, cudaMemcpyDeviceToDevice, st));
+  LA_TRY(dot(S, r, r, OP_STORE, st));
+  double rr0;
+  LA_TRY(read_scalar(S, S_DOT, &rr0, st));
+  const double r0 = std::sqrt(rr0);
+  if (r0 == 0.0) {
+    *rel_out = 0.0;
+    return LA_OK;
+  }
+  LA_TRY(trsv_launch(S->L, r, t, st));
+  LA_TRY(trsv_launch(S->U, t, z, st));
+  LA_CUDA_TRY(cudaMemcpyAsync(p, z, sizeof(X) * n, cudaMemcpyDeviceToDevice, st));
+  LA_TRY(dot(S, r, z, OP_STORE, st));
+  LA_CUDA_TRY(cudaMemcpyAsync(S->scal.as<double>() + S_RZ,
+                              S->scal.as<double>() + S_DOT, sizeof(double),
+                              cudaMemcpyDeviceToDevice, st));
+  for (int it = 1; it <= maxit; it++) {
+    LA_TRY(spmv_launch(S->Ap, 1.0, p, 0.0, q, q, vd, st));
+    LA_TRY(dot(S, p, q, OP_ALPHA, st));
+    xr_update_kernel<X><<<g, 256, 0, st>>>(n, y, r, p, q, S->scal.as<double>());
+    LA_TRY(dot(S, r, r, OP_STORE, st));
+    double rr;
+    LA_TRY(read_scalar(S, S_DOT, &rr, st));
+    *iters = it;
+    const double rel = std::sqrt(rr) / r0;
+    *rel_out = rel;
+    if (!std::isfinite(rel)) {
+      set_error("PCG breakdown: non-finite residual at iteration %d", it);
+      return LA_ERR_BREAKDOWN;
+    }
+    if (rel < tol) {
+      if (!b_true)
+        return LA_OK;
+      double trel;
+      LA_TRY(true_residual(S, b_true, (const double *)y, bnorm_true, &trel, st));
+      *rel_out = trel;
+      if (trel < tol)
+        return LA_OK;
+    }
+    LA_TRY(trsv_launch(S->L, r, t, st));
+    LA_TRY(trsv_launch(S->U, t, z, st));
+    LA_TRY(dot(S, r, z, OP_BETA, st));
+    p_update_kernel<X><<<g, 256, 0, st>>>(n, p, z, S->scal.as<double>());
+  }
+  LA_TRY(trsv_check(S->L, st));
+  LA_TRY(trsv_check(S->U, st));
+  return LA_ERR_NOT_CONVERGED;
+}
+
+} // namespace
+
+la_status pcg_create(la_csr_t A, const int *u_ai, const int *u_aj,
+                     const double *icc_av, la_pcg_mode mode, la_pcg_t *out) {
+  auto *S = new la_pcg_s();
+  S->A = A;
+  S->mode = mode;
+  const int n = S->n = A->n, base = A->base;
+  auto fail = [&](la_status s) {
+    delete S;
+    return s;
+  };
+  // Preconditioner factors: strict U + diag, and strict L = U^T (same diag).
+  const int unnz = u_ai[n] - base;
+  std::vector<int> l_ai(n + 1), l_aj(std::max(unnz, 1)), s_ai(n + 1),
+      s_aj(std::max(unnz, 1)), t_ai(n + 1), t_aj(std::max(unnz, 1));
+  std::vector<double> l_av(std::max(unnz, 1)), s_av(std::max(unnz, 1)),
+      t_av(std::max(unnz, 1)), d(n);
+  int lnnz = 0, snnz = 0;
+  split_ldu(n, base, u_ai, u_aj, icc_av, l_ai.data(), l_aj.data(), l_av.data(),
+            d.data(), s_ai.data(), s_aj.data(), s_av.data(), &lnnz, &snnz);
+  if (lnnz != 0) {
+    set_error("IC factor must be upper triangular");
+    return fail(LA_ERR_INVALID_ARG);
+  }
+  transpose(n, n, base, s_ai.data(), s_aj.data(), s_av.data(), t_ai.data(),
+            t_aj.data(), t_av.data());
+  const la_dtype fd = mode == LA_PCG_MIXED ? LA_F32 : LA_F64;
+  la_status s;
+  S->L = new la_trsv_plan_s();
+  S->L->n = n;
+  S->L->nnz = snnz;
+  S->L->base = base;
+  S->L->uplo = LA_LOWER;
+  S->L->dtype = fd;
+  S->L->unit = false;
+  if ((s = trsv_build(S->L, t_ai.data(), t_aj.data(), t_av.data(), d.data())) != LA_OK)
+    return fail(s);
+  S->U = new la_trsv_plan_s();
+  S->U->n = n;
+  S->U->nnz = snnz;
+  S->U->base = base;
+  S->U->uplo = LA_UPPER;
+  S->U->dtype = fd;
+  S->U->unit = false;
+  if ((s = trsv_build(S->U, s_ai.data(), s_aj.data(), s_av.data(), d.data())) != LA_OK)
+    return fail(s);
+  S->Ap = new la_spmv_plan_s();
+  S->Ap->A = A;
+  S->Ap->kind = LA_SPMV_SEGSUM;
+  if ((s = spmv_plan_build(S->Ap)) != LA_OK)
+    return fail(s);
+  if (mode == LA_PCG_MIXED && A->av32.p == nullptr) {
+    set_error("mixed PCG needs FP32 matrix values (create A with LA_CSR_KEEP_F32)");
+    return fail(LA_ERR_INVALID_ARG);
+  }
+  const size_t v8 = sizeof(double) * std::max(n, 1), v4 = sizeof(float) * std::max(n, 1);
+  for (DevBuf *b : {&S->r, &S->z, &S->p, &S->q, &S->t})
+    if ((s = b->alloc(v8)) != LA_OK)
+      return fail(s);
+  if (mode == LA_PCG_MIXED)
+    for (DevBuf *b : {&S->r32, &S->z32, &S->p32, &S->q32, &S->t32, &S->d32})
+      if ((s = b->alloc(v4)) != LA_OK)
+        return fail(s);
+  S->dot_blocks = std::max(1, std::min(2 * sm_count(), (n + kDotThreads - 1) / kDotThreads));
+  if ((s = S->scal.alloc(sizeof(double) * S_COUNT)) != LA_OK ||
+      (s = S->partials.alloc(sizeof(double) * S->dot_blocks)) != LA_OK ||
+      (s = S->ticket.alloc(sizeof(unsigned))) != LA_OK)
+    return fail(s);
+  if (cudaMemset(S->ticket.p, 0, sizeof(unsigned)) != cudaSuccess ||
+      cudaEventCreate(&S->ev0) != cudaSuccess || cudaEventCreate(&S->ev1) != cudaSuccess) {
+    set_error("PCG setup: CUDA error");
+    return fail(LA_ERR_CUDA);
+  }
+  *out = S;
+  return LA_OK;
+}
+
+la_status pcg_solve(la_pcg_t S, const double *b, double *x, double rtol,
+                    int maxit, la_pcg_info *info, cudaStream_t st) {
+  la_pcg_info loc{};
+  la_status res = LA_OK;
+  const int n = S->n;
+  LA_CUDA_TRY(cudaEventRecord(S->ev0, st));
+  // ||b||
+  LA_TRY(dot(S, b, b, OP_STORE, st));
+  double bb;
+  LA_TRY(read_scalar(S, S_DOT, &bb, st));
+  const double bn = std::sqrt(bb);
+  if (bn == 0.0 || n == 0) {
+    zero_kernel<<<vec_grid(n), 256, 0, st>>>(n, x);
+    loc.outer_iterations = 1;
+  } else if (S->mode == LA_PCG_FP64) {
+    res = pcg_run<double>(S, b, x, S->r.as<double>(), S->z.as<double>(),
+                          S->p.as<double>(), S->q.as<double>(), S->t.as<double>(),
+                          LA_F64, rtol, maxit, b, bn, &loc.iterations,
+                          &loc.rel_residual, st);
+    loc.outer_iterations = 1;
+  } else {
+    zero_kernel<<<vec_grid(n), 256, 0, st>>>(n, x);
+    double rel = 1.0;
+    int total = 0;
+    // r = b - A x (x = 0 -> r = b)
+    LA_CUDA_TRY(cudaMemcpyAsync(S->r.p, b, sizeof(double) * n,
+                                cudaMemcpyDeviceToDevice, st));
+    double rn = bn;
+    for (int outer = 1; outer <= 20; outer++) {
+      loc.outer_iterations = outer;
+      scale_copy_kernel<float, double><<<vec_grid(n), 256, 0, st>>>(
+          n, S->q32.as<float>(), S->r.as<double>(), 1.0 / rn);
+      int it = 0;
+      double irel = 0;
+      const la_status s = pcg_run<float>(
+          S, S->q32.as<float>(), S->d32.as<float>(), S->r32.as<float>(),
+          S->z32.as<float>(), S->p32.as<float>(), S->t32.as<float>(),
+          S->t32.as<float>() /* scratch reused below */, LA_F32, kInnerTol,
+          maxit - total, nullptr, 1.0, &it, &irel, st);
+      total += it;
+      if (s != LA_OK && s != LA_ERR_NOT_CONVERGED) {
+        res = s;
+        break;
+      }
+      refine_kernel<<<vec_grid(n), 256, 0, st>>>(n, x, S->d32.as<float>(), rn);
+      LA_TRY(spmv_launch(S->Ap, -1.0, x, 1.0, S->r.p, b, LA_F64, st));
+      LA_TRY(dot(S, S->r.as<double>(), S->r.as<double>(), OP_STORE, st));
+      double rr;
+      LA_TRY(read_scalar(S, S_DOT, &rr, st));
+      rn = std::sqrt(rr);
+      rel = rn / bn;
+      if (rel < rtol)
+        break;
+      if (total >= maxit) {
+        res = LA_ERR_NOT_CONVERGED;
+        break;
+      }
+    }
+    loc.iterations = total;
+    loc.rel_residual = rel;
+    if (res == LA_OK && rel >= rtol)
+      res = LA_ERR_NOT_CONVERGED;
+  }
+  LA_CUDA_TRY(cudaEventRecord(S->ev1, st));
+  LA_CUDA_TRY(cudaEventSynchronize(S->ev1));
+  float ms = 0;
+  LA_CUDA_TRY(cudaEventElapsedTime(&ms, S->ev0, S->ev1));
+  loc.solve_ms = ms;
+  if (res == LA_OK) {
+    LA_TRY(trsv_check(S->L, st));
+    LA_TRY(trsv_check(S->U, st));
+  }
+  if (info)
+    *info = loc;
+  if (res == LA_ERR_NOT_CONVERGED)
+    set_error("PCG did not reach rtol %.3g in %d iterations (residual %.3g)",
+              rtol, maxit, loc.rel_residual);
+  return res;
+}
+
+void pcg_destroy(la_pcg_t S) {
+  if (!S)
+    return;
+  if (S->ev0)
+    cudaEventDestroy(S->ev0);
+  if (S->ev1)
+    cudaEventDestroy(S->ev1);
+  delete S->L;
+  delete S->U;
+  delete S->Ap;
+  delete S;
+}
+
+} // namespace la

@@ -1,0 +1,193 @@
+"""GPU SpMV parity: both reference forms through the C-ABI vs the oracle.
+
+Tolerance (FP64): relative 2-norm error <= 1e-13 against the reference's
+serial result, plus an element-wise bound.  FP32
+results state their error against the FP64 oracle.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import golden_matrices
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+TOL = 1e-13
+KINDS = ("segsum", "albus")
+
+
+def kind_id(lab, k):
+    return lab.api.LA_SPMV_SEGSUM if k == "segsum" else lab.api.LA_SPMV_ALBUS
+
+
+def dev(a, dtype=torch.float64):
+    return torch.as_tensor(np.ascontiguousarray(a)).to("cuda", dtype)
+
+
+def rel(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
+
+
+def run_spmv(lab, m, n, ai, aj, av, x, y0, alpha, beta, kind, base=0):
+    A = lab.CSR(m, n, base, ai, aj, av)
+    plan = lab.SPMV(A, kind_id(lab, kind))
+    xd, yd = dev(x), dev(y0)
+    plan(xd, yd, alpha, beta)
+    torch.cuda.synchronize()
+    return yd.cpu().numpy()
+
+
+def oracle_serial(orc, m, ai, aj, av, x, y0, alpha, beta, base=0):
+    y = np.array(y0, dtype=np.float64, copy=True)
+    P = orc.ptr
+    orc.port().oracle_serial_spmv(m, base, P(ai), P(aj), P(av), P(x), P(y), alpha, beta)
+    return y
+
+
+@pytest.mark.parametrize("kind", KINDS)
+def test_spmv_golden(lab, golden, kind):
+    for name, m, n, ai, aj, av in golden_matrices(golden):
+        x, y0 = golden[f"{name}/spmv_x"], golden[f"{name}/spmv_y0"]
+        ref = golden[f"{name}/spmv_serial"]
+        y = run_spmv(lab, m, n, ai, aj, av, x, y0, 1.5, 0.5, kind)
+        assert rel(y, ref) <= TOL, (name, rel(y, ref))
+        assert np.all(np.abs(y - ref) <= 1e-12 * (np.abs(ref) + np.abs(y0) + 1)), name
+        # the reference's own test vector: b = ones, alpha 1, beta 0
+        y = run_spmv(lab, m, n, ai, aj, av, np.ones(n), np.zeros(m), 1.0, 0.0, kind)
+        assert rel(y, golden[f"{name}/spmv_ones"]) <= TOL, name
+        # the multi-threaded reference forms agree with the GPU as well
+        for T in (7, 10):
+            assert rel(run_spmv(lab, m, n, ai, aj, av, x, y0, 1.5, 0.5, kind),
+                       golden[f"{name}/spmv_{kind}_T{T}"]) <= TOL
+
+
+@pytest.mark.parametrize("kind", KINDS)
+def test_spmv_host_path_drop_in(lab, golden, kind):
+    cls = lab.SegSumSPMV if kind == "segsum" else lab.ALBUSSPMV
+    for name, m, n, ai, aj, av in golden_matrices(golden):
+        if m != n:
+            continue
+        s = cls(10)
+        s.preprocess(m, 0, ai, aj, av)
+        x = golden[f"{name}/spmv_x"]
+        y = golden[f"{name}/spmv_y0"].copy()
+        s(m, 0, ai, aj, av, x, y, 1.5, 0.5)
+        assert rel(y, golden[f"{name}/spmv_serial"]) <= TOL, name
+
+
+def _edge_matrices():
+    rng = np.random.default_rng(42)
+    out = []
+    # leading, trailing and interior empty rows, rows ending on tile edges
+    lens = [0, 0, 3, 0, 2048, 0, 0, 1, 2047, 2049, 0, 5000, 1, 0, 4096, 7, 0, 0]
+    out.append(("empty_rows_tile_edges", lens))
+    # one huge row spanning many tiles between tiny rows
+    out.append(("long_row", [1, 2, 20000, 3, 1]))
+    # a single row
+    out.append(("single_row", [9000]))
+    # many empty rows in one tile
+    out.append(("sparse_rows", [0] * 5000 + [1] + [0] * 7000 + [2] + [0] * 3))
+    mats = []
+    for name, lens in out:
+        m = len(lens)
+        ncols = 25000
+        ai = np.zeros(m + 1, np.int64)
+        np.cumsum(lens, out=ai[1:])
+        aj = np.concatenate([np.sort(rng.choice(ncols, L, replace=False)) for L in lens]
+                            if sum(lens) else [np.zeros(0, np.int64)])
+        av = rng.standard_normal(int(ai[-1]))
+        mats.append((name, m, ncols, ai.astype(np.int32), aj.astype(np.int32), av))
+    return mats
+
+
+@pytest.mark.parametrize("kind", KINDS)
+def test_spmv_edge_cases(lab, orc, kind):
+    rng = np.random.default_rng(1)
+    for name, m, n, ai, aj, av in _edge_matrices():
+        x = rng.uniform(-1, 1, n)
+        y0 = rng.uniform(-1, 1, m)
+        for alpha, beta in ((1.0, 0.0), (-2.0, 0.75), (0.5, 1.0)):
+            y = run_spmv(lab, m, n, ai, aj, av, x, y0, alpha, beta, kind)
+            ref = oracle_serial(orc, m, ai, aj, av, x, y0, alpha, beta)
+            assert rel(y, ref) <= TOL, (name, alpha, beta, rel(y, ref))
+    # nnz == 0: y = beta * y
+    ai = np.zeros(6, np.int32)
+    y = run_spmv(lab, 5, 5, ai, np.zeros(0, np.int32), np.zeros(0), np.ones(5), np.arange(5.0),
+                 2.0, 0.5, kind)
+    assert np.array_equal(y, 0.5 * np.arange(5.0))
+
+
+@pytest.mark.parametrize("kind", KINDS)
+def test_spmv_beta_zero_does_not_read_y_and_base1(lab, orc, golden, kind):
+    ai, aj, av = golden["rdist1/ai"], golden["rdist1/aj"], golden["rdist1/av"]
+    n = len(ai) - 1
+    x = golden["rdist1/spmv_x"]
+    y0 = np.full(n, np.nan)
+    y = run_spmv(lab, n, n, ai, aj, av, x, y0, 1.0, 0.0, kind)
+    assert np.all(np.isfinite(y))
+    ref = oracle_serial(orc, n, ai, aj, av, x, np.zeros(n), 1.0, 0.0)
+    assert rel(y, ref) <= TOL
+    # one-based indices give the same result
+    y1 = run_spmv(lab, n, n, ai + 1, aj + 1, av, x, np.zeros(n), 1.0, 0.0, kind, base=1)
+    assert rel(y1, ref) <= TOL
+
+
+@pytest.mark.parametrize("kind", KINDS)
+def test_spmv_deterministic(lab, golden, kind):
+    ai, aj, av = golden["powerlaw_3000/ai"], golden["powerlaw_3000/aj"], golden["powerlaw_3000/av"]
+    n = len(ai) - 1
+    A = lab.CSR(n, n, 0, ai, aj, av)
+    plan = lab.SPMV(A, kind_id(lab, kind))
+    xd = dev(golden["powerlaw_3000/spmv_x"])
+    outs = []
+    for _ in range(5):
+        yd = dev(golden["powerlaw_3000/spmv_y0"])
+        plan(xd, yd, 1.5, 0.5)
+        outs.append(yd.cpu().numpy())
+    assert all(np.array_equal(outs[0], o) for o in outs[1:])
+
+
+def test_spmv_full_size_configs(lab, orc):
+    """C1 (2D Laplacian 512^2), C3 (3D Laplacian 128^3) and C2 (power law,
+    4M rows) at full size, FP64 both forms vs the oracle; FP32 error stated."""
+    from linearalgebra_b200 import gen
+    for label, (n, ai, aj, av) in (("C1", gen.laplacian_2d(512)), ("C3", gen.laplacian_3d(128)),
+                                   ("C2", gen.powerlaw(4_000_000, seed=0))):
+        x = gen.uniform_vector(n, 0)
+        ref = oracle_serial(orc, n, ai, aj, av, x, np.zeros(n), 1.0, 0.0)
+        A = lab.CSR(n, n, 0, ai, aj, av, keep_f32=True)
+        for kind in KINDS:
+            plan = lab.SPMV(A, kind_id(lab, kind))
+            yd = torch.empty(n, dtype=torch.float64, device="cuda")
+            plan(dev(x), yd, 1.0, 0.0)
+            e = rel(yd.cpu().numpy(), ref)
+            assert e <= TOL, (label, kind, e)
+            y32 = torch.empty(n, dtype=torch.float32, device="cuda")
+            plan(dev(x, torch.float32), y32, 1.0, 0.0)
+            e32 = rel(y32.double().cpu().numpy(), ref)
+            print(f"{label} {kind}: fp64 rel err {e:.2e}; fp32 (values+vectors) rel err {e32:.2e}")
+            assert e32 <= 1e-5, (label, kind, e32)
+
+
+def test_spmv_adjoints(lab, orc, golden):
+    """dL/dx = A^T g and dL/dvalues = g_i x_j, against the oracle."""
+    P = orc.ptr
+    for name, m, n, ai, aj, av in golden_matrices(golden):
+        rng = np.random.default_rng(3)
+        g = rng.standard_normal(m)
+        x = rng.standard_normal(n)
+        out0 = rng.standard_normal(n)
+        A = lab.CSR(m, n, 0, ai, aj, av)
+        plan = lab.SPMV(A)
+        od = dev(out0)
+        plan.transpose(dev(g), od, 0.75, 0.5)
+        ref = out0.copy()
+        orc.port().oracle_spmv_transpose(m, n, 0, P(ai), P(aj), P(av), P(g), P(ref), 0.75, 0.5)
+        assert rel(od.cpu().numpy(), ref) <= TOL, name
+        dv = torch.empty(len(aj), dtype=torch.float64, device="cuda")
+        plan.sddmm(dev(g), dev(x), dv, -1.25)
+        ref = np.empty(len(aj))
+        orc.port().oracle_sddmm_pattern(m, 0, P(ai), P(aj), P(g), P(x), P(ref), -1.25)
+        assert np.array_equal(dv.cpu().numpy(), ref), name

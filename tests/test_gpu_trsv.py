@@ -1,0 +1,134 @@
+"""GPU level-scheduled triangular solves vs the oracle and the reference.
+
+Level sets must match TopologicalSort2 bit-exactly; FP64 solutions agree
+with the reference's OptimizedTriangularSolve<Barrier> to <= 1e-13
+relative 2-norm; the FP32 plan states its error against the FP64 oracle.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import golden_matrices, strict_triangle
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+TOL = 1e-13
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def dev(a, dtype=torch.float64):
+    return torch.as_tensor(np.ascontiguousarray(a)).to("cuda", dtype)
+
+
+def solve(lab, uplo, n, t_ai, t_aj, t_av, diag, b, dtype=np.float64):
+    ts = lab.OptimizedTriangularSolve(uplo, 5, dtype=dtype).analysis(n, 0, t_ai, t_aj, t_av, diag)
+    tdt = torch.float64 if dtype == np.float64 else torch.float32
+    x = torch.empty(n, dtype=tdt, device="cuda")
+    ts(dev(b, tdt), x)
+    return ts, x.double().cpu().numpy()
+
+
+def test_trsv_golden_and_levels(lab, golden):
+    checked = 0
+    for name, m, n, ai, aj, av in golden_matrices(golden):
+        if f"{name}/fwd_unit" not in golden:
+            continue
+        l_ai, l_aj, l_av = strict_triangle(n, ai, aj, av, True)
+        ts, x = solve(lab, "L", n, l_ai, l_aj, l_av, None, np.ones(n))
+        assert rel(x, golden[f"{name}/fwd_unit"]) <= TOL, name
+        lv, ip, pf = ts.levels()
+        assert lv == int(golden[f"{name}/topoL_levels"][0])
+        assert np.array_equal(ip, golden[f"{name}/topoL_iperm"])
+        assert np.array_equal(pf, golden[f"{name}/topoL_prefix"])
+        if f"{name}/bwd_diag" in golden:
+            u_ai, u_aj, u_av = strict_triangle(n, ai, aj, av, False)
+            ts, x = solve(lab, "U", n, u_ai, u_aj, u_av, golden[f"{name}/ldu_D"], np.ones(n))
+            assert rel(x, golden[f"{name}/bwd_diag"]) <= TOL, name
+            lv, ip, pf = ts.levels()
+            assert np.array_equal(ip, golden[f"{name}/topoU_iperm"])
+        checked += 1
+    assert checked >= 8
+
+
+def _ic_factor_rcm(lab, n, ai, aj, av):
+    """RCM-permute, IC(0)-factor; returns B (permuted A) and strict L=U^T,
+    strict U, diag as the PCG preconditioner uses them."""
+    from linearalgebra_b200 import gen
+    iperm, perm = lab.SerialCM(n, 0, ai, aj)
+    b_ai, b_aj, b_av = lab.Permute(n, 0, ai, aj, av, iperm, perm)
+    ua, uj, uv = gen.upper_with_diag(n, b_ai, b_aj, b_av)
+    f = lab.ICCLevelNumeric0(n, 0, ua, uj, uv)
+    _, d, (s_ai, s_aj, s_av) = lab.SplitLDU(n, 0, ua, uj, f)
+    t_ai, t_aj, t_av = lab.Transpose(n, n, 0, s_ai, s_aj, s_av)
+    return (b_ai, b_aj, b_av), (t_ai, t_aj, t_av), (s_ai, s_aj, s_av), d
+
+
+def test_trsv_ic_factors_rcm(lab, orc):
+    from linearalgebra_b200 import gen
+    P = orc.ptr
+    for n, ai, aj, av in (gen.laplacian_3d(32), gen.stencil27(20), gen.aniso7(24, seed=1)):
+        _, (t_ai, t_aj, t_av), (s_ai, s_aj, s_av), d = _ic_factor_rcm(lab, n, ai, aj, av)
+        b = np.random.default_rng(0).uniform(-1, 1, n)
+        for uplo, (c_ai, c_aj, c_av) in (("L", (t_ai, t_aj, t_av)), ("U", (s_ai, s_aj, s_av))):
+            ts, x = solve(lab, uplo, n, c_ai, c_aj, c_av, d, b)
+            lv, ip, pf = ts.levels()
+            ref = np.zeros(n)
+            orc.port().oracle_level_solve(lv, P(ip), P(pf), 0, P(c_ai), P(c_aj), P(c_av), P(d),
+                                          P(b), P(ref))
+            assert rel(x, ref) <= TOL, (n, uplo, rel(x, ref))
+            if uplo == "L":
+                ser = np.zeros(n)
+                orc.port().oracle_forward_substitution_diag(n, 0, P(c_ai), P(c_aj), P(c_av), P(d),
+                                                            P(b), P(ser))
+            else:
+                ser = np.zeros(n)
+                orc.port().oracle_backward_substitution(n, 0, P(c_ai), P(c_aj), P(c_av), P(d),
+                                                        P(b), P(ser))
+            assert rel(x, ser) <= TOL
+            _, x32 = solve(lab, uplo, n, c_ai, c_aj, c_av, d, b, dtype=np.float32)
+            e32 = rel(x32, ref)
+            print(f"n={n} {uplo}: fp64 err {rel(x, ref):.2e}, fp32 err {e32:.2e}, levels {lv}")
+            assert e32 <= 1e-4
+
+
+def test_trsv_repeated_and_reference_levels_3d(lab, orc):
+    """128^3 Laplacian under RCM keeps 3(g-1)+1 = 382 levels; repeated solves
+    are identical (tests/triangular_solve_test.cpp repeats 100 times)."""
+    from linearalgebra_b200 import gen
+    n, ai, aj, av = gen.laplacian_3d(128)
+    _, (t_ai, t_aj, t_av), _, d = _ic_factor_rcm(lab, n, ai, aj, av)
+    ts = lab.OptimizedTriangularSolve("L").analysis(n, 0, t_ai, t_aj, t_av, d)
+    lv, ip, pf = ts.levels()
+    assert lv == 382
+    rf = orc.ref()
+    if rf is not None:
+        P = orc.ptr
+        ip2, pf2 = np.empty(n, np.int32), np.empty(n + 1, np.int32)
+        assert rf.la_ref_topological_sort2(0, n, 0, P(t_ai), P(t_aj), P(ip2), P(pf2)) == 382
+        assert np.array_equal(ip, ip2) and np.array_equal(pf, pf2[:383])
+    b = dev(np.random.default_rng(5).uniform(-1, 1, n))
+    x = torch.empty(n, dtype=torch.float64, device="cuda")
+    ts(b, x)
+    first = x.clone()
+    for _ in range(20):
+        ts(b, x)
+    assert torch.equal(first, x)
+    ref = np.zeros(n)
+    P = orc.ptr
+    orc.port().oracle_level_solve(lv, P(ip), P(pf), 0, P(t_ai), P(t_aj), P(t_av), P(d),
+                                  P(b.cpu().numpy()), P(ref))
+    assert rel(x.cpu().numpy(), ref) <= TOL
+
+
+def test_trsv_host_path(lab, golden):
+    ai, aj, av = golden["lap2d_32/ai"], golden["lap2d_32/aj"], golden["lap2d_32/av"]
+    n = len(ai) - 1
+    l_ai, l_aj, l_av = strict_triangle(n, ai, aj, av, True)
+    ts = lab.OptimizedTriangularSolve("L").analysis(n, 0, l_ai, l_aj, l_av)
+    x = np.zeros(n)
+    ts(np.ones(n), x)
+    assert rel(x, golden["lap2d_32/fwd_unit"]) <= TOL
