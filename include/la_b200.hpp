@@ -1,0 +1,189 @@
+// la_b200.hpp -- header-only C++ drop-in for the reference's hot-path API.
+//
+// Same class and function names, template parameters and call signatures
+// as the reference's sparse_mat_op/ headers, in namespace
+// matrix_utils::b200, forwarding to the C-ABI in la_b200.h (the GPU does
+// the work).  A caller switches by replacing
+//     matrix_utils::SegSumSPMV<int, int, double>
+// with
+//     matrix_utils::b200::SegSumSPMV<int, int, double>
+// (and likewise ALBUSSPMV, SPMV, OptimizedTriangularSolve,
+// TopologicalSort2).  Only the <int, int, double> instantiation exists, as
+// in the reference (triangle_solve.cpp:3-44, precond.cpp:4-27).
+//
+// Semantics kept: preprocess()/analysis() run once per matrix and the matrix
+// must not change afterwards (the reference's preprocessed state assumes the
+// same); operator() is const but uses the object's device scratch, so one
+// object must not be called from two threads at once.  Differences: b and x
+// are host arrays here as in the reference, and each call copies b in and x
+// out (use the C-ABI device-pointer entry points to keep vectors resident);
+// when beta == 0, x is not read.  Errors throw matrix_utils::b200::Error.
+#pragma once
+
+#include "la_b200.h"
+
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+namespace matrix_utils {
+namespace b200 {
+
+struct Error : std::runtime_error {
+  la_status status;
+  Error(la_status s, const std::string &what)
+      : std::runtime_error(what + ": " + la_last_error_string()), status(s) {}
+};
+
+inline void check(la_status s, const char *what) {
+  if (s != LA_OK)
+    throw Error(s, what);
+}
+
+template <typename R, typename C, typename V> constexpr void require_int_double() {
+  static_assert(std::is_same_v<R, int> && std::is_same_v<C, int> &&
+                    std::is_same_v<V, double>,
+                "only the <int, int, double> instantiation is provided, as in "
+                "the reference");
+}
+
+// SegSumSPMV (spmv.hpp:59-185) / ALBUSSPMV (spmv.hpp:186-300).
+template <la_spmv_kind KIND, typename ROWTYPE = int, typename COLTYPE = int,
+          typename VALTYPE = double>
+class SpmvGpu {
+public:
+  explicit SpmvGpu(const int num_threads = 1) : _nthreads{num_threads} {
+    require_int_double<ROWTYPE, COLTYPE, VALTYPE>();
+  }
+  ~SpmvGpu() { release(); }
+  SpmvGpu(const SpmvGpu &) = delete;
+  SpmvGpu &operator=(const SpmvGpu &) = delete;
+
+  void setNumThreads(const int num_threads) { _nthreads = num_threads; }
+
+  void preprocess(const COLTYPE size, const int base, ROWTYPE const *ai,
+                  COLTYPE const *aj, VALTYPE const *av) {
+    release();
+    COLTYPE ncols = size;
+    for (ROWTYPE k = 0; k < ai[size] - base; k++)
+      ncols = aj[k] - base + 1 > ncols ? aj[k] - base + 1 : ncols;
+    check(la_csr_create(size, ncols, base, ai, aj, av, LA_F64, 0, &_A),
+          "la_csr_create");
+    check(la_spmv_plan_create(_A, KIND, &_plan), "la_spmv_plan_create");
+    _size = size;
+  }
+
+  // x = alpha * A * b + beta * x
+  void operator()(const COLTYPE size, const int base, ROWTYPE const *ai,
+                  COLTYPE const *aj, VALTYPE const *av, const VALTYPE *const b,
+                  VALTYPE *const x, const VALTYPE alpha,
+                  const VALTYPE beta) const {
+    if (!_plan || size != _size)
+      const_cast<SpmvGpu *>(this)->preprocess(size, base, ai, aj, av);
+    check(la_spmv_host(_plan, alpha, b, beta, x), "la_spmv_host");
+  }
+
+  int get_num_threads() const { return _nthreads; }
+
+private:
+  void release() {
+    if (_plan)
+      la_spmv_plan_destroy(_plan);
+    if (_A)
+      la_csr_destroy(_A);
+    _plan = nullptr;
+    _A = nullptr;
+  }
+  int _nthreads;
+  COLTYPE _size{-1};
+  la_csr_t _A{nullptr};
+  la_spmv_plan_t _plan{nullptr};
+};
+
+template <typename R = int, typename C = int, typename V = double>
+using SegSumSPMV = SpmvGpu<LA_SPMV_SEGSUM, R, C, V>;
+template <typename R = int, typename C = int, typename V = double>
+using ALBUSSPMV = SpmvGpu<LA_SPMV_ALBUS, R, C, V>;
+
+// SPMV<CSRMatrixType, SPMVType> adapter (spmv.hpp:310-334).
+template <typename CSRMatrixType, typename SPMVType> struct SPMV {
+  using ROWTYPE = typename CSRMatrixType::ROWTYPE;
+  using COLTYPE = typename CSRMatrixType::COLTYPE;
+  using VALTYPE = typename CSRMatrixType::VALTYPE;
+
+  SPMV() : _matrix{nullptr} {}
+  void setMatrix(CSRMatrixType const *matrix) { _matrix = matrix; }
+  void preprocess() {
+    _spmv.preprocess(_matrix->rows, _matrix->Base(), _matrix->AI(),
+                     _matrix->AJ(), _matrix->AV());
+  }
+  void operator()(const VALTYPE *const b, VALTYPE *const x,
+                  const VALTYPE alpha = 1., const VALTYPE beta = 0.) const {
+    _spmv(_matrix->rows, _matrix->Base(), _matrix->AI(), _matrix->AJ(),
+          _matrix->AV(), b, x, alpha, beta);
+  }
+  CSRMatrixType const *_matrix;
+  SPMVType _spmv;
+};
+
+enum TriangularMatrix { L = 0, U = 1 };
+enum class FBSubstitutionType { Barrier, NoBarrier, NoBarrierSuperNode };
+
+// OptimizedTriangularSolve (triangle_solve.hpp:149-208).  Every FBST maps to
+// the one GPU schedule (persistent kernel, per-row readiness).
+template <FBSubstitutionType FBST = FBSubstitutionType::Barrier,
+          TriangularMatrix TS = TriangularMatrix::L, typename ROWTYPE = int,
+          typename COLTYPE = int, typename VALTYPE = double>
+class OptimizedTriangularSolve {
+public:
+  explicit OptimizedTriangularSolve(const int num_threads = 1)
+      : _nthreads{num_threads} {
+    require_int_double<ROWTYPE, COLTYPE, VALTYPE>();
+  }
+  ~OptimizedTriangularSolve() {
+    if (_plan)
+      la_trsv_plan_destroy(_plan);
+  }
+  OptimizedTriangularSolve(const OptimizedTriangularSolve &) = delete;
+  OptimizedTriangularSolve &operator=(const OptimizedTriangularSolve &) = delete;
+
+  void analysis(const COLTYPE rows, const int base, ROWTYPE const *ai,
+                COLTYPE const *aj, VALTYPE const *av,
+                VALTYPE const *diag = nullptr) {
+    if (_plan)
+      la_trsv_plan_destroy(_plan);
+    _plan = nullptr;
+    check(la_trsv_analysis(TS == L ? LA_LOWER : LA_UPPER, rows, base, ai, aj,
+                           av, diag, LA_F64, &_plan),
+          "la_trsv_analysis");
+  }
+
+  void operator()(const VALTYPE *const b, VALTYPE *const x) const {
+    check(la_trsv_host(_plan, b, x), "la_trsv_host");
+  }
+
+  int get_num_threads() const { return _nthreads; }
+
+private:
+  int _nthreads;
+  la_trsv_plan_t _plan{nullptr};
+};
+
+// TopologicalSort2<TS> (matrix_utils.hpp:637-675), bit-identical output.
+template <TriangularMatrix TS = L, typename ROWTYPE, typename COLTYPE,
+          typename VEC>
+COLTYPE TopologicalSort2(const COLTYPE nodes, const int base, ROWTYPE const *ai,
+                         COLTYPE const *aj, VEC &iperm, VEC &prefix) {
+  iperm.resize(nodes);
+  prefix.resize(nodes + 1);
+  int levels = 0;
+  check(la_topological_sort2(TS == L ? LA_LOWER : LA_UPPER, nodes, base, ai,
+                             aj, iperm.data(), prefix.data(), &levels),
+        "la_topological_sort2");
+  prefix.resize(levels + 1);
+  return levels;
+}
+
+} // namespace b200
+} // namespace matrix_utils

@@ -66,11 +66,13 @@ int sm_count() {
   return sms > 0 ? sms : 1;
 }
 
+// Every device buffer is allocated kPad bytes longer than asked, so that
+// 16-byte-granular bulk copies of a ragged tail never leave the allocation.
+constexpr size_t kPad = 64;
+
 la_status DevBuf::alloc(size_t b) {
   release();
-  if (b == 0)
-    b = 16;
-  cudaError_t e = cudaMalloc(&p, b);
+  cudaError_t e = cudaMalloc(&p, b + kPad);
   if (e != cudaSuccess) {
     p = nullptr;
     set_error("cudaMalloc(%zu) failed: %s", b, cudaGetErrorString(e));

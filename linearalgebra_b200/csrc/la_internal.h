@@ -94,11 +94,8 @@ struct la_spmv_plan_s {
   la_csr_t A = nullptr;
   la_spmv_kind kind = LA_SPMV_SEGSUM;
   int ntiles = 0;
-  la::DevBuf tile_row;  // int[ntiles + 1]: row holding each tile's first nz
-  la::DevBuf head_slot; // int[ntiles]: first tile sharing this tile's row
-  la::DevBuf slot_cnt;  // int[ntiles + 1]: contributors per merge slot
-  la::DevBuf part;      // double[2 * ntiles]: head / tail partial sums
-  la::DevBuf arrive;    // unsigned[ntiles + 1]: arrival counters (self-reset)
+  la::DevBuf tile_row; // int[ntiles + 1]: row holding each tile's first nz
+  la::DevBuf part;     // double[2 * ntiles]: head / tail partial sums
   // lazily built transpose for the adjoint
   la_csr_t At = nullptr;
   la_spmv_plan_t Atplan = nullptr;
@@ -114,7 +111,7 @@ struct la_trsv_plan_s {
   std::vector<int> h_iperm, h_prefix;
   // execution-ordered strict triangle: row p of the plan is original row
   // exec_row[p]; columns keep the original numbering.
-  la::DevBuf ai, aj, av, diag, exec_row, chunk_start, err;
+  la::DevBuf ai, aj, av, diag, exec_row, chunk_start, err, ticket;
   int nchunks = 0;
   int grid = 0;
   la::DevBuf hb, hx; // staging for the host form

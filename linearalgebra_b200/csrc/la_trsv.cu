@@ -11,17 +11,17 @@
 //
 // B200 design.  The same host analysis (bit-identical level sets) stores
 // the rows in level order and cuts every level into 32-row chunks, so a
-// chunk never straddles a level.  One cooperative launch keeps every warp
-// resident; warp w takes chunks w, w + W, ... in order, one lane per row.
-// Instead of a grid barrier per level, each lane waits only for the x
+// chunk never straddles a level.  One launch of a persistent grid walks all
+// levels: warps claim chunks in order from an atomic ticket, one lane per
+// row.  Instead of a grid barrier per level, each lane waits only for the x
 // entries its row reads: x is pre-filled with a sentinel NaN bit pattern and
 // a finished row publishes x[i] with a device-scope store, so a dependency
 // is ready when its x entry stops being the sentinel (the value is its own
-// flag; one L2 round trip).  Chunks are taken in level order, so the lowest
-// unfinished chunk always has its inputs ready: the solve cannot deadlock
-// while all warps are resident, which the cooperative launch guarantees.
-// Every wait is bounded by the global timer; on expiry the kernel records a
-// timeout in the plan's error word and all warps leave.
+// flag; one L2 round trip).  Because chunks are claimed in level order, the
+// lowest unfinished chunk always has its inputs ready and the solve cannot
+// deadlock.  Waiting lanes back off with nanosleep; every wait is bounded by
+// the global timer, and on expiry the kernel records a timeout in the plan's
+// error word and all warps leave.
 //
 // Roofline: latency-bound at these sizes (one dependent L2 round trip per
 // level); algorithmic bytes per solve
@@ -32,6 +32,7 @@
 #include "la_internal.h"
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 
 namespace la {
@@ -39,6 +40,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kChunk = 32;
+constexpr int kDeps = 8; // dependency loads issued together per row
 constexpr unsigned long long kWaitNs = 1000000000ull; // 1 s per wait
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -67,47 +69,117 @@ template <> struct Sentinel<float> {
   }
 };
 
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double div_rn(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
+
+// Warps claim 32-row chunks in level order from an atomic ticket, one lane
+// per row.  A chunk is claimed only after every earlier chunk has been
+// claimed by a running warp, so the lowest unfinished chunk always has its
+// inputs ready and the solve cannot deadlock, whatever the grid size.
+//
+// Each lane runs its row as a small state machine inside a warp-uniform
+// loop, so a row is published the moment its own inputs are present rather
+// than when the slowest lane of the warp is done: dependencies are read
+// kDeps at a time (all loads issued before any is checked, so a level costs
+// one L2 round trip), still-missing ones are re-polled each pass, and the
+// sum is formed in stored column order with exact (never fused) operations,
+// so each x_i is bit-identical to the reference's
+//   x[idx] = diag ? (b[idx] - val) / diag[idx] : b[idx] - val.
 template <typename V, typename X, bool UNIT>
 __global__ void __launch_bounds__(kThreads)
     trsv_level_kernel(const int nchunks, const int *__restrict__ chunk_start,
                       const int *__restrict__ ai, const int *__restrict__ aj,
                       const V *__restrict__ av, const V *__restrict__ diag,
                       const int *__restrict__ exec_row,
-                      const X *__restrict__ b, X *x, const int base, int *err) {
+                      const X *__restrict__ b, X *x, const int base, int *err,
+                      int *ticket) {
   const int lane = threadIdx.x & 31;
-  const int warp = (blockIdx.x * kThreads + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * kThreads) >> 5;
-  for (int c = warp; c < nchunks; c += nwarps) {
+  for (;;) {
+    int c = 0;
+    if (lane == 0)
+      c = atomicAdd(ticket, 1);
+    c = __shfl_sync(0xffffffffu, c, 0);
+    if (c >= nchunks)
+      return;
     const int p = __ldg(chunk_start + c) + lane;
-    if (p >= __ldg(chunk_start + c + 1))
-      continue;
-    const int i = __ldg(exec_row + p);
+    bool done = p >= __ldg(chunk_start + c + 1);
+    int i = 0, k0 = 0, ke = 0;
+    unsigned pend = 0;
+    int jj[kDeps];
+    X a[kDeps], xv[kDeps];
     X sum = X(0);
-    const int ke = __ldg(ai + p + 1) - base;
-    for (int k = __ldg(ai + p) - base; k < ke; k++) {
-      const int j = __ldg(aj + k) - base;
-      X xv = dev::ld_relaxed(x + j);
-      if (Sentinel<X>::is(xv)) {
-        const unsigned long long t0 = global_ns();
-        unsigned polls = 0;
-        do {
-          if ((++polls & 63u) == 0u) {
-            if (dev::ld_relaxed(err) != 0)
-              return;
-            if (global_ns() - t0 > kWaitNs) {
-              atomicExch(err, 1);
-              return;
-            }
-          }
-          xv = dev::ld_relaxed(x + j);
-        } while (Sentinel<X>::is(xv));
-      }
-      sum += X(__ldg(av + k)) * xv;
+    // load the dependency group starting at k0; returns the missing mask
+    auto load_group = [&]() {
+      unsigned m = 0;
+#pragma unroll
+      for (int q = 0; q < kDeps; q++)
+        if (k0 + q < ke) {
+          jj[q] = __ldg(aj + k0 + q) - base;
+          a[q] = X(__ldg(av + k0 + q));
+        }
+#pragma unroll
+      for (int q = 0; q < kDeps; q++)
+        if (k0 + q < ke) {
+          xv[q] = dev::ld_relaxed(x + jj[q]);
+          if (Sentinel<X>::is(xv[q]))
+            m |= 1u << q;
+        }
+      return m;
+    };
+    if (!done) {
+      i = __ldg(exec_row + p);
+      k0 = __ldg(ai + p) - base;
+      ke = __ldg(ai + p + 1) - base;
+      pend = load_group();
     }
-    X xi = __ldg(b + i) - sum;
-    if (!UNIT)
-      xi = xi / X(__ldg(diag + p));
-    dev::st_relaxed(x + i, Sentinel<X>::scrub(xi));
+    const unsigned long long t0 = global_ns();
+    for (unsigned pass = 1;; pass++) {
+      if (!done) {
+        if (pend) {
+#pragma unroll
+          for (int q = 0; q < kDeps; q++)
+            if (pend & (1u << q)) {
+              xv[q] = dev::ld_relaxed(x + jj[q]);
+              if (!Sentinel<X>::is(xv[q]))
+                pend &= ~(1u << q);
+            }
+        }
+        if (!pend) {
+#pragma unroll
+          for (int q = 0; q < kDeps; q++)
+            if (k0 + q < ke)
+              sum = add_rn(sum, mul_rn(a[q], xv[q]));
+          k0 += kDeps;
+          if (k0 < ke) {
+            pend = load_group();
+          } else {
+            X xi = sub_rn(__ldg(b + i), sum);
+            if (!UNIT)
+              xi = div_rn(xi, X(__ldg(diag + p)));
+            dev::st_relaxed(x + i, Sentinel<X>::scrub(xi));
+            done = true;
+          }
+        }
+      }
+      if (__all_sync(0xffffffffu, done))
+        break;
+      bool abort = false;
+      if ((pass & 31u) == 0u && lane == 0)
+        abort = dev::ld_relaxed(err) != 0 || global_ns() - t0 > kWaitNs;
+      if (__shfl_sync(0xffffffffu, abort, 0)) {
+        if (lane == 0)
+          atomicExch(err, 1);
+        return;
+      }
+      if (!done && pend)
+        __nanosleep(32);
+    }
   }
 }
 
@@ -116,28 +188,38 @@ la_status launch_typed(la_trsv_plan_t P, const X *b, X *x, cudaStream_t st) {
   if (P->n == 0)
     return LA_OK;
   LA_CUDA_TRY(cudaMemsetAsync(x, 0xff, sizeof(X) * (size_t)P->n, st));
+  LA_CUDA_TRY(cudaMemsetAsync(P->ticket.p, 0, sizeof(int), st));
   const int *cs = P->chunk_start.as<int>(), *ai = P->ai.as<int>(),
             *aj = P->aj.as<int>(), *er = P->exec_row.as<int>();
   const V *av = P->av.as<V>(), *dg = P->diag.as<V>();
-  int *err = P->err.as<int>();
-  int nchunks = P->nchunks, base = P->base;
-  void *args[] = {&nchunks, &cs, &ai, &aj, &av, &dg, &er, &b, &x, &base, &err};
-  const void *fn = P->unit ? (const void *)trsv_level_kernel<V, X, true>
-                           : (const void *)trsv_level_kernel<V, X, false>;
-  LA_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(P->grid), dim3(kThreads),
-                                          args, 0, st));
+  if (P->unit)
+    trsv_level_kernel<V, X, true><<<P->grid, kThreads, 0, st>>>(
+        P->nchunks, cs, ai, aj, av, dg, er, b, x, P->base, P->err.as<int>(),
+        P->ticket.as<int>());
+  else
+    trsv_level_kernel<V, X, false><<<P->grid, kThreads, 0, st>>>(
+        P->nchunks, cs, ai, aj, av, dg, er, b, x, P->base, P->err.as<int>(),
+        P->ticket.as<int>());
+  LA_CUDA_TRY(cudaGetLastError());
   return LA_OK;
 }
 
-template <typename V, typename X> int grid_for() {
-  int per_sm = 0;
+// Persistent grid: a few CTAs per SM (LA_TRSV_CTAS_PER_SM overrides the
+// default of 2), capped by occupancy and by the number of chunks.  More
+// warps than the widest levels can use only add polling traffic.
+template <typename V, typename X> int grid_for(int nchunks) {
+  int per_sm = 0, per_sm_u = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(
       &per_sm, trsv_level_kernel<V, X, false>, kThreads, 0);
-  int per_sm_u = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(
       &per_sm_u, trsv_level_kernel<V, X, true>, kThreads, 0);
-  per_sm = std::min(per_sm, per_sm_u);
-  return std::max(1, per_sm) * sm_count();
+  int want = 2;
+  if (const char *e = std::getenv("LA_TRSV_CTAS_PER_SM"))
+    want = std::max(1, std::atoi(e));
+  const int fit = std::max(1, std::min(per_sm, per_sm_u));
+  const int g = std::min(want, fit) * sm_count();
+  const int need = (nchunks + kThreads / 32 - 1) / (kThreads / 32);
+  return std::max(1, std::min(g, need));
 }
 
 } // namespace
@@ -190,15 +272,16 @@ la_status trsv_build(la_trsv_plan_t P, const int *ai, const int *aj,
   if (P->dtype == LA_F64) {
     LA_TRY(P->av.upload(eav.data(), sizeof(double) * eav.size()));
     LA_TRY(P->diag.upload(ediag.data(), sizeof(double) * n));
-    P->grid = grid_for<double, double>();
+    P->grid = grid_for<double, double>(P->nchunks);
   } else {
     std::vector<float> f(eav.begin(), eav.end()), fd(ediag.begin(), ediag.end());
     LA_TRY(P->av.upload(f.data(), sizeof(float) * f.size()));
     LA_TRY(P->diag.upload(fd.data(), sizeof(float) * n));
-    P->grid = grid_for<float, float>();
+    P->grid = grid_for<float, float>(P->nchunks);
   }
   LA_TRY(P->err.alloc(sizeof(int)));
   LA_CUDA_TRY(cudaMemset(P->err.p, 0, sizeof(int)));
+  LA_TRY(P->ticket.alloc(sizeof(int)));
   return LA_OK;
 }
 

@@ -27,6 +27,8 @@ _PORT_SIGS = {
     "oracle_serial_spmv": ([I, I, P, P, P, P, P, D, D], None),
     "oracle_segsum_spmv": ([I, I, I, P, P, P, P, P, D, D], None),
     "oracle_albus_spmv": ([I, I, I, P, P, P, P, P, D, D], None),
+    "oracle_segsum_spmv_tiled": ([I, I, I, P, P, P, P, P, D, D], None),
+    "oracle_albus_spmv_tiled": ([I, I, I, P, P, P, P, P, D, D], None),
     "oracle_spmv_transpose": ([I, I, I, P, P, P, P, P, D, D], None),
     "oracle_sddmm_pattern": ([I, I, P, P, P, P, P, D], None),
     "oracle_forward_substitution": ([I, I, P, P, P, P, P], None),

@@ -55,9 +55,10 @@ void oracle_serial_spmv(int n, int base, const int *ai, const int *aj,
  * phase 5 writes x[i] = product[last nz of row i] + beta * x[i].
  * Unlike the reference (spmv.hpp:95 writes flag index nnz for trailing
  * empty rows, one past its buffer), the flag array here has nnz + 1 bytes. */
-void oracle_segsum_spmv(int T, int n, int base, const int *ai, const int *aj,
-                        const double *av, const double *b, double *x,
-                        double alpha, double beta) {
+static void segsum_core(int T, const long *pre, int n, int base,
+                        const int *ai, const int *aj, const double *av,
+                        const double *b, double *x, double alpha,
+                        double beta) {
   const long nnz = (long)ai[n] - base;
   unsigned char *bv = calloc((size_t)nnz + 1, 1);
   double *prod = malloc(sizeof(double) * (size_t)(nnz > 0 ? nnz : 1));
@@ -66,8 +67,7 @@ void oracle_segsum_spmv(int T, int n, int base, const int *ai, const int *aj,
   for (int i = 0; i < n; i++)
     bv[ai[i] - base] = 1;
   for (int t = 0; t < T; t++) {
-    long s, e;
-    balanced_range(nnz, t, T, &s, &e);
+    const long s = pre[t], e = pre[t + 1];
     for (long i = s; i < e; i++) {
       prod[i] = alpha * av[i] * b[aj[i] - base];
       if (i > s && !bv[i]) {
@@ -91,8 +91,7 @@ void oracle_segsum_spmv(int T, int n, int base, const int *ai, const int *aj,
     }
   }
   for (int t = 0; t < T; t++) {
-    long s, e;
-    balanced_range(nnz, t, T, &s, &e);
+    const long s = pre[t], e = pre[t + 1];
     for (long i = s; i < e; i++) {
       if (bv[i])
         break;
@@ -109,6 +108,45 @@ void oracle_segsum_spmv(int T, int n, int base, const int *ai, const int *aj,
   free(prod);
   free(tbv);
   free(tprod);
+}
+
+/* Chunk prefixes: the reference's balanced split of nnz over T workers
+ * (utils.h:176-185, spmv.hpp:99 and :202-208), or fixed chunks of `tile`
+ * nonzeros (the GPU tiles), T = ceil(nnz / tile). */
+static long *balanced_prefix(long nnz, int T) {
+  long *pre = malloc(sizeof(long) * ((size_t)T + 1));
+  for (int t = 0; t < T; t++) {
+    long s, e;
+    balanced_range(nnz, t, T, &s, &e);
+    pre[t] = s;
+    pre[t + 1] = e;
+  }
+  return pre;
+}
+static long *tiled_prefix(long nnz, int tile, int *T) {
+  *T = nnz == 0 ? 1 : (int)((nnz + tile - 1) / tile);
+  long *pre = malloc(sizeof(long) * ((size_t)*T + 1));
+  for (int t = 0; t <= *T; t++)
+    pre[t] = (long)t * tile < nnz ? (long)t * tile : nnz;
+  return pre;
+}
+
+void oracle_segsum_spmv(int T, int n, int base, const int *ai, const int *aj,
+                        const double *av, const double *b, double *x,
+                        double alpha, double beta) {
+  long *pre = balanced_prefix((long)ai[n] - base, T);
+  segsum_core(T, pre, n, base, ai, aj, av, b, x, alpha, beta);
+  free(pre);
+}
+
+/* SegSumSPMV's algorithm over fixed chunks of `tile` nonzeros. */
+void oracle_segsum_spmv_tiled(int tile, int n, int base, const int *ai,
+                              const int *aj, const double *av, const double *b,
+                              double *x, double alpha, double beta) {
+  int T;
+  long *pre = tiled_prefix((long)ai[n] - base, tile, &T);
+  segsum_core(T, pre, n, base, ai, aj, av, b, x, alpha, beta);
+  free(pre);
 }
 
 /* First index p in ai[0..n] with ai[p] > v (std::upper_bound). */
@@ -132,17 +170,11 @@ static int upper_bound_int(const int *a, int len, long v) {
  * merge scales each boundary row by beta once and adds the partials in
  * block order.  The reference leaves rows that precede the first block's
  * start row untouched (leading empty rows); this restatement does the same. */
-void oracle_albus_spmv(int T, int n, int base, const int *ai, const int *aj,
-                       const double *av, const double *b, double *x,
-                       double alpha, double beta) {
-  const long nnz = (long)ai[n] - base;
-  long *pre = malloc(sizeof(long) * ((size_t)T + 1));
+static void albus_core(int T, const long *pre, int n, int base,
+                       const int *ai, const int *aj, const double *av,
+                       const double *b, double *x, double alpha, double beta) {
   int *srow = malloc(sizeof(int) * ((size_t)T + 1));
   double *bnd = calloc(2 * (size_t)T, sizeof(double));
-  long w = nnz / T, r = nnz % T;
-  pre[0] = 0;
-  for (int i = 0; i < T; i++)
-    pre[i + 1] = i >= r ? (i + 1) * w + r : (i + 1) * (w + 1);
   for (int i = 0; i <= T; i++)
     srow[i] = upper_bound_int(ai, n + 1, pre[i] + base) - 1;
   for (int t = 0; t < T; t++) {
@@ -187,9 +219,26 @@ void oracle_albus_spmv(int T, int n, int base, const int *ai, const int *aj,
     }
     x[idx] += bnd[2 * t + 1];
   }
-  free(pre);
   free(srow);
   free(bnd);
+}
+
+void oracle_albus_spmv(int T, int n, int base, const int *ai, const int *aj,
+                       const double *av, const double *b, double *x,
+                       double alpha, double beta) {
+  long *pre = balanced_prefix((long)ai[n] - base, T);
+  albus_core(T, pre, n, base, ai, aj, av, b, x, alpha, beta);
+  free(pre);
+}
+
+/* ALBUSSPMV's algorithm over fixed chunks of `tile` nonzeros. */
+void oracle_albus_spmv_tiled(int tile, int n, int base, const int *ai,
+                             const int *aj, const double *av, const double *b,
+                             double *x, double alpha, double beta) {
+  int T;
+  long *pre = tiled_prefix((long)ai[n] - base, tile, &T);
+  albus_core(T, pre, n, base, ai, aj, av, b, x, alpha, beta);
+  free(pre);
 }
 
 /* Transposed product y = alpha * A^T g + beta * y, the SpMV adjoint

@@ -63,6 +63,49 @@ def test_spmv_golden(lab, golden, kind):
                        golden[f"{name}/spmv_{kind}_T{T}"]) <= TOL
 
 
+TILE = 1024       # nonzeros per GPU tile (la_spmv.cu kTile)
+LONG_SEG = 64     # in-tile row segments longer than this use a warp sum
+
+
+def short_segments_only(ai):
+    """True when every row's part inside every 1024-nonzero tile is <= 64
+    long (then each GPU row sum runs in the reference's sequential order)."""
+    ai = ai.astype(np.int64)
+    for r in range(len(ai) - 1):
+        lo, hi = ai[r], ai[r + 1]
+        while lo < hi:
+            end = min(hi, (lo // TILE + 1) * TILE)
+            if end - lo > LONG_SEG:
+                return False
+            lo = end
+    return True
+
+
+@pytest.mark.parametrize("kind", KINDS)
+def test_spmv_bit_exact_vs_tiled_reference_algorithm(lab, orc, golden, kind):
+    """With the reference's SegSum / ALBUS algorithm run over the GPU's
+    1024-nonzero chunks, the GPU result is bit-identical; rows that do not
+    cross a tile are bit-identical to SerialSPMV (ALBUS form)."""
+    P = orc.ptr
+    fn = getattr(orc.port(), f"oracle_{kind}_spmv_tiled")
+    checked = 0
+    for name, m, n, ai, aj, av in golden_matrices(golden):
+        if not short_segments_only(ai) or ai[1] == ai[0]:
+            continue
+        x, y0 = golden[f"{name}/spmv_x"], golden[f"{name}/spmv_y0"]
+        for alpha, beta, xv, yv in ((1.5, 0.5, x, y0), (1.0, 0.0, np.ones(n), np.zeros(m))):
+            ref = yv.copy()
+            fn(TILE, m, 0, P(ai), P(aj), P(av), P(xv), P(ref), alpha, beta)
+            y = run_spmv(lab, m, n, ai, aj, av, xv, yv, alpha, beta, kind)
+            assert np.array_equal(y, ref), (name, kind, alpha, np.abs(y - ref).max())
+            if kind == "albus":
+                ser = oracle_serial(orc, m, ai, aj, av, xv, yv, alpha, beta)
+                inside = (ai[:-1] // TILE == np.maximum(ai[1:] - 1, ai[:-1]) // TILE)
+                assert np.array_equal(y[inside], ser[inside]), name
+        checked += 1
+    assert checked >= 6
+
+
 @pytest.mark.parametrize("kind", KINDS)
 def test_spmv_host_path_drop_in(lab, golden, kind):
     cls = lab.SegSumSPMV if kind == "segsum" else lab.ALBUSSPMV
