@@ -111,6 +111,30 @@ la_status la_spmv_host(la_spmv_plan_t plan, double alpha, const double *x,
                        double beta, double *y);
 la_status la_spmv_plan_destroy(la_spmv_plan_t plan);
 
+/* Allocation-free SpMV.  No counterpart in the reference (which has no
+ * device code); it exists for callers that must not allocate device memory:
+ * code embedded in an application that hands out the whole device memory
+ * budget through its own pool, where a library cudaMalloc would fail or
+ * break that budget, and latency-critical loops that cannot take the
+ * implicit device-wide synchronisation of cudaMalloc / cudaFree.
+ * y = alpha*A*x + beta*y in FP64 with the SegSum or ALBUS form, from DEVICE
+ * CSR arrays (d_ai[n+1], d_aj[nnz], d_av[nnz], base 0 or 1), d_x (ncols
+ * entries) and d_y (n entries, not aliasing d_x); the result equals
+ * la_spmv's.  No cudaMalloc, cudaFree or allocating library call is made:
+ * the scratch lives in a fixed device array of 655,616 bytes that every GPU
+ * loading the library holds until the process exits, so nnz is limited to
+ * LA_SPMV_NOALLOC_MAX_NNZ (larger inputs return LA_ERR_INVALID_ARG).  The
+ * first call on a device looks up that array's device address (a one-time
+ * set-up per device); make that first call before any stream capture.  All
+ * calls share the array: each call rewrites what it reads, so nothing has
+ * to start at zero, but calls whose kernels overlap on the GPU (other
+ * streams, other host threads) race on it. */
+#define LA_SPMV_NOALLOC_MAX_NNZ (32768 * 1024)
+la_status la_spmv_noalloc(la_spmv_kind kind, int n, int nnz, int base,
+                          const int *d_ai, const int *d_aj, const double *d_av,
+                          double alpha, const double *d_x, double beta,
+                          double *d_y, la_stream_t stream);
+
 /* Adjoints of y = A x (no reference counterpart; the reference has none).
  * la_spmv_transpose: out = alpha * A^T g + beta * out (dL/dx), through a
  * transposed copy of A built once per plan on first use (the role

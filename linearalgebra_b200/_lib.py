@@ -58,6 +58,7 @@ _SIGS = {
     "la_spmv": [P, D, P, D, P, I, P],
     "la_spmv_host": [P, D, P, D, P],
     "la_spmv_plan_destroy": [P],
+    "la_spmv_noalloc": [I, I, I, I, P, P, P, D, P, D, P, P],
     "la_spmv_transpose": [P, D, P, D, P, P],
     "la_sddmm_pattern": [P, D, P, P, P, P],
     "la_topological_sort2": [I, I, I, P, P, P, P, IP],

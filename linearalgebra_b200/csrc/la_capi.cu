@@ -12,6 +12,9 @@ la_status spmv_launch(la_spmv_plan_t P, double alpha, const void *x,
                       cudaStream_t st);
 la_status sddmm_launch(la_spmv_plan_t P, double alpha, const double *g,
                        const double *x, double *dv, cudaStream_t st);
+la_status spmv_noalloc(la_spmv_kind kind, int n, int nnz, int base, const int *ai,
+                       const int *aj, const double *av, double alpha, const double *x,
+                       double beta, double *y, cudaStream_t st);
 la_status spmv_plan_build(la_spmv_plan_t P);
 la_status trsv_launch(la_trsv_plan_t P, const void *b, void *x,
                       cudaStream_t st);
@@ -309,6 +312,18 @@ la_status la_spmv_transpose(la_spmv_plan_t plan, double alpha, const double *g,
   LA_CHECK_ARG(plan && g && out && g != out, "arguments");
   LA_TRY(ensure_transpose(plan));
   return spmv_launch(plan->Atplan, alpha, g, beta, out, out, LA_F64, S(stream));
+}
+
+la_status la_spmv_noalloc(la_spmv_kind kind, int n, int nnz, int base,
+                          const int *d_ai, const int *d_aj, const double *d_av,
+                          double alpha, const double *d_x, double beta, double *d_y,
+                          la_stream_t stream) {
+  LA_CHECK_ARG(n >= 0 && nnz >= 0 && (base == 0 || base == 1), "sizes / base");
+  LA_CHECK_ARG(kind == LA_SPMV_SEGSUM || kind == LA_SPMV_ALBUS, "kind");
+  LA_CHECK_ARG(n == 0 || (d_ai && d_x && d_y && d_x != d_y), "pointers");
+  LA_CHECK_ARG(nnz == 0 || (d_aj && d_av), "aj / av");
+  return spmv_noalloc(kind, n, nnz, base, d_ai, d_aj, d_av, alpha, d_x, beta, d_y,
+                      S(stream));
 }
 
 la_status la_sddmm_pattern(la_spmv_plan_t plan, double alpha, const double *g,

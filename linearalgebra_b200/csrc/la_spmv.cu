@@ -41,6 +41,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 
 namespace la {
 namespace {
@@ -368,5 +369,118 @@ la_status spmv_plan_build(la_spmv_plan_t P) {
 }
 
 int spmv_tile_nnz() { return kTile; }
+
+// ---------------------------------------------------------------------------
+// Allocation-free SpMV (la_spmv_noalloc).  The per-call scratch of the tile
+// pass -- the row holding each tile's first nonzero and the head / tail
+// partial sums -- lives in this file-scope device array instead of plan
+// memory, so a call allocates nothing.  Capacity: kNoAllocMaxTiles tiles,
+// i.e. nnz <= kNoAllocMaxTiles * kTile = 33,554,432.  Every GPU that loads
+// the library holds the array (655,616 bytes) until the process exits.  All
+// calls share it: a call rewrites every entry it reads (nothing has to start
+// at zero), and calls whose kernels overlap on the GPU race on it.
+namespace {
+constexpr int kNoAllocMaxTiles = 32768;
+constexpr size_t kNoAllocPartBytes = sizeof(double) * 2 * kNoAllocMaxTiles;
+constexpr size_t kNoAllocBytes =
+    (kNoAllocPartBytes + sizeof(int) * (kNoAllocMaxTiles + 1) + 255) / 256 * 256;
+static __device__ __align__(256) unsigned char g_spmv_scratch[kNoAllocBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[kMaxDevices] = {};
+
+// Device address of g_spmv_scratch on the current device.  In host code the
+// array's name is only a host-side stand-in, so the address is looked up
+// once per device (the first call on that device) with that device current.
+la_status noalloc_scratch(void **out) {
+  int dev = 0;
+  LA_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) {
+    set_error("device ordinal %d out of range", dev);
+    return LA_ERR_INVALID_ARG;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void *p = nullptr;
+    LA_CUDA_TRY(cudaGetSymbolAddress(&p, g_spmv_scratch));
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return LA_OK;
+}
+
+// tile_row[t] = upper_bound(ai, min(t * kTile, nnz) + base) - 1, t <= ntiles
+__global__ void noalloc_tile_row_kernel(const int n, const int nnz, const int base,
+                                        const int *__restrict__ ai, const int ntiles,
+                                        int *tile_row) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t > ntiles)
+    return;
+  const int k = min(t * kTile, nnz) + base;
+  int lo = 0, hi = n + 1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(ai + mid) > k)
+      hi = mid;
+    else
+      lo = mid + 1;
+  }
+  tile_row[t] = lo - 1;
+}
+
+template <int FORM>
+la_status noalloc_launch(int n, int nnz, int base, const int *ai, const int *aj,
+                         const double *av, double alpha, const double *x, double beta,
+                         double *y, cudaStream_t st) {
+  if (n == 0)
+    return LA_OK;
+  if (nnz == 0) {
+    spmv_empty_kernel<double, double><<<std::min((n + 255) / 256, 4096), 256, 0, st>>>(
+        n, y, y, beta);
+    LA_CUDA_TRY(cudaGetLastError());
+    return LA_OK;
+  }
+  void *scratch = nullptr;
+  LA_TRY(noalloc_scratch(&scratch));
+  double *part = static_cast<double *>(scratch);
+  int *tile_row = reinterpret_cast<int *>(static_cast<unsigned char *>(scratch) +
+                                          kNoAllocPartBytes);
+  const int ntiles = (nnz + kTile - 1) / kTile;
+  noalloc_tile_row_kernel<<<(ntiles + 1 + 255) / 256, 256, 0, st>>>(n, nnz, base, ai,
+                                                                      ntiles, tile_row);
+  LA_CUDA_TRY(cudaGetLastError());
+  spmv_tile_kernel<FORM, double, double, double><<<ntiles, kThreads, 0, st>>>(
+      n, nnz, base, ai, aj, av, x, y, y, alpha, beta, tile_row, part);
+  LA_CUDA_TRY(cudaGetLastError());
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((ntiles + 255) / 256);
+  cfg.blockDim = dim3(256);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const double *yin = y, *pt = part;
+  const int *tr = tile_row;
+  LA_CUDA_TRY(cudaLaunchKernelEx(&cfg, spmv_merge_kernel<FORM, double, double>, ntiles, y,
+                                 yin, beta, tr, pt));
+  return LA_OK;
+}
+} // namespace
+
+la_status spmv_noalloc(la_spmv_kind kind, int n, int nnz, int base, const int *ai,
+                       const int *aj, const double *av, double alpha, const double *x,
+                       double beta, double *y, cudaStream_t st) {
+  if (nnz > kNoAllocMaxTiles * kTile) {
+    set_error("la_spmv_noalloc: nnz %d exceeds the allocation-free limit of %d "
+              "(use la_spmv with a plan)", nnz, kNoAllocMaxTiles * kTile);
+    return LA_ERR_INVALID_ARG;
+  }
+  if (kind == LA_SPMV_ALBUS)
+    return noalloc_launch<kAlbus>(n, nnz, base, ai, aj, av, alpha, x, beta, y, st);
+  return noalloc_launch<kSegSum>(n, nnz, base, ai, aj, av, alpha, x, beta, y, st);
+}
 
 } // namespace la
