@@ -285,6 +285,43 @@ def cpu_pcg(mats):
             "cores": T, "iterations": it, "s": dt, "rel_residual": float(rel[0])}
 
 
+def run_case(case):
+    """A small, fixed workload for profiling: builds one configuration and
+    launches its kernel 3 times (the first is a warm-up)."""
+    import torch
+    import linearalgebra_b200 as la
+    from linearalgebra_b200 import gen
+    if case.startswith("spmv"):
+        n, ai, aj, av = (gen.powerlaw(4_000_000, seed=0) if case == "spmv-powerlaw"
+                         else gen.laplacian_3d(128))
+        A = la.CSR(n, n, 0, ai, aj, av)
+        P = la.SPMV(A, la.api.LA_SPMV_SEGSUM)
+        x = torch.as_tensor(gen.uniform_vector(n, 0)).cuda()
+        y = torch.empty_like(x)
+        for _ in range(3):
+            P(x, y)
+    else:
+        n, ai, aj, av = gen.laplacian_3d(128)
+        iperm, perm = la.SerialCM(n, 0, ai, aj)
+        b_ai, b_aj, b_av = la.Permute(n, 0, ai, aj, av, iperm, perm)
+        ua, uj, uv = gen.upper_with_diag(n, b_ai, b_aj, b_av)
+        f = la.ICCLevelNumeric0(n, 0, ua, uj, uv)
+        b = torch.as_tensor(gen.uniform_vector(n, 0)).cuda()
+        x = torch.empty_like(b)
+        if case == "trsv-lap3d":
+            _, d, (s_ai, s_aj, s_av) = la.SplitLDU(n, 0, ua, uj, f)
+            t_ai, t_aj, t_av = la.Transpose(n, n, 0, s_ai, s_aj, s_av)
+            ts = la.OptimizedTriangularSolve("L").analysis(n, 0, t_ai, t_aj, t_av, d)
+            for _ in range(3):
+                ts(b, x)
+        else:
+            A = la.CSR(n, n, 0, b_ai, b_aj, b_av)
+            s = la.PCG(A, ua, uj, f)
+            s.solve(b, x, rtol=1e-10, maxit=5, allow_not_converged=True)
+    torch.cuda.synchronize()
+    print(f"case {case} done")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -293,11 +330,17 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-cpu-pcg", action="store_true")
+    ap.add_argument("--case", default=None,
+                    choices=["spmv-powerlaw", "spmv-lap3d", "trsv-lap3d", "pcg-lap3d"],
+                    help="run one kernel workload a few times and exit (for ncu)")
     args = ap.parse_args()
     args.steps_given = args.steps is not None
     if args.steps is None:
         args.steps = 1000
     args.warmup = max(args.warmup, 3)
+    if args.case:
+        run_case(args.case)
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -383,12 +426,13 @@ def main():
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "roofline": {"bound": "hbm", "achieved": byt / launch_s / 1e9, "peak": peak,
                      "unit": "GB/s", "frac": byt / launch_s / 1e9 / peak,
-                     "peak_kind": peak_kind, "kernel": "spmv_tile_kernel<SegSum, f64>",
+                     "peak_kind": peak_kind,
+                     "kernel": "spmv_tile_kernel<SegSum, f64> + spmv_merge_kernel (one step)",
                      "traffic": profiled_traffic("spmv_tile_kernel_segsum_f64_powerlaw4M")},
         "e2e": {"value": e2e, "unit": "GB/s", "h2d_bytes_per_step": n * 8,
                 "d2h_bytes_per_step": n * 8, "steps": e2e_steps,
                 "api": "SPMV.__call__ host arrays -> la_spmv_host", "matches_device": bool(ok)},
-        "gpu_launches": args.steps,
+        "gpu_launches": 2 * args.steps,
         "clocks": sampler.summary(),
     }
     if rank == 0 and world == 1:
