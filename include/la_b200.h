@@ -206,6 +206,20 @@ la_status la_trsv_analysis(la_uplo uplo, int n, int base, const int *ai,
                            const int *aj, const double *av,
                            const double *diag, la_dtype dtype,
                            la_trsv_plan_t *out);
+/* Same, with a caller-built level structure instead of TopologicalSort2's:
+ * iperm[n] (values carry the base) and zero-based prefix[nlevels + 1], the
+ * form TopologicalSort2 returns (matrix_utils.hpp:637-675) and
+ * LevelScheduleForward/BackwardSubstitution consume (triangle_solve.hpp:
+ * 100-145).  iperm must be a permutation and prefix run from 0 to n; that
+ * every row comes after the rows it reads is the caller's promise -- if it
+ * is broken, a solve may stall, and its bounded waits then end it with
+ * LA_ERR_TIMEOUT. */
+la_status la_trsv_analysis_levels(la_uplo uplo, int n, int base,
+                                  const int *ai, const int *aj,
+                                  const double *av, const double *diag,
+                                  la_dtype dtype, const int *iperm,
+                                  const int *prefix, int nlevels,
+                                  la_trsv_plan_t *out);
 /* x = T^-1 b (triangle_solve.tpp:115-155 operator()/BarrierOp): b, x device
  * arrays of the plan's dtype; b and x must not alias.  LA_ERR_TIMEOUT if a
  * dependency wait exceeded its bound (x is then undefined). */
@@ -254,6 +268,17 @@ la_status la_pcg_solve(la_pcg_t s, const double *b, double *x, double rtol,
 /* Host-pointer form (synchronous): b, x host arrays of n doubles. */
 la_status la_pcg_solve_host(la_pcg_t s, const double *b, double *x,
                             double rtol, int maxit, la_pcg_info *info);
+/* Adjoint of u = A^-1 b through a full solve (no reference counterpart; the
+ * reference has no derivatives).  For a loss L(u) with g = dL/du (device):
+ * lambda = A^-T g by one more preconditioned CG solve with the same operator
+ * (A is symmetric), returned as dl_db = dL/db; if dl_dvalues is non-NULL it
+ * receives dL/dA over A's stored pattern, -lambda_i * u_j for entry (i, j)
+ * (nnz values, A's order).  u is the forward solution (device).  For a
+ * symmetric parameterisation (a_ij and a_ji one parameter) add the two
+ * mirrored entries. */
+la_status la_pcg_adjoint(la_pcg_t s, const double *g, const double *u,
+                         double *dl_db, double *dl_dvalues, double rtol,
+                         int maxit, la_pcg_info *info, la_stream_t stream);
 la_status la_pcg_destroy(la_pcg_t s);
 
 #ifdef __cplusplus

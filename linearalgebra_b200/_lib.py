@@ -71,6 +71,7 @@ _SIGS = {
     "la_icc0": [I, I, P, P, P, D, P],
     "la_icc0_shifted": [I, I, P, P, P, P, C.POINTER(C.c_double)],
     "la_trsv_analysis": [I, I, I, P, P, P, P, I, C.POINTER(P)],
+    "la_trsv_analysis_levels": [I, I, I, P, P, P, P, I, P, P, I, C.POINTER(P)],
     "la_trsv": [P, P, P, P],
     "la_trsv_launch": [P, P, P, P],
     "la_trsv_status": [P, P],
@@ -80,6 +81,7 @@ _SIGS = {
     "la_pcg_create": [P, P, P, P, I, C.POINTER(P)],
     "la_pcg_solve": [P, P, P, D, I, C.POINTER(PcgInfo), P],
     "la_pcg_solve_host": [P, P, P, D, I, C.POINTER(PcgInfo)],
+    "la_pcg_adjoint": [P, P, P, P, P, D, I, C.POINTER(PcgInfo), P],
     "la_pcg_destroy": [P],
 }
 _RESTYPES = {"la_last_error_string": C.c_char_p, "la_version": C.c_char_p}

@@ -63,6 +63,17 @@ def _stream(t) -> C.c_void_p:
     return C.c_void_p(torch.cuda.current_stream(t.device).cuda_stream)
 
 
+def _release(fn: str, obj) -> None:
+    """Destroy a handle; quiet during interpreter shutdown."""
+    h = getattr(obj, "h", None)
+    obj.h = None
+    if h is not None and h.value:
+        try:
+            getattr(_lib.lib(), fn)(h)
+        except Exception:
+            pass
+
+
 def _is_device(a) -> bool:
     return not isinstance(a, np.ndarray) and getattr(a, "is_cuda", False)
 
@@ -93,10 +104,7 @@ class CSR:
             call("la_csr_update_values", self.h, _ptr(av), 0)
 
     def __del__(self):
-        h = getattr(self, "h", None)
-        if h is not None and h.value:
-            _lib.lib().la_csr_destroy(h)
-            self.h = None
+        _release("la_csr_destroy", self)
 
 
 class SPMV:
@@ -137,10 +145,7 @@ class SPMV:
         return dv
 
     def __del__(self):
-        h = getattr(self, "h", None)
-        if h is not None and h.value:
-            _lib.lib().la_spmv_plan_destroy(h)
-            self.h = None
+        _release("la_spmv_plan_destroy", self)
 
 
 def spmv_transpose(plan: SPMV, g, out, alpha=1.0, beta=0.0):
@@ -206,6 +211,20 @@ class OptimizedTriangularSolve:
         self.n = int(rows)
         return self
 
+    def analysis_levels(self, rows, base, ai, aj, av, iperm, prefix, diag=None):
+        """analysis() with a caller-built level structure (iperm, prefix)."""
+        ai, aj, av = _i32(ai), _i32(aj), _f64(av)
+        iperm, prefix = _i32(iperm), _i32(prefix)
+        d = None if diag is None else _f64(diag)
+        h = C.c_void_p()
+        call("la_trsv_analysis_levels", self.uplo, int(rows), int(base), _ptr(ai),
+             _ptr(aj), _ptr(av), _ptr(d),
+             LA_F64 if self.dtype == np.float64 else LA_F32, _ptr(iperm),
+             _ptr(prefix), len(prefix) - 1, C.byref(h))
+        self.h = h
+        self.n = int(rows)
+        return self
+
     def levels(self):
         lv = C.c_int()
         call("la_trsv_levels", self.h, C.byref(lv), None, None)
@@ -234,10 +253,7 @@ class OptimizedTriangularSolve:
         return self._nthreads
 
     def __del__(self):
-        h = getattr(self, "h", None)
-        if h is not None and h.value:
-            _lib.lib().la_trsv_plan_destroy(h)
-            self.h = None
+        _release("la_trsv_plan_destroy", self)
 
 
 # --------------------------------------------------------- host analysis
@@ -383,8 +399,14 @@ class PCG:
                          info.rel_residual, info.solve_ms,
                          _lib.STATUS_NAMES.get(st, str(st)))
 
+    def adjoint(self, g, u, dl_db, dl_dvalues=None, rtol=1e-10, maxit=10000):
+        """lambda = A^-T g into dl_db; dL/dA_ij = -lambda_i u_j into dl_dvalues
+        (device FP64 tensors)."""
+        info = PcgInfo()
+        call("la_pcg_adjoint", self.h, _ptr(g), _ptr(u), _ptr(dl_db),
+             _ptr(dl_dvalues), float(rtol), int(maxit), C.byref(info), _stream(g))
+        return PCGResult(info.iterations, info.outer_iterations, info.rel_residual,
+                         info.solve_ms, "LA_OK")
+
     def __del__(self):
-        h = getattr(self, "h", None)
-        if h is not None and h.value:
-            _lib.lib().la_pcg_destroy(h)
-            self.h = None
+        _release("la_pcg_destroy", self)

@@ -19,13 +19,17 @@ la_status spmv_plan_build(la_spmv_plan_t P);
 la_status trsv_launch(la_trsv_plan_t P, const void *b, void *x,
                       cudaStream_t st);
 la_status trsv_build(la_trsv_plan_t P, const int *ai, const int *aj,
-                     const double *av, const double *diag);
+                     const double *av, const double *diag, const int *iperm = nullptr,
+                     const int *prefix = nullptr, int nlevels = 0);
 la_status trsv_check(la_trsv_plan_t P, cudaStream_t st);
 la_status pcg_create(la_csr_t A, const int *u_ai, const int *u_aj,
                      const double *icc_av, la_pcg_mode mode, la_pcg_t *out);
 la_status pcg_solve(la_pcg_t S, const double *b, double *x, double rtol,
                     int maxit, la_pcg_info *info, cudaStream_t st);
 void pcg_destroy(la_pcg_t S);
+la_status pcg_adjoint(la_pcg_t S, const double *g, const double *u, double *dl_db,
+                      double *dl_dv, double rtol, int maxit, la_pcg_info *info,
+                      cudaStream_t st);
 
 namespace {
 thread_local char g_err[512] = "";
@@ -439,10 +443,11 @@ la_status la_icc0_shifted(int n, int base, const int *u_ai, const int *u_aj,
 }
 
 // ------------------------------------------------------------------ trsv
-la_status la_trsv_analysis(la_uplo uplo, int n, int base, const int *ai,
-                           const int *aj, const double *av,
-                           const double *diag, la_dtype dtype,
-                           la_trsv_plan_t *out) {
+static la_status trsv_analysis_impl(la_uplo uplo, int n, int base, const int *ai,
+                                    const int *aj, const double *av,
+                                    const double *diag, la_dtype dtype,
+                                    const int *iperm, const int *prefix,
+                                    int nlevels, la_trsv_plan_t *out) {
   LA_CHECK_ARG(out && ai && n >= 0, "arguments");
   LA_CHECK_ARG(uplo == LA_LOWER || uplo == LA_UPPER, "uplo");
   LA_CHECK_ARG(dtype == LA_F64 || dtype == LA_F32, "dtype");
@@ -460,6 +465,18 @@ la_status la_trsv_analysis(la_uplo uplo, int n, int base, const int *ai,
         return LA_ERR_INVALID_ARG;
       }
     }
+  if (iperm) {
+    LA_CHECK_ARG(prefix && nlevels >= 0 && prefix[0] == 0 && prefix[nlevels] == n,
+                 "level prefix must start at 0 and end at n");
+    for (int l = 0; l < nlevels; l++)
+      LA_CHECK_ARG(prefix[l + 1] >= prefix[l], "level prefix must be non-decreasing");
+    std::vector<char> seen(n, 0);
+    for (int p = 0; p < n; p++) {
+      const int i = iperm[p] - base;
+      LA_CHECK_ARG(i >= 0 && i < n && !seen[i], "iperm must be a permutation");
+      seen[i] = 1;
+    }
+  }
   LA_TRY(require_device());
   std::unique_ptr<la_trsv_plan_s> P(new la_trsv_plan_s());
   P->n = n;
@@ -468,9 +485,27 @@ la_status la_trsv_analysis(la_uplo uplo, int n, int base, const int *ai,
   P->uplo = uplo;
   P->dtype = dtype;
   P->unit = diag == nullptr;
-  LA_TRY(trsv_build(P.get(), ai, aj, av, diag));
+  LA_TRY(trsv_build(P.get(), ai, aj, av, diag, iperm, prefix, nlevels));
   *out = P.release();
   return LA_OK;
+}
+
+la_status la_trsv_analysis(la_uplo uplo, int n, int base, const int *ai,
+                           const int *aj, const double *av,
+                           const double *diag, la_dtype dtype,
+                           la_trsv_plan_t *out) {
+  return trsv_analysis_impl(uplo, n, base, ai, aj, av, diag, dtype, nullptr, nullptr,
+                            0, out);
+}
+
+la_status la_trsv_analysis_levels(la_uplo uplo, int n, int base, const int *ai,
+                                  const int *aj, const double *av,
+                                  const double *diag, la_dtype dtype,
+                                  const int *iperm, const int *prefix,
+                                  int nlevels, la_trsv_plan_t *out) {
+  LA_CHECK_ARG(iperm && prefix, "iperm / prefix are NULL");
+  return trsv_analysis_impl(uplo, n, base, ai, aj, av, diag, dtype, iperm, prefix,
+                            nlevels, out);
 }
 
 la_status la_trsv(la_trsv_plan_t plan, const void *b, void *x,
@@ -552,6 +587,13 @@ la_status la_pcg_solve_host(la_pcg_t s, const double *b, double *x,
                                  rtol, maxit, info, nullptr);
   LA_CUDA_TRY(cudaMemcpy(x, s->hx.p, sizeof(double) * s->n, cudaMemcpyDeviceToHost));
   return st;
+}
+
+la_status la_pcg_adjoint(la_pcg_t s, const double *g, const double *u,
+                         double *dl_db, double *dl_dvalues, double rtol, int maxit,
+                         la_pcg_info *info, la_stream_t stream) {
+  LA_CHECK_ARG(s && g && u && dl_db && g != dl_db && rtol > 0 && maxit > 0, "arguments");
+  return pcg_adjoint(s, g, u, dl_db, dl_dvalues, rtol, maxit, info, S(stream));
 }
 
 la_status la_pcg_destroy(la_pcg_t s) {

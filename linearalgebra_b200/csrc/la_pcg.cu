@@ -35,7 +35,8 @@ la_status trsv_launch(la_trsv_plan_t P, const void *b, void *x,
                       cudaStream_t st);
 la_status trsv_check(la_trsv_plan_t P, cudaStream_t st);
 la_status trsv_build(la_trsv_plan_t P, const int *ai, const int *aj,
-                     const double *av, const double *diag);
+                     const double *av, const double *diag, const int *iperm = nullptr,
+                     const int *prefix = nullptr, int nlevels = 0);
 la_status spmv_plan_build(la_spmv_plan_t P);
 
 namespace {
@@ -392,6 +393,22 @@ la_status pcg_solve(la_pcg_t S, const double *b, double *x, double rtol,
     set_error("PCG did not reach rtol %.3g in %d iterations (residual %.3g)",
               rtol, maxit, loc.rel_residual);
   return res;
+}
+
+// Adjoint of u = A^-1 b for a loss L(u): lambda = A^-T dL/du (A is
+// symmetric, so one more PCG solve with the same operator and
+// preconditioner), dL/db = lambda, dL/dA_ij = -lambda_i u_j over A's stored
+// pattern (the sampled outer product of la_sddmm_pattern).
+la_status sddmm_launch(la_spmv_plan_t P, double alpha, const double *g,
+                       const double *x, double *dv, cudaStream_t st);
+
+la_status pcg_adjoint(la_pcg_t S, const double *g, const double *u, double *dl_db,
+                      double *dl_dv, double rtol, int maxit, la_pcg_info *info,
+                      cudaStream_t st) {
+  LA_TRY(pcg_solve(S, g, dl_db, rtol, maxit, info, st));
+  if (dl_dv)
+    LA_TRY(sddmm_launch(S->Ap, -1.0, dl_db, u, dl_dv, st));
+  return LA_OK;
 }
 
 void pcg_destroy(la_pcg_t S) {

@@ -233,15 +233,24 @@ la_status trsv_launch(la_trsv_plan_t P, const void *b, void *x,
 
 // Analysis: TopologicalSort2 levels, rows in execution order, 32-row chunks
 // that never cross a level (triangle_solve.tpp:17-113 equivalent).
+// A caller-supplied level structure (iperm/prefix as TopologicalSort2
+// returns them) replaces the computed one when `iperm` is non-null.
 la_status trsv_build(la_trsv_plan_t P, const int *ai, const int *aj,
-                     const double *av, const double *diag) {
+                     const double *av, const double *diag, const int *iperm,
+                     const int *prefix, int nlevels) {
   const int n = P->n, base = P->base;
-  P->h_iperm.resize(n);
-  P->h_prefix.resize(n + 1);
-  P->levels = n == 0 ? 0
-                     : topological_sort2(P->uplo, n, base, ai, aj,
-                                         P->h_iperm.data(), P->h_prefix.data());
-  P->h_prefix.resize(P->levels + 1);
+  if (iperm) {
+    P->levels = nlevels;
+    P->h_iperm.assign(iperm, iperm + n);
+    P->h_prefix.assign(prefix, prefix + nlevels + 1);
+  } else {
+    P->h_iperm.resize(n);
+    P->h_prefix.resize(n + 1);
+    P->levels = n == 0 ? 0
+                       : topological_sort2(P->uplo, n, base, ai, aj,
+                                           P->h_iperm.data(), P->h_prefix.data());
+    P->h_prefix.resize(P->levels + 1);
+  }
   if (n == 0)
     return LA_OK;
   std::vector<int> eai(n + 1), erow(n), cstart;

@@ -204,20 +204,27 @@ static void albus_core(int T, const long *pre, int n, int base,
       bnd[2 * t + 1] = 0;
     }
   }
+  /* With more chunks than nonzeros the trailing empty chunks start at row n
+   * and the reference's merge writes x[n], one past the output
+   * (spmv.hpp:275-292); rows >= n are skipped here (their partials are 0). */
   int idx = -1;
   for (int t = 0; t < T; t++) {
     if (srow[t] != idx) {
       idx = srow[t];
-      x[idx] *= beta;
+      if (idx < n)
+        x[idx] *= beta;
     }
-    x[idx] += bnd[2 * t];
+    if (idx < n)
+      x[idx] += bnd[2 * t];
     if (t == T - 1)
       break;
     if (srow[t + 1] != idx) {
       idx = srow[t + 1];
-      x[idx] *= beta;
+      if (idx < n)
+        x[idx] *= beta;
     }
-    x[idx] += bnd[2 * t + 1];
+    if (idx < n)
+      x[idx] += bnd[2 * t + 1];
   }
   free(srow);
   free(bnd);

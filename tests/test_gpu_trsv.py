@@ -135,3 +135,52 @@ def test_trsv_host_path(lab, golden):
     x = np.zeros(n)
     ts(np.ones(n), x)
     assert rel(x, golden["lap2d_32/fwd_unit"]) <= TOL
+
+
+def _chain(n):
+    """Row i reads row i - 1 (strict lower bidiagonal, values 0.5)."""
+    ai = np.zeros(n + 1, np.int32)
+    ai[2:] = np.arange(1, n, dtype=np.int32)
+    return ai, np.arange(n - 1, dtype=np.int32), np.full(n - 1, 0.5)
+
+
+def test_trsv_bounded_wait_reports_timeout(lab, orc):
+    """A caller-built level set that schedules every row before the row it
+    reads stalls the persistent solve (all resident warps wait on chunks no
+    warp can claim).  The bounded waits end it with LA_ERR_TIMEOUT after about
+    a second, without a fault, trap or hang, and the context stays usable."""
+    import time
+    n = 200_000
+    ai, aj, av = _chain(n)
+    iperm = np.arange(n, dtype=np.int32)[::-1].copy()
+    prefix = np.array([0, n], np.int32)
+    bad = lab.OptimizedTriangularSolve("L").analysis_levels(n, 0, ai, aj, av, iperm, prefix)
+    b = torch.ones(n, dtype=torch.float64, device="cuda")
+    x = torch.empty_like(b)
+    t0 = time.time()
+    with pytest.raises(lab.LAError) as e:
+        bad(b, x)
+    assert e.value.name == "LA_ERR_TIMEOUT"
+    assert time.time() - t0 < 30
+    good = lab.OptimizedTriangularSolve("L").analysis(n, 0, ai, aj, av)
+    good(b, x)
+    ref = np.zeros(n)
+    P = orc.ptr
+    bn = np.ones(n)
+    orc.port().oracle_forward_substitution(n, 0, P(ai), P(aj), P(av), P(bn), P(ref))
+    assert np.array_equal(x.cpu().numpy(), ref)
+    # a level order that respects the dependencies works through the same entry
+    ok = lab.OptimizedTriangularSolve("L").analysis_levels(
+        n, 0, ai, aj, av, np.arange(n, dtype=np.int32), np.arange(n + 1, dtype=np.int32))
+    ok(b, x)
+    assert np.array_equal(x.cpu().numpy(), ref)
+
+
+def test_trsv_levels_validation(lab):
+    ai, aj, av = _chain(8)
+    with pytest.raises(lab.LAError):  # not a permutation
+        lab.OptimizedTriangularSolve("L").analysis_levels(
+            8, 0, ai, aj, av, np.zeros(8, np.int32), np.array([0, 8], np.int32))
+    with pytest.raises(lab.LAError):  # prefix does not end at n
+        lab.OptimizedTriangularSolve("L").analysis_levels(
+            8, 0, ai, aj, av, np.arange(8, dtype=np.int32), np.array([0, 7], np.int32))
