@@ -246,14 +246,16 @@ la_status la_trsv_plan_destroy(la_trsv_plan_t plan);
  * 150-251, mkl_wrapper/incomplete_cholesky.cpp:21-29, 286-342).
  * A: FP64 CSR handle (full symmetric storage).  u_ai/u_aj/icc_av: HOST IC
  * factor U (upper, diagonal first, as la_icc0 returns).  mode LA_PCG_FP64:
- * everything FP64.  mode LA_PCG_MIXED: FP64 outer iterative refinement
- * (r = b - A x with FP64 A, FP64 update) around an inner PCG whose SpMV and
- * triangular solves read FP32 A / FP32 factors and accumulate in FP32,
- * with FP64 dot products and norms. */
+ * everything FP64.  mode LA_PCG_MIXED: FP64 iterative refinement by
+ * reliable updates -- the CG recurrence runs on FP32 vectors whose SpMV and
+ * triangular solves read FP32 A / FP32 factors and accumulate in FP32, with
+ * FP64 dot products and scalars; whenever its residual has dropped tenfold,
+ * x is updated in FP64 and the residual is replaced by r = b - A x computed
+ * with the FP64 matrix, keeping the search direction. */
 typedef enum { LA_PCG_FP64 = 0, LA_PCG_MIXED = 1 } la_pcg_mode;
 typedef struct {
   int iterations;        /* total (inner) PCG iterations */
-  int outer_iterations;  /* refinement steps (1 for FP64) */
+  int outer_iterations;  /* FP64 residual replacements (1 for FP64) */
   double rel_residual;   /* true ||b - A x|| / ||b|| in FP64 at exit */
   double solve_ms;       /* device time of the solve, CUDA events */
 } la_pcg_info;

@@ -114,6 +114,7 @@ struct la_trsv_plan_s {
   la::DevBuf ai, aj, av, diag, exec_row, chunk_start, err, ticket;
   int nchunks = 0;
   int grid = 0;
+  int kd = 0; // dependency slots of the kernel variant (0: grouped form)
   la::DevBuf hb, hx; // staging for the host form
 };
 

@@ -15,11 +15,10 @@
 // only if that is below rtol too (the reference's test, evaluated where it
 // can change the outcome instead of after every iteration).
 //
-// Mixed mode: FP64 iterative refinement.  r = b - A x with the FP64 matrix,
-// then an inner PCG on A d = r / ||r|| whose SpMV and triangular solves read
-// FP32 values and FP32 vectors and accumulate in FP32, with FP64 dot
-// products and scalars; x += ||r|| d in FP64.  The inner solve stops at a
-// relative residual of kInnerTol.
+// Mixed mode: FP64 iterative refinement by reliable updates (pcg_mixed):
+// the CG recurrence runs on FP32 vectors with FP32 matrix / factors, and the
+// FP64 residual b - A x, FP64 update of x and FP64 dot products and norms
+// recover the accuracy without restarting the Krylov space.
 
 #include "la_device.cuh"
 #include "la_internal.h"
@@ -42,7 +41,6 @@ la_status spmv_plan_build(la_spmv_plan_t P);
 namespace {
 
 constexpr int kDotThreads = 512;
-constexpr double kInnerTol = 1e-5;
 
 // Scalar slots in device memory.
 enum { S_RZ = 0, S_PQ, S_RR, S_ALPHA, S_BETA, S_DOT, S_COUNT };
@@ -237,6 +235,84 @@ la_status pcg_run(la_pcg_t S, const X *rhs, X *y, X *r, X *z, X *p, X *q,
   return LA_ERR_NOT_CONVERGED;
 }
 
+// Mixed precision with reliable updates (FP64 iterative refinement that
+// keeps the Krylov space): the CG recurrence runs on FP32 vectors with the
+// FP32 matrix and FP32 IC(0) factors (FP32 SpMV and triangular solves, FP32
+// accumulation in those kernels), its dot products and scalars in FP64.  The
+// FP32 iterate is a correction d accumulated since the last update; whenever
+// the FP32 residual has fallen by kReliableDelta since then (or below rtol),
+// x += d in FP64, the residual is recomputed as r = b - A x with the FP64
+// matrix, and the FP32 residual is replaced by it -- without restarting the
+// search direction, so the iteration count stays close to the FP64 solver's.
+// The solve stops when that FP64 residual satisfies ||r|| / ||b|| < rtol.
+constexpr double kReliableDelta = 0.1;
+
+la_status pcg_mixed(la_pcg_t S, const double *b, double *x, double bn, double rtol,
+                    int maxit, la_pcg_info *loc, cudaStream_t st) {
+  const int n = S->n, g = vec_grid(n);
+  float *r32 = S->r32.as<float>(), *z32 = S->z32.as<float>(), *p32 = S->p32.as<float>(),
+        *q32 = S->q32.as<float>(), *t32 = S->t32.as<float>(), *d32 = S->d32.as<float>();
+  double *r64 = S->r.as<double>();
+  zero_kernel<<<g, 256, 0, st>>>(n, x);
+  LA_CUDA_TRY(cudaMemsetAsync(d32, 0, sizeof(float) * n, st));
+  scale_copy_kernel<float, double><<<g, 256, 0, st>>>(n, r32, b, 1.0);
+  LA_TRY(trsv_launch(S->L, r32, t32, st));
+  LA_TRY(trsv_launch(S->U, t32, z32, st));
+  LA_CUDA_TRY(cudaMemcpyAsync(p32, z32, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+  LA_TRY(dot(S, r32, z32, OP_STORE, st));
+  LA_CUDA_TRY(cudaMemcpyAsync(S->scal.as<double>() + S_RZ, S->scal.as<double>() + S_DOT,
+                              sizeof(double), cudaMemcpyDeviceToDevice, st));
+  double rmax = bn, rel = 1.0;
+  int updates = 0, it;
+  for (it = 1; it <= maxit; it++) {
+    LA_TRY(spmv_launch(S->Ap, 1.0, p32, 0.0, q32, q32, LA_F32, st));
+    LA_TRY(dot(S, p32, q32, OP_ALPHA, st));
+    xr_update_kernel<float><<<g, 256, 0, st>>>(n, d32, r32, p32, q32, S->scal.as<double>());
+    LA_TRY(dot(S, r32, r32, OP_STORE, st));
+    double rr;
+    LA_TRY(read_scalar(S, S_DOT, &rr, st));
+    const double rn = std::sqrt(rr);
+    if (!std::isfinite(rn)) {
+      set_error("mixed PCG breakdown: non-finite residual at iteration %d", it);
+      loc->iterations = it;
+      return LA_ERR_BREAKDOWN;
+    }
+    if (rn < kReliableDelta * rmax || rn / bn < rtol) {
+      refine_kernel<<<g, 256, 0, st>>>(n, x, d32, 1.0);
+      LA_CUDA_TRY(cudaMemsetAsync(d32, 0, sizeof(float) * n, st));
+      LA_TRY(spmv_launch(S->Ap, -1.0, x, 1.0, r64, b, LA_F64, st));
+      LA_TRY(dot(S, r64, r64, OP_STORE, st));
+      double rr64;
+      LA_TRY(read_scalar(S, S_DOT, &rr64, st));
+      rmax = std::sqrt(rr64);
+      rel = rmax / bn;
+      updates++;
+      if (rel < rtol)
+        break;
+      scale_copy_kernel<float, double><<<g, 256, 0, st>>>(n, r32, r64, 1.0);
+    }
+    LA_TRY(trsv_launch(S->L, r32, t32, st));
+    LA_TRY(trsv_launch(S->U, t32, z32, st));
+    LA_TRY(dot(S, r32, z32, OP_BETA, st));
+    p_update_kernel<float><<<g, 256, 0, st>>>(n, p32, z32, S->scal.as<double>());
+  }
+  loc->iterations = std::min(it, maxit);
+  loc->outer_iterations = updates;
+  loc->rel_residual = rel;
+  if (rel >= rtol) {
+    // final FP64 residual of the last iterate
+    refine_kernel<<<g, 256, 0, st>>>(n, x, d32, 1.0);
+    LA_TRY(spmv_launch(S->Ap, -1.0, x, 1.0, r64, b, LA_F64, st));
+    LA_TRY(dot(S, r64, r64, OP_STORE, st));
+    double rr64;
+    LA_TRY(read_scalar(S, S_DOT, &rr64, st));
+    loc->rel_residual = std::sqrt(rr64) / bn;
+    if (loc->rel_residual >= rtol)
+      return LA_ERR_NOT_CONVERGED;
+  }
+  return LA_OK;
+}
+
 } // namespace
 
 la_status pcg_create(la_csr_t A, const int *u_ai, const int *u_aj,
@@ -336,47 +412,7 @@ la_status pcg_solve(la_pcg_t S, const double *b, double *x, double rtol,
                           &loc.rel_residual, st);
     loc.outer_iterations = 1;
   } else {
-    zero_kernel<<<vec_grid(n), 256, 0, st>>>(n, x);
-    double rel = 1.0;
-    int total = 0;
-    // r = b - A x (x = 0 -> r = b)
-    LA_CUDA_TRY(cudaMemcpyAsync(S->r.p, b, sizeof(double) * n,
-                                cudaMemcpyDeviceToDevice, st));
-    double rn = bn;
-    for (int outer = 1; outer <= 20; outer++) {
-      loc.outer_iterations = outer;
-      scale_copy_kernel<float, double><<<vec_grid(n), 256, 0, st>>>(
-          n, S->q32.as<float>(), S->r.as<double>(), 1.0 / rn);
-      int it = 0;
-      double irel = 0;
-      const la_status s = pcg_run<float>(
-          S, S->q32.as<float>(), S->d32.as<float>(), S->r32.as<float>(),
-          S->z32.as<float>(), S->p32.as<float>(), S->t32.as<float>(),
-          S->t32.as<float>() /* scratch reused below */, LA_F32, kInnerTol,
-          maxit - total, nullptr, 1.0, &it, &irel, st);
-      total += it;
-      if (s != LA_OK && s != LA_ERR_NOT_CONVERGED) {
-        res = s;
-        break;
-      }
-      refine_kernel<<<vec_grid(n), 256, 0, st>>>(n, x, S->d32.as<float>(), rn);
-      LA_TRY(spmv_launch(S->Ap, -1.0, x, 1.0, S->r.p, b, LA_F64, st));
-      LA_TRY(dot(S, S->r.as<double>(), S->r.as<double>(), OP_STORE, st));
-      double rr;
-      LA_TRY(read_scalar(S, S_DOT, &rr, st));
-      rn = std::sqrt(rr);
-      rel = rn / bn;
-      if (rel < rtol)
-        break;
-      if (total >= maxit) {
-        res = LA_ERR_NOT_CONVERGED;
-        break;
-      }
-    }
-    loc.iterations = total;
-    loc.rel_residual = rel;
-    if (res == LA_OK && rel >= rtol)
-      res = LA_ERR_NOT_CONVERGED;
+    res = pcg_mixed(S, b, x, bn, rtol, maxit, &loc, st);
   }
   LA_CUDA_TRY(cudaEventRecord(S->ev1, st));
   LA_CUDA_TRY(cudaEventSynchronize(S->ev1));
