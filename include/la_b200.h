@@ -200,8 +200,12 @@ la_status la_icc0_shifted(int n, int base, const int *u_ai, const int *u_aj,
  * host, rows stored in execution (level) order, uploaded once.  ai/aj/av:
  * HOST CSR of the STRICT triangle; diag: host array of n values or NULL
  * (unit diagonal).  `dtype` selects FP64 or FP32 storage (FP32 values and
- * FP32 vectors in la_trsv).  The persistent solve kernel walks the levels
- * with per-row readiness (no launch per level) and bounded waits. */
+ * FP32 vectors in la_trsv).  One kernel launch per solve, with one of two
+ * schedules chosen here by a cost model (see la_trsv_schedule): the level
+ * order over the whole GPU with per-row readiness, or a partition of the
+ * rows into co-resident CTAs that keep their rows' values in shared memory
+ * and hand values across parts through global memory.  Every wait is
+ * bounded. */
 la_status la_trsv_analysis(la_uplo uplo, int n, int base, const int *ai,
                            const int *aj, const double *av,
                            const double *diag, la_dtype dtype,
@@ -238,6 +242,12 @@ la_status la_trsv_host(la_trsv_plan_t plan, const double *b, double *x);
  * prefix[levels + 1] exactly as TopologicalSort2 returns them. */
 la_status la_trsv_levels(la_trsv_plan_t plan, int *levels, int *iperm,
                          int *prefix);
+/* Schedule the analysis chose (no reference counterpart; both compute the
+ * same bits): *schedule = 0 for level order over the whole GPU with per-row
+ * readiness, 1 for the partitioned form (*parts co-resident CTAs, each
+ * keeping its rows' values in shared memory).  Set LA_TRSV_SCHEDULE=flags or
+ * =parts in the environment before the analysis to force one. */
+la_status la_trsv_schedule(la_trsv_plan_t plan, int *schedule, int *parts);
 la_status la_trsv_plan_destroy(la_trsv_plan_t plan);
 
 /* ---------------------------------------------------------- IC(0)-PCG */

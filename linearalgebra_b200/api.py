@@ -225,6 +225,12 @@ class OptimizedTriangularSolve:
         self.n = int(rows)
         return self
 
+    def schedule(self):
+        """('levels', 0) or ('parts', number of parts): the analysis's choice."""
+        s, p = C.c_int(), C.c_int()
+        call("la_trsv_schedule", self.h, C.byref(s), C.byref(p))
+        return ("parts" if s.value == 1 else "levels"), p.value
+
     def levels(self):
         lv = C.c_int()
         call("la_trsv_levels", self.h, C.byref(lv), None, None)

@@ -553,6 +553,13 @@ la_status la_trsv_levels(la_trsv_plan_t plan, int *levels, int *iperm,
   return LA_OK;
 }
 
+la_status la_trsv_schedule(la_trsv_plan_t plan, int *schedule, int *parts) {
+  LA_CHECK_ARG(plan && schedule && parts, "arguments");
+  *schedule = plan->sched;
+  *parts = plan->sched == 1 ? plan->nparts : 0;
+  return LA_OK;
+}
+
 la_status la_trsv_plan_destroy(la_trsv_plan_t plan) {
   delete plan;
   return LA_OK;

@@ -78,6 +78,13 @@ int split_triangle(int uplo, int n, int base, const int *ai, const int *aj,
 bool icc0(int n, int base, const int *u_ai, const int *u_aj, const double *u_av,
           double omega, double *icc_av);
 void rcm(int n, int base, const int *ai, const int *aj, int *iperm, int *perm);
+// Row partition for the partitioned triangular solve (la_partition.cpp):
+// k-d cuts on coordinates monotone along the dependency edges (row i reads
+// row j for every stored (i, j) of dep_ptr/dep_col, which carry `base`), so
+// the parts' dependency graph is acyclic.  xadj/adj: the 0-based undirected
+// graph; lvl: the rows' levels.  Returns the number of coordinates used.
+int monotone_partition(int n, const int *xadj, const int *adj, const int *dep_ptr,
+                       const int *dep_col, int base, const int *lvl, int nparts, int *part);
 
 } // namespace la
 
@@ -115,6 +122,14 @@ struct la_trsv_plan_s {
   int nchunks = 0;
   int grid = 0;
   int kd = 0; // dependency slots of the kernel variant (0: grouped form)
+  // schedule: 0 = level order over the whole GPU with per-row readiness;
+  // 1 = partitioned (one co-resident CTA per part, part values in shared
+  // memory).  For schedule 1 the execution order is part-major, level-minor
+  // and aj holds -1 - (position in the part) for a column of the same part.
+  int sched = 0, nparts = 0, part_rows = 0;
+  size_t part_smem = 0; // x slots of the largest part + its level boundaries
+  la::DevBuf pstart, psub, sb;
+  la::DevBuf ej, ev; // first slots of every row, slot-major (schedule 1)
   la::DevBuf hb, hx; // staging for the host form
 };
 

@@ -1,0 +1,251 @@
+// la_partition.cpp -- row partition for the partitioned triangular solve.
+//
+// Goal: parts whose dependency graph (part A -> part B when a row of B reads
+// a row of A) is acyclic and shallow, so that a dependency path crosses few
+// part boundaries.  Every cut is made on a coordinate f that is monotone
+// along the dependency edges (f(j) <= f(i) whenever row i reads row j), low
+// values to one side, high values to the other: an edge can then only cross
+// from the low side to the high side, so ordering the parts low-before-high
+// at every cut makes every cross-part edge go forward (acyclic), and a path
+// crosses each cut at most once.  Cutting P ways along ONE coordinate (say
+// the level) gives P slabs that a path crosses P - 1 times; cutting along
+// three independent monotone coordinates gives boxes, crossed about
+// 3 * P^(1/3) times.
+//
+// Coordinates: differences of breadth-first distances to landmark vertices,
+// d_a - d_b, kept when monotone along every dependency edge; the level is
+// always a candidate.  Landmarks are spread by farthest-point sampling over
+// the vertices of minimum degree (the corners of a mesh: on a grid, corner
+// landmarks make d_a - d_b a multiple of one grid axis).  Among the monotone
+// candidates, the narrowest are taken first, each only if it is independent
+// enough of those already taken (Gram-Schmidt residual), up to three.  The
+// parts then come from a k-d tree: each node is cut on the candidate with
+// the largest span over its rows, at the value that best splits its rows in
+// the ratio of the part counts of its two halves.
+//
+// This is scheduling, not arithmetic: the triangular solve computes every
+// row with the same operations whatever the partition.
+
+#include "la_internal.h"
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <numeric>
+#include <vector>
+
+namespace la {
+namespace {
+
+// breadth-first distances from src; -1 where unreachable
+void bfs_dist(int n, const int *xadj, const int *adj, int src, std::vector<int> &d,
+              std::vector<int> &queue) {
+  d.assign(n, -1);
+  queue.clear();
+  d[src] = 0;
+  queue.push_back(src);
+  for (size_t h = 0; h < queue.size(); h++) {
+    const int u = queue[h];
+    for (int k = xadj[u]; k < xadj[u + 1]; k++) {
+      const int v = adj[k];
+      if (d[v] < 0) {
+        d[v] = d[u] + 1;
+        queue.push_back(v);
+      }
+    }
+  }
+}
+
+} // namespace
+
+int monotone_partition(int n, const int *xadj, const int *adj, const int *dep_ptr,
+                       const int *dep_col, int base, const int *lvl, int nparts, int *part) {
+  if (n == 0)
+    return 0;
+  std::vector<std::vector<int>> coords; // chosen coordinates
+  std::vector<std::vector<double>> basis;
+  // candidate: orientation-normalised values, ascending range order later
+  struct Cand {
+    int a, b, sign;
+    long long range;
+  };
+  std::vector<Cand> cands;
+  std::vector<std::vector<int>> dist;
+  {
+    std::vector<int> queue;
+    int dmin = INT_MAX;
+    for (int v = 0; v < n; v++)
+      dmin = std::min(dmin, xadj[v + 1] - xadj[v]);
+    std::vector<int> low;
+    for (int v = 0; v < n; v++)
+      if (xadj[v + 1] - xadj[v] == dmin)
+        low.push_back(v);
+    std::vector<int> d, mind;
+    bfs_dist(n, xadj, adj, low[0], d, queue);
+    bool connected = (int)queue.size() == n;
+    if (connected) {
+      dist.push_back(d);
+      mind = d;
+      while (dist.size() < 8) {
+        int best = -1;
+        for (int v : low)
+          if (best < 0 || mind[v] > mind[best])
+            best = v;
+        if (best < 0 || mind[best] == 0)
+          break;
+        bfs_dist(n, xadj, adj, best, d, queue);
+        dist.push_back(d);
+        for (int v = 0; v < n; v++)
+          mind[v] = std::min(mind[v], d[v]);
+      }
+    }
+    const int L = (int)dist.size();
+    for (int a = 0; a < L; a++)
+      for (int b = a + 1; b < L; b++) {
+        const std::vector<int> &da = dist[a], &db = dist[b];
+        long long pos = 0, neg = 0;
+        for (int i = 0; i < n && !(pos && neg); i++)
+          for (int k = dep_ptr[i] - base; k < dep_ptr[i + 1] - base; k++) {
+            const int j = dep_col[k] - base;
+            const int df = (da[i] - db[i]) - (da[j] - db[j]);
+            pos += df > 0;
+            neg += df < 0;
+          }
+        if ((pos == 0) == (neg == 0))
+          continue; // not monotone, or constant along every edge
+        int lo = INT_MAX, hi = INT_MIN;
+        for (int v = 0; v < n; v++) {
+          const int f = da[v] - db[v];
+          lo = std::min(lo, f);
+          hi = std::max(hi, f);
+        }
+        cands.push_back({a, b, pos > 0 ? 1 : -1, (long long)hi - lo});
+      }
+    int lo = INT_MAX, hi = INT_MIN;
+    for (int v = 0; v < n; v++) {
+      lo = std::min(lo, lvl[v]);
+      hi = std::max(hi, lvl[v]);
+    }
+    cands.push_back({-1, -1, 1, (long long)hi - lo});
+    std::stable_sort(cands.begin(), cands.end(),
+                     [](const Cand &x, const Cand &y) { return x.range < y.range; });
+  }
+  // greedy selection: narrowest first, each with a Gram-Schmidt residual of
+  // at least half its norm against those already chosen
+  for (const Cand &c : cands) {
+    if (coords.size() == 3)
+      break;
+    std::vector<int> f(n);
+    for (int v = 0; v < n; v++)
+      f[v] = c.a < 0 ? lvl[v] : c.sign * (dist[c.a][v] - dist[c.b][v]);
+    double mean = 0, var = 0;
+    for (int v = 0; v < n; v++)
+      mean += f[v];
+    mean /= n;
+    for (int v = 0; v < n; v++)
+      var += (f[v] - mean) * (f[v] - mean);
+    var /= n;
+    if (var <= 0)
+      continue;
+    const double sd = std::sqrt(var);
+    std::vector<double> r(n);
+    for (int v = 0; v < n; v++)
+      r[v] = (f[v] - mean) / sd;
+    for (const std::vector<double> &q : basis) {
+      double dot = 0;
+      for (int v = 0; v < n; v++)
+        dot += r[v] * q[v];
+      dot /= n;
+      for (int v = 0; v < n; v++)
+        r[v] -= dot * q[v];
+    }
+    double nr = 0;
+    for (int v = 0; v < n; v++)
+      nr += r[v] * r[v];
+    nr = std::sqrt(nr / n);
+    if (nr < 0.5)
+      continue;
+    for (int v = 0; v < n; v++)
+      r[v] /= nr;
+    basis.push_back(std::move(r));
+    coords.push_back(std::move(f));
+  }
+  dist.clear();
+  basis.clear();
+
+  // k-d tree of value-threshold cuts
+  std::vector<int> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  struct Task {
+    int lo, hi, k, p0;
+  };
+  std::vector<Task> stack{{0, n, std::max(1, nparts), 0}};
+  std::vector<long long> hist;
+  while (!stack.empty()) {
+    const Task t = stack.back();
+    stack.pop_back();
+    if (t.k == 1 || t.hi - t.lo <= 1) {
+      for (int q = t.lo; q < t.hi; q++)
+        part[order[q]] = t.p0;
+      // a single row split further leaves parts empty
+      continue;
+    }
+    const int k1 = t.k / 2;
+    const long long want = (long long)(t.hi - t.lo) * k1 / t.k;
+    // coordinates by span, widest first; take the first that splits
+    std::vector<std::pair<long long, int>> spans;
+    for (int a = 0; a < (int)coords.size(); a++) {
+      int lo = INT_MAX, hi = INT_MIN;
+      for (int q = t.lo; q < t.hi; q++) {
+        const int f = coords[a][order[q]];
+        lo = std::min(lo, f);
+        hi = std::max(hi, f);
+      }
+      spans.push_back({(long long)hi - lo, a});
+    }
+    std::sort(spans.begin(), spans.end(), [](auto &x, auto &y) { return x.first > y.first; });
+    int cut = -1;
+    for (const auto &sa : spans) {
+      if (sa.first == 0)
+        break;
+      const std::vector<int> &f = coords[sa.second];
+      int lo = INT_MAX;
+      for (int q = t.lo; q < t.hi; q++)
+        lo = std::min(lo, f[order[q]]);
+      // histogram of the node's values; the threshold keeps f < thr low
+      hist.assign((size_t)sa.first + 2, 0);
+      for (int q = t.lo; q < t.hi; q++)
+        hist[f[order[q]] - lo]++;
+      long long below = 0, bdev = LLONG_MAX;
+      int thr = 0;
+      bool found = false;
+      for (size_t v = 1; v < hist.size(); v++) {
+        below += hist[v - 1];
+        if (hist[v] == 0 && v + 1 < hist.size())
+          continue; // only thresholds just below a present value
+        const long long dev = std::llabs(below - want);
+        if (below > 0 && below < t.hi - t.lo && dev < bdev) {
+          bdev = dev;
+          thr = lo + (int)v;
+          found = true;
+        }
+      }
+      if (!found)
+        continue;
+      const auto mid = std::stable_partition(order.begin() + t.lo, order.begin() + t.hi,
+                                             [&](int v) { return f[v] < thr; });
+      cut = (int)(mid - order.begin());
+      break;
+    }
+    if (cut < 0) { // no coordinate separates these rows: keep them together
+      for (int q = t.lo; q < t.hi; q++)
+        part[order[q]] = t.p0;
+      continue;
+    }
+    stack.push_back({cut, t.hi, t.k - k1, t.p0 + k1});
+    stack.push_back({t.lo, cut, k1, t.p0});
+  }
+  return (int)coords.size();
+}
+
+} // namespace la

@@ -1,5 +1,5 @@
-// la_trsv.cu -- level-scheduled sparse triangular solve, one persistent
-// kernel per solve.
+// la_trsv.cu -- level-scheduled sparse triangular solve, one kernel launch
+// per solve.
 //
 // Reference: OptimizedTriangularSolve<Barrier, L|U> (sparse_mat_op/
 // triangle_solve.hpp:149-208, triangle_solve.tpp:17-155).  analysis()
@@ -9,22 +9,39 @@
 // barrier after each one and computes
 //   x[i] = diag ? (b[i] - sum_j T_ij x[j]) / diag[i] : b[i] - sum_j T_ij x[j].
 //
-// B200 design.  The same host analysis (bit-identical level sets) stores
-// the rows in level order and cuts every level into 32-row chunks, so a
-// chunk never straddles a level.  One launch of a persistent grid walks all
-// levels: warps claim chunks in order from an atomic ticket, one lane per
-// row.  Instead of a grid barrier per level, each lane waits only for the x
-// entries its row reads: x is pre-filled with a sentinel NaN bit pattern and
-// a finished row publishes x[i] with a device-scope store, so a dependency
-// is ready when its x entry stops being the sentinel (the value is its own
-// flag; one L2 round trip).  Because chunks are claimed in level order, the
-// lowest unfinished chunk always has its inputs ready and the solve cannot
-// deadlock.  Waiting lanes back off with nanosleep; every wait is bounded by
-// the global timer, and on expiry the kernel records a timeout in the plan's
-// error word and all warps leave.
+// B200 design.  The same host analysis (bit-identical level sets) feeds one
+// of two schedules, both computing every x_i with the reference's exact
+// operations in stored column order (so the results are bit-identical):
 //
-// Roofline: latency-bound at these sizes (one dependent L2 round trip per
-// level); algorithmic bytes per solve
+// Level order (schedule 0).  Rows are stored in level order and cut into
+// 32-row chunks that never straddle a level.  One launch of a persistent
+// grid walks all levels: warps claim chunks in order from an atomic ticket,
+// one lane per row.  Instead of a grid barrier per level, each lane waits
+// only for the x entries its row reads: x is pre-filled with a sentinel NaN
+// bit pattern and a finished row publishes x[i] with a device-scope store,
+// so a dependency is ready when its x entry stops being the sentinel (the
+// value is its own flag; one L2 round trip).  Because chunks are claimed in
+// level order, the lowest unfinished chunk always has its inputs ready and
+// the solve cannot deadlock.
+//
+// Partitioned (schedule 1).  The rows are split into parts whose dependency
+// graph is acyclic and shallow (la_partition.cpp), one co-resident CTA per
+// part (cooperative launch).  A CTA walks the levels present in its part with
+// one __syncthreads per level and keeps its rows' x values in shared memory,
+// so a dependency inside the part is a shared-memory read; a dependency on
+// another part is awaited in global memory as above.  A dependency path
+// crosses few part boundaries, so most of the per-level cost is a
+// shared-memory step instead of an L2 round trip.  No deadlock: every CTA is
+// resident and processes its rows in level order, so the unfinished row of
+// lowest level always has its inputs ready.  The analysis models both
+// schedules' critical paths and keeps the partitioned one when it is clearly
+// shorter.
+//
+// Every wait is bounded by the global timer; on expiry the kernel records a
+// timeout in the plan's error word and all warps leave.
+//
+// Roofline: latency-bound at these sizes (levels x per-level step); the
+// algorithmic bytes per solve are
 //   nnz*(sizeof(V)+4) + (n+1)*4 + n*4 [exec->row map] + n*sizeof(V) [diag]
 //   + n*sizeof(X) [b] + n*sizeof(X) [x].
 
@@ -34,6 +51,8 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <numeric>
+#include <vector>
 
 namespace la {
 namespace {
@@ -261,6 +280,197 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// ---------------------------------------------------------------- parts
+// Partitioned schedule.  The rows are split into compact parts (recursive
+// BFS bisection of the triangle's graph), one CTA per part, all CTAs
+// co-resident (cooperative launch).  A CTA walks the levels present in its
+// part in increasing order, one __syncthreads per level, and keeps the x
+// values of its own rows in shared memory: a dependency inside the part costs
+// a shared-memory read, and only a dependency on another part goes through
+// global memory, where it is awaited as in the level-order schedule (the
+// sentinel value is its own flag, waits bounded by the global timer).  A
+// dependency path crosses each part boundary at most once, so the critical
+// path is the number of levels times a shared-memory step plus a few global
+// hand-offs, instead of the number of levels times an L2 round trip.
+// No deadlock: every CTA is resident and processes its rows in level order,
+// so the unfinished row of lowest level always has its inputs ready.
+constexpr int kEmptySlot = 0x7fffffff; // column of an unused slot
+
+// threads per CTA: four prefetched rows live in registers
+template <typename X, int KD> constexpr int part_threads() {
+  return KD <= 4 ? 512 : 256;
+}
+
+template <typename X, int KD> struct PartRow {
+  int r, i; // execution position (-1: none) and original row
+  int j[KD];
+  X a[KD];
+  X dg;
+  X xr[KD]; // values of other parts' rows, loaded ahead
+};
+
+// Nothing but shared-memory reads, arithmetic and the barrier may sit on a
+// level's critical path, so everything global is fetched ahead:
+//  * the part's level boundaries and the b values of its rows are staged in
+//    shared memory at kernel start (row r's x slot holds b until row r
+//    overwrites it with x);
+//  * the first KD entries of every row are stored slot-major by execution
+//    position (ej[s*n + r], ev[s*n + r]; kEmptySlot marks an unused slot), so
+//    a thread's row is one coalesced load per slot; every thread fetches its
+//    first row of level q+3 while it solves level q (four register sets);
+//  * at the end of level q it issues the loads of the other parts' values
+//    that its level-(q+2) row reads -- two levels after that row's columns
+//    were requested, so the addresses are there -- and only re-reads (waits
+//    for) those that were not yet published when it gets to them.
+// Entries beyond KD (only when some row is longer than 16) come from the CSR
+// copy, and rows beyond the first per thread in levels wider than the CTA
+// are loaded when reached.
+template <typename V, typename X, bool UNIT, int KD>
+__global__ void __launch_bounds__(part_threads<X, KD>(), 1)
+    trsv_part_kernel(const int n, const int *__restrict__ pstart,
+                     const int *__restrict__ psub, const int *__restrict__ sb,
+                     const int *__restrict__ ai, const int *__restrict__ aj,
+                     const V *__restrict__ av, const int *__restrict__ ej,
+                     const V *__restrict__ ev, const V *__restrict__ diag,
+                     const int *__restrict__ exec_row, const X *__restrict__ b, X *x,
+                     int *err, const int tail, const int rows_cap) {
+  constexpr int T = part_threads<X, KD>();
+  extern __shared__ __align__(16) unsigned char part_smem[];
+  X *xs = reinterpret_cast<X *>(part_smem);
+  int *ssb = reinterpret_cast<int *>(xs + rows_cap); // level boundaries
+  const int p = blockIdx.x, tid = threadIdx.x;
+  const int P0 = __ldg(pstart + p), P1 = __ldg(pstart + p + 1);
+  const int q0 = __ldg(psub + p), q1 = __ldg(psub + p + 1);
+  const unsigned long long t0 = global_ns();
+  int aborted = 0; // this thread gave up on a wait (or saw another give up)
+
+  auto load_row = [&](int r, PartRow<X, KD> &R) {
+    R.r = r;
+    R.i = __ldg(exec_row + r);
+#pragma unroll
+    for (int s = 0; s < KD; s++) {
+      R.j[s] = __ldg(ej + (size_t)s * n + r);
+      R.a[s] = X(__ldg(ev + (size_t)s * n + r));
+    }
+    R.dg = UNIT ? X(1) : X(__ldg(diag + r));
+  };
+  auto prefetch = [&](int q, PartRow<X, KD> &R) {
+    R.r = -1;
+    if (q < q1) {
+      const int r = ssb[q - q0] + tid;
+      if (r < ssb[q - q0 + 1])
+        load_row(r, R);
+    }
+  };
+  auto arm = [&](PartRow<X, KD> &R) {
+    if (R.r >= 0) {
+#pragma unroll
+      for (int s = 0; s < KD; s++)
+        if (R.j[s] >= 0 && R.j[s] != kEmptySlot)
+          R.xr[s] = dev::ld_relaxed(x + R.j[s]);
+    }
+  };
+  // a value of another part: wait (bounded) until it stops being the sentinel
+  auto await = [&](int c, X v) {
+    for (unsigned pass = 1; Sentinel<X>::is(v) && !aborted; pass++) {
+      if ((pass & 63u) == 0u && (dev::ld_relaxed(err) != 0 || global_ns() - t0 > kWaitNs)) {
+        atomicExch(err, 1);
+        aborted = 1;
+      }
+      v = dev::ld_relaxed(x + c);
+    }
+    return v;
+  };
+  auto solve_row = [&](const PartRow<X, KD> &R, bool armed) {
+    const X bi = xs[R.r - P0];
+    X sum = X(0);
+#pragma unroll
+    for (int s = 0; s < KD; s++)
+      if (R.j[s] != kEmptySlot) {
+        const int c = R.j[s];
+        const X v = c < 0 ? xs[-1 - c] : await(c, armed ? R.xr[s] : dev::ld_relaxed(x + c));
+        sum = add_rn(sum, mul_rn(R.a[s], v));
+      }
+    if (tail) {
+      const int k1 = __ldg(ai + R.r + 1);
+      for (int k = __ldg(ai + R.r) + KD; k < k1; k++) {
+        const int c = __ldg(aj + k);
+        const X v = c < 0 ? xs[-1 - c] : await(c, dev::ld_relaxed(x + c));
+        sum = add_rn(sum, mul_rn(X(__ldg(av + k)), v));
+      }
+    }
+    X xi = sub_rn(bi, sum);
+    if (!UNIT)
+      xi = div_rn(xi, R.dg);
+    xs[R.r - P0] = xi;
+    dev::st_relaxed(x + R.i, Sentinel<X>::scrub(xi));
+  };
+  auto run_level = [&](int q, const PartRow<X, KD> &R) {
+    if (R.r < 0)
+      return;
+    solve_row(R, true);
+    const int e = ssb[q - q0 + 1];
+    for (int r = R.r + T; r < e; r += T) { // levels wider than the CTA
+      PartRow<X, KD> S;
+      load_row(r, S);
+      solve_row(S, false);
+    }
+  };
+
+  for (int q = q0 + tid; q <= q1; q += T)
+    ssb[q - q0] = __ldg(sb + q);
+  __syncthreads();
+  PartRow<X, KD> R0, R1, R2, R3;
+  prefetch(q0, R0);
+  prefetch(q0 + 1, R1);
+  prefetch(q0 + 2, R2);
+  // b of the part's rows into their x slots, 16 rows per thread per batch
+  // (all row indices, then all b values, in flight together)
+  constexpr int kStage = 16;
+  for (int r0 = P0 + tid; r0 < P1; r0 += kStage * T) {
+    int ii[kStage];
+    X bv[kStage];
+#pragma unroll
+    for (int u = 0; u < kStage; u++)
+      ii[u] = r0 + u * T < P1 ? __ldg(exec_row + r0 + u * T) : -1;
+#pragma unroll
+    for (int u = 0; u < kStage; u++)
+      bv[u] = ii[u] >= 0 ? __ldg(b + ii[u]) : X(0);
+#pragma unroll
+    for (int u = 0; u < kStage; u++)
+      if (ii[u] >= 0)
+        xs[r0 + u * T - P0] = bv[u];
+  }
+  __syncthreads();
+  arm(R0);
+  arm(R1);
+  // four register sets rotate: level q runs while q+3 is fetched and q+2 is
+  // armed; one barrier per level, and every thread leaves together if any
+  // gave up
+  for (int q = q0; q < q1; q += 4) {
+    prefetch(q + 3, R3);
+    run_level(q, R0);
+    arm(R2);
+    if (__syncthreads_or(aborted) || q + 1 >= q1)
+      break;
+    prefetch(q + 4, R0);
+    run_level(q + 1, R1);
+    arm(R3);
+    if (__syncthreads_or(aborted) || q + 2 >= q1)
+      break;
+    prefetch(q + 5, R1);
+    run_level(q + 2, R2);
+    arm(R0);
+    if (__syncthreads_or(aborted) || q + 3 >= q1)
+      break;
+    prefetch(q + 6, R2);
+    run_level(q + 3, R3);
+    arm(R1);
+    if (__syncthreads_or(aborted))
+      break;
+  }
+}
+
 template <typename V, typename X, bool UNIT>
 void launch_kernel(la_trsv_plan_t P, const X *b, X *x, cudaStream_t st) {
   const int *cs = P->chunk_start.as<int>(), *ai = P->ai.as<int>(),
@@ -287,11 +497,51 @@ void launch_kernel(la_trsv_plan_t P, const X *b, X *x, cudaStream_t st) {
   }
 }
 
+template <typename V, typename X, bool UNIT, int KD>
+const void *part_fn() {
+  return (const void *)trsv_part_kernel<V, X, UNIT, KD>;
+}
+
+template <typename V, typename X, bool UNIT, int KD>
+cudaError_t launch_parts_kd(la_trsv_plan_t P, const X *b, X *x, cudaStream_t st) {
+  const int n = P->n, tail = P->kd == 0;
+  const int *ps = P->pstart.as<int>(), *pq = P->psub.as<int>(), *sb = P->sb.as<int>(),
+            *ai = P->ai.as<int>(), *aj = P->aj.as<int>(), *ej = P->ej.as<int>(),
+            *er = P->exec_row.as<int>();
+  const V *av = P->av.as<V>(), *ev = P->ev.as<V>(), *dg = P->diag.as<V>();
+  int *err = P->err.as<int>();
+  const int cap = P->part_rows;
+  void *args[] = {(void *)&n,  (void *)&ps, (void *)&pq, (void *)&sb,  (void *)&ai,
+                  (void *)&aj, (void *)&av, (void *)&ej, (void *)&ev,  (void *)&dg,
+                  (void *)&er, (void *)&b,  (void *)&x,  (void *)&err, (void *)&tail,
+                  (void *)&cap};
+  return cudaLaunchCooperativeKernel(part_fn<V, X, UNIT, KD>(), dim3(P->nparts),
+                                     dim3(part_threads<X, KD>()), args, P->part_smem, st);
+}
+
+template <typename V, typename X, bool UNIT>
+cudaError_t launch_parts(la_trsv_plan_t P, const X *b, X *x, cudaStream_t st) {
+  switch (P->kd) {
+  case 4:
+    return launch_parts_kd<V, X, UNIT, 4>(P, b, x, st);
+  case 8:
+    return launch_parts_kd<V, X, UNIT, 8>(P, b, x, st);
+  default: // 16 slots; longer rows finish from the CSR tail
+    return launch_parts_kd<V, X, UNIT, 16>(P, b, x, st);
+  }
+}
+
 template <typename V, typename X>
 la_status launch_typed(la_trsv_plan_t P, const X *b, X *x, cudaStream_t st) {
   if (P->n == 0)
     return LA_OK;
   LA_CUDA_TRY(cudaMemsetAsync(x, 0xff, sizeof(X) * (size_t)P->n, st));
+  if (P->sched == 1) {
+    const cudaError_t e = P->unit ? launch_parts<V, X, true>(P, b, x, st)
+                                  : launch_parts<V, X, false>(P, b, x, st);
+    LA_CUDA_TRY(e);
+    return LA_OK;
+  }
   LA_CUDA_TRY(cudaMemsetAsync(P->ticket.p, 0, sizeof(int), st));
   if (P->unit)
     launch_kernel<V, X, true>(P, b, x, st);
@@ -346,6 +596,228 @@ la_status trsv_launch(la_trsv_plan_t P, const void *b, void *x,
   return launch_typed<float, float>(P, (const float *)b, (float *)x, st);
 }
 
+// Partitioned layout (schedule 1).  Leaves the plan untouched and reports
+// *ok = false when the parts would not fit in shared memory or the device
+// cannot keep one CTA per part resident.
+template <typename X>
+la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const double *av,
+                      const double *diag, bool force, bool *ok) {
+  *ok = false;
+  const int n = P->n, base = P->base, nnz = P->nnz;
+  int dev = 0, optin = 0;
+  LA_CUDA_TRY(cudaGetDevice(&dev));
+  LA_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  const int cap = (optin - 1024) / (int)sizeof(X);
+  int nparts = std::min(sm_count(), std::max(1, (n + 2047) / 2048));
+  if (const char *e = std::getenv("LA_TRSV_PARTS")) // tuning override
+    nparts = std::max(1, std::min(sm_count(), std::atoi(e)));
+  if ((long long)nparts * cap < (long long)n + n / 16)
+    return LA_OK;
+  // rows' levels, and the triangle's graph made undirected
+  std::vector<int> lvl(n);
+  for (int l = 0; l < P->levels; l++)
+    for (int p = P->h_prefix[l]; p < P->h_prefix[l + 1]; p++)
+      lvl[P->h_iperm[p] - base] = l;
+  std::vector<int> xadj(n + 1, 0), adj(2 * (size_t)nnz);
+  for (int i = 0; i < n; i++)
+    for (int k = ai[i] - base; k < ai[i + 1] - base; k++) {
+      xadj[i + 1]++;
+      xadj[aj[k] - base + 1]++;
+    }
+  std::partial_sum(xadj.begin(), xadj.end(), xadj.begin());
+  {
+    std::vector<int> fill(xadj.begin(), xadj.end() - 1);
+    for (int i = 0; i < n; i++)
+      for (int k = ai[i] - base; k < ai[i + 1] - base; k++) {
+        const int j = aj[k] - base;
+        adj[fill[i]++] = j;
+        adj[fill[j]++] = i;
+      }
+  }
+  std::vector<int> part(n);
+  monotone_partition(n, xadj.data(), adj.data(), ai, aj, base, lvl.data(), nparts, part.data());
+  std::vector<int> pstart(nparts + 1, 0);
+  for (int i = 0; i < n; i++)
+    pstart[part[i] + 1]++;
+  int rows_max = 0;
+  for (int p = 0; p < nparts; p++)
+    rows_max = std::max(rows_max, pstart[p + 1]);
+  if (rows_max > cap)
+    return LA_OK;
+  std::partial_sum(pstart.begin(), pstart.end(), pstart.begin());
+  // register slots from the longest row (16 plus the CSR tail beyond)
+  int longest = 0;
+  for (int i = 0; i < n; i++)
+    longest = std::max(longest, ai[i + 1] - ai[i]);
+  const int kd = longest <= 4 ? 4 : longest <= 8 ? 8 : longest <= 16 ? 16 : 0;
+  const int ks = kd ? kd : 16;
+  // the device must hold one CTA per part with this much shared memory
+  // levels per part (their boundaries are staged in shared memory too)
+  int subs_max = 0;
+  {
+    std::vector<int> last(nparts, -1), subs(nparts, 0);
+    for (int q = 0; q < n; q++) {
+      const int i = P->h_iperm[q] - base;
+      if (last[part[i]] != lvl[i]) {
+        last[part[i]] = lvl[i];
+        subs_max = std::max(subs_max, ++subs[part[i]]);
+      }
+    }
+  }
+  const size_t smem = sizeof(X) * (size_t)rows_max + sizeof(int) * ((size_t)subs_max + 1);
+  if (smem + 1024 > (size_t)optin)
+    return LA_OK;
+  const void *fns[2];
+  int threads = 0;
+  if (ks == 4) {
+    fns[0] = part_fn<X, X, false, 4>(), fns[1] = part_fn<X, X, true, 4>();
+    threads = part_threads<X, 4>();
+  } else if (ks == 8) {
+    fns[0] = part_fn<X, X, false, 8>(), fns[1] = part_fn<X, X, true, 8>();
+    threads = part_threads<X, 8>();
+  } else {
+    fns[0] = part_fn<X, X, false, 16>(), fns[1] = part_fn<X, X, true, 16>();
+    threads = part_threads<X, 16>();
+  }
+  for (const void *f : fns) {
+    // the limit is per kernel, shared by every plan: allow the device's
+    // maximum once, so that a smaller plan never lowers a larger plan's limit
+    if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      return LA_OK;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, threads, smem) !=
+            cudaSuccess ||
+        (long long)per_sm * sm_count() < nparts) {
+      cudaGetLastError();
+      return LA_OK;
+    }
+  }
+  // Modelled critical path (microseconds; B200 measurements): a part takes
+  // ~0.35 us per level it holds plus ~1 us for every further round of rows
+  // in a level wider than its CTA, and a value crossing parts arrives
+  // ~1.5 us after it is written; the level-order schedule takes ~2 us per
+  // level.  The partition is used when it models at most 0.8 of that.
+  if (!force) {
+    std::vector<double> ready(n), last(nparts, 0.0), fin(nparts, 0.0);
+    std::vector<int> width(nparts, 0), touched;
+    for (int l = 0; l < P->levels; l++) {
+      touched.clear();
+      for (int q = P->h_prefix[l]; q < P->h_prefix[l + 1]; q++) {
+        const int i = P->h_iperm[q] - base, pi = part[i];
+        double t = 0;
+        for (int k = ai[i] - base; k < ai[i + 1] - base; k++) {
+          const int j = aj[k] - base;
+          t = std::max(t, ready[j] + (part[j] != pi ? 1.5 : 0.0));
+        }
+        if (width[pi]++ == 0) {
+          touched.push_back(pi);
+          fin[pi] = last[pi];
+        }
+        fin[pi] = std::max(fin[pi], t);
+      }
+      for (int p : touched)
+        fin[p] += 0.35 + 1.0 * ((width[p] + threads - 1) / threads - 1);
+      for (int q = P->h_prefix[l]; q < P->h_prefix[l + 1]; q++) {
+        const int i = P->h_iperm[q] - base;
+        ready[i] = fin[part[i]];
+      }
+      for (int p : touched) {
+        last[p] = fin[p];
+        width[p] = 0;
+      }
+    }
+    double est = 0;
+    for (int p = 0; p < nparts; p++)
+      est = std::max(est, last[p]);
+    if (est > 0.8 * 2.0 * P->levels)
+      return LA_OK;
+  }
+  // execution order: part-major, level order inside a part
+  std::vector<int> erow(n), pos(n);
+  {
+    std::vector<int> fill(pstart.begin(), pstart.end() - 1);
+    for (int p = 0; p < n; p++) {
+      const int i = P->h_iperm[p] - base, r = fill[part[i]]++;
+      erow[r] = i;
+      pos[i] = r;
+    }
+  }
+  std::vector<int> sb, psub(nparts + 1);
+  for (int p = 0; p < nparts; p++) {
+    psub[p] = (int)sb.size();
+    for (int r = pstart[p]; r < pstart[p + 1]; r++)
+      if (r == pstart[p] || lvl[erow[r]] != lvl[erow[r - 1]])
+        sb.push_back(r);
+  }
+  psub[nparts] = (int)sb.size();
+  sb.push_back(n);
+  // encoded columns (-1 - position in the part for the part's own rows),
+  // first ks entries slot-major, all entries in CSR for rows beyond ks
+  const size_t cells = (size_t)ks * n;
+  std::vector<int> ej(cells, kEmptySlot);
+  std::vector<double> ev(cells, 0.0), ediag(n, 1.0);
+  std::vector<int> eai, eaj;
+  std::vector<double> eav;
+  if (!kd) {
+    eai.assign(n + 1, 0);
+    eaj.resize(std::max(nnz, 1));
+    eav.resize(std::max(nnz, 1));
+  }
+  int w = 0;
+  for (int r = 0; r < n; r++) {
+    const int i = erow[r], pi = part[i];
+    if (diag)
+      ediag[r] = diag[i];
+    for (int k = ai[i] - base, s = 0; k < ai[i + 1] - base; k++, s++, w++) {
+      const int j = aj[k] - base;
+      const int c = part[j] == pi ? -1 - (pos[j] - pstart[pi]) : j;
+      if (s < ks) {
+        ej[(size_t)s * n + r] = c;
+        ev[(size_t)s * n + r] = av[k];
+      }
+      if (!kd) {
+        eaj[w] = c;
+        eav[w] = av[k];
+      }
+    }
+    if (!kd)
+      eai[r + 1] = w;
+  }
+  if (!kd) {
+    LA_TRY(P->ai.upload(eai.data(), sizeof(int) * eai.size()));
+    LA_TRY(P->aj.upload(eaj.data(), sizeof(int) * eaj.size()));
+  }
+  LA_TRY(P->ej.upload(ej.data(), sizeof(int) * cells));
+  LA_TRY(P->exec_row.upload(erow.data(), sizeof(int) * erow.size()));
+  LA_TRY(P->pstart.upload(pstart.data(), sizeof(int) * pstart.size()));
+  LA_TRY(P->psub.upload(psub.data(), sizeof(int) * psub.size()));
+  LA_TRY(P->sb.upload(sb.data(), sizeof(int) * sb.size()));
+  if (P->dtype == LA_F64) {
+    if (!kd)
+      LA_TRY(P->av.upload(eav.data(), sizeof(double) * eav.size()));
+    LA_TRY(P->ev.upload(ev.data(), sizeof(double) * cells));
+    LA_TRY(P->diag.upload(ediag.data(), sizeof(double) * n));
+  } else {
+    if (!kd) {
+      std::vector<float> f(eav.begin(), eav.end());
+      LA_TRY(P->av.upload(f.data(), sizeof(float) * f.size()));
+    }
+    std::vector<float> f(ev.begin(), ev.end()), fd(ediag.begin(), ediag.end());
+    LA_TRY(P->ev.upload(f.data(), sizeof(float) * cells));
+    LA_TRY(P->diag.upload(fd.data(), sizeof(float) * n));
+  }
+  P->kd = kd;
+  P->nparts = nparts;
+  P->part_rows = rows_max;
+  P->part_smem = smem;
+  P->sched = 1;
+  *ok = true;
+  return LA_OK;
+}
+
 // Analysis: TopologicalSort2 levels, rows in execution order, 32-row chunks
 // that never cross a level (triangle_solve.tpp:17-113 equivalent).
 // A caller-supplied level structure (iperm/prefix as TopologicalSort2
@@ -368,6 +840,38 @@ la_status trsv_build(la_trsv_plan_t P, const int *ai, const int *aj,
   }
   if (n == 0)
     return LA_OK;
+  LA_TRY(P->err.alloc(sizeof(int)));
+  LA_CUDA_TRY(cudaMemset(P->err.p, 0, sizeof(int)));
+  LA_TRY(P->ticket.alloc(sizeof(int)));
+  // The partitioned schedule needs true level sets: every row reads only
+  // rows of earlier levels (TopologicalSort2's are by construction; a
+  // caller-built structure is checked here and otherwise keeps the
+  // level-order schedule, whose bounded waits report a broken order).
+  bool exact = true;
+  if (iperm) {
+    std::vector<int> lvl(n);
+    for (int l = 0; l < P->levels; l++)
+      for (int p = P->h_prefix[l]; p < P->h_prefix[l + 1]; p++)
+        lvl[P->h_iperm[p] - base] = l;
+    for (int i = 0; i < n && exact; i++)
+      for (int k = ai[i] - base; k < ai[i + 1] - base; k++)
+        if (lvl[aj[k] - base] >= lvl[i]) {
+          exact = false;
+          break;
+        }
+  }
+  // LA_TRSV_SCHEDULE=flags keeps the level-order schedule, =parts takes the
+  // partitioned one whenever it fits (both compute bit-identical results)
+  const char *sched_env = std::getenv("LA_TRSV_SCHEDULE");
+  const bool want_parts = exact && !(sched_env && std::strcmp(sched_env, "flags") == 0);
+  const bool force_parts = sched_env && std::strcmp(sched_env, "parts") == 0;
+  if (want_parts) {
+    bool ok = false;
+    LA_TRY(P->dtype == LA_F64 ? build_parts<double>(P, ai, aj, av, diag, force_parts, &ok)
+                              : build_parts<float>(P, ai, aj, av, diag, force_parts, &ok));
+    if (ok)
+      return LA_OK;
+  }
   std::vector<int> eai(n + 1), erow(n), cstart;
   std::vector<int> eaj(std::max(P->nnz, 1));
   std::vector<double> eav(std::max(P->nnz, 1)), ediag(n, 1.0);
@@ -407,9 +911,6 @@ la_status trsv_build(la_trsv_plan_t P, const int *ai, const int *aj,
     LA_TRY(P->diag.upload(fd.data(), sizeof(float) * n));
     P->grid = grid_for<float, float>(P->nchunks, P->kd);
   }
-  LA_TRY(P->err.alloc(sizeof(int)));
-  LA_CUDA_TRY(cudaMemset(P->err.p, 0, sizeof(int)));
-  LA_TRY(P->ticket.alloc(sizeof(int)));
   return LA_OK;
 }
 

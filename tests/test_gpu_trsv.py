@@ -184,3 +184,65 @@ def test_trsv_levels_validation(lab):
     with pytest.raises(lab.LAError):  # prefix does not end at n
         lab.OptimizedTriangularSolve("L").analysis_levels(
             8, 0, ai, aj, av, np.arange(8, dtype=np.int32), np.array([0, 7], np.int32))
+
+
+def _long_rows_lower(n, seed):
+    """Strict lower triangle with a few rows longer than 16 entries (the
+    partitioned schedule's CSR tail) and some empty rows."""
+    r = np.random.default_rng(seed)
+    rows = []
+    for i in range(n):
+        k = 0 if i % 7 == 3 else (int(r.integers(17, 40)) if i % 97 == 50 else int(r.integers(0, 5)))
+        k = min(k, i)
+        rows.append(np.sort(r.choice(i, k, replace=False)) if k else np.zeros(0, np.int64))
+    ai = np.concatenate([[0], np.cumsum([len(c) for c in rows])]).astype(np.int32)
+    aj = (np.concatenate(rows) if ai[-1] else np.zeros(0)).astype(np.int32)
+    return ai, aj, r.uniform(-0.3, 0.3, int(ai[-1]))
+
+
+@pytest.mark.parametrize("schedule", ["parts", "flags"])
+def test_trsv_schedules_bit_identical(lab, orc, monkeypatch, schedule):
+    """Both schedules -- level order with per-row readiness, and the
+    partitioned one (co-resident CTAs, part values in shared memory) --
+    give the oracle's level solve bit for bit, in both triangles and both
+    storage precisions, including rows longer than the register slots and a
+    forced small part count (many cross-part waits)."""
+    from linearalgebra_b200 import gen
+    P = orc.ptr
+    monkeypatch.setenv("LA_TRSV_SCHEDULE", schedule)
+    cases = []
+    for n, ai, aj, av in (gen.laplacian_3d(40), gen.stencil27(16), gen.aniso7(28, seed=3)):
+        _, lt, ut, d = _ic_factor_rcm(lab, n, ai, aj, av)
+        cases += [(n, "L", lt, d), (n, "U", ut, d)]
+    n = 30_000
+    cases.append((n, "L", _long_rows_lower(n, 1), np.random.default_rng(2).uniform(1, 2, n)))
+    for parts in (None, "3"):
+        if parts:
+            monkeypatch.setenv("LA_TRSV_PARTS", parts)
+        for n, uplo, (c_ai, c_aj, c_av), d in cases:
+            b = np.random.default_rng(n).uniform(-1, 1, n)
+            ts, x = solve(lab, uplo, n, c_ai, c_aj, c_av, d, b)
+            assert ts.schedule()[0] == ("parts" if schedule == "parts" else "levels")
+            lv, ip, pf = ts.levels()
+            ref = np.zeros(n)
+            orc.port().oracle_level_solve(lv, P(ip), P(pf), 0, P(c_ai), P(c_aj), P(c_av),
+                                          P(d), P(b), P(ref))
+            assert np.array_equal(x, ref), (n, uplo, schedule, parts)
+            ts32, x32 = solve(lab, uplo, n, c_ai, c_aj, c_av, d, b, dtype=np.float32)
+            assert rel(x32, ref) <= 1e-4
+            monkeypatch.setenv("LA_TRSV_SCHEDULE", "flags" if schedule == "parts" else "parts")
+            _, y32 = solve(lab, uplo, n, c_ai, c_aj, c_av, d, b, dtype=np.float32)
+            monkeypatch.setenv("LA_TRSV_SCHEDULE", schedule)
+            assert np.array_equal(x32, y32), (n, uplo, "fp32 schedules differ")
+
+
+def test_trsv_partitioned_is_chosen_for_3d_ic0(lab):
+    """The analysis picks the partitioned schedule for the RCM-ordered IC(0)
+    factor of the 128^3 Laplacian (the preconditioner of the PCG workload)."""
+    from linearalgebra_b200 import gen
+    n, ai, aj, av = gen.laplacian_3d(128)
+    _, (t_ai, t_aj, t_av), _, d = _ic_factor_rcm(lab, n, ai, aj, av)
+    for dt in (np.float64, np.float32):
+        ts = lab.OptimizedTriangularSolve("L", dtype=dt).analysis(n, 0, t_ai, t_aj, t_av, d)
+        kind, parts = ts.schedule()
+        assert kind == "parts" and parts > 1, (dt, kind, parts)
