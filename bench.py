@@ -189,6 +189,23 @@ def run_reference(args, rank, world):
     }), flush=True)
 
 
+def max_over_ranks(pg, seconds, device):
+    """The largest of every rank's time (each rank passes its own); the job's
+    time for a replica run.  pg is torch.distributed or None (one rank)."""
+    if pg is None:
+        return seconds
+    import torch
+    tt = torch.tensor([seconds], dtype=torch.float64, device=device)
+    pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def replica_value(world, steps, bytes_per_step, seconds):
+    """Whole-job GB/s of `world` replicas that each ran `steps` steps of
+    `bytes_per_step` within `seconds` (the max over ranks)."""
+    return world * steps * bytes_per_step / seconds / 1e9
+
+
 def time_device_spmv(la, torch, plan, xd, yd, steps, warmup, alpha=1.0, beta=0.0):
     for _ in range(warmup):
         plan(xd, yd, alpha, beta)
@@ -385,12 +402,8 @@ def main():
         torch.cuda.synchronize()
         if pg:
             pg.barrier()
-    t = e0.elapsed_time(e1) / 1e3
-    if pg:
-        tt = torch.tensor([t], device="cuda")
-        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-        t = float(tt.item())
-    value = world * args.steps * byt / t / 1e9
+    t = max_over_ranks(pg, e0.elapsed_time(e1) / 1e3, "cuda")
+    value = replica_value(world, args.steps, byt, t)
     launch_s = t / args.steps
 
     # end to end through the reference-facing host-pointer call: pinned host
@@ -406,12 +419,8 @@ def main():
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         plan(hxn, hyn)
-    te = time.perf_counter() - t0
-    if pg:
-        tt = torch.tensor([te], device="cuda")
-        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-        te = float(tt.item())
-    e2e = world * e2e_steps * byt / te / 1e9
+    te = max_over_ranks(pg, time.perf_counter() - t0, "cuda")
+    e2e = replica_value(world, e2e_steps, byt, te)
     ok = np.allclose(hyn, yd.cpu().numpy(), rtol=1e-12, atol=1e-12)
 
     result = {

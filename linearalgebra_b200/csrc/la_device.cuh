@@ -34,6 +34,25 @@ template <typename T> __device__ __forceinline__ T ld_stream(const T *p) {
   return __ldg(p);
 }
 
+// Read-only loads that stay where they are written (asm volatile): used to
+// fetch data several steps ahead of its use, which the compiler might
+// otherwise move next to the use.
+__device__ __forceinline__ int ld_ahead(const int *p) {
+  int v;
+  asm volatile("ld.global.nc.s32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ float ld_ahead(const float *p) {
+  float v;
+  asm volatile("ld.global.nc.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ double ld_ahead(const double *p) {
+  double v;
+  asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+
 // Device-scope relaxed accesses (bypass the non-coherent L1) used for data
 // exchanged between CTAs of one kernel.
 __device__ __forceinline__ double ld_relaxed(const double *p) {

@@ -346,13 +346,13 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
 
   auto load_row = [&](int r, PartRow<X, KD> &R) {
     R.r = r;
-    R.i = __ldg(exec_row + r);
+    R.i = dev::ld_ahead(exec_row + r);
 #pragma unroll
     for (int s = 0; s < KD; s++) {
-      R.j[s] = __ldg(ej + (size_t)s * n + r);
-      R.a[s] = X(__ldg(ev + (size_t)s * n + r));
+      R.j[s] = dev::ld_ahead(ej + (size_t)s * n + r);
+      R.a[s] = X(dev::ld_ahead(ev + (size_t)s * n + r));
     }
-    R.dg = UNIT ? X(1) : X(__ldg(diag + r));
+    R.dg = UNIT ? X(1) : X(dev::ld_ahead(diag + r));
   };
   auto prefetch = [&](int q, PartRow<X, KD> &R) {
     R.r = -1;
