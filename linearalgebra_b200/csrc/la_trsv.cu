@@ -420,7 +420,43 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
   for (int q = q0 + tid; q <= q1; q += T)
     ssb[q - q0] = __ldg(sb + q);
   __syncthreads();
+  // Level q's slices of the row arrays are pulled into L2 six levels ahead
+  // (fire-and-forget bulk prefetches, one array per warp), so the register
+  // fetch three levels ahead reads L2 rather than HBM.
+  auto l2_ahead = [&](int q) {
+    const int a = tid >> 5;
+    if ((tid & 31) != 0 || a >= 2 * KD + 2 || q >= q1)
+      return;
+    const int s = ssb[q - q0], e = ssb[q - q0 + 1];
+    const char *base_ptr;
+    size_t es;
+    if (a == 0) {
+      base_ptr = reinterpret_cast<const char *>(exec_row);
+      es = 4;
+    } else if (a == 1) {
+      base_ptr = reinterpret_cast<const char *>(diag);
+      es = sizeof(V);
+      if (UNIT)
+        return;
+    } else if (a < 2 + KD) {
+      base_ptr = reinterpret_cast<const char *>(ej + (size_t)(a - 2) * n);
+      es = 4;
+    } else {
+      base_ptr = reinterpret_cast<const char *>(ev + (size_t)(a - 2 - KD) * n);
+      es = sizeof(V);
+    }
+    // a bulk prefetch needs a 16-byte aligned address and size: round the
+    // absolute range outwards (allocations are 256-byte aligned and padded by
+    // 64 bytes, so this stays inside them)
+    const size_t lo = reinterpret_cast<size_t>(base_ptr + (size_t)s * es) & ~(size_t)15;
+    const size_t hi = (reinterpret_cast<size_t>(base_ptr + (size_t)e * es) + 15) & ~(size_t)15;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo),
+                 "r"((unsigned)(hi - lo))
+                 : "memory");
+  };
   PartRow<X, KD> R0, R1, R2, R3;
+  for (int q = q0 + 3; q < q0 + 6; q++)
+    l2_ahead(q);
   prefetch(q0, R0);
   prefetch(q0 + 1, R1);
   prefetch(q0 + 2, R2);
@@ -448,21 +484,25 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
   // armed; one barrier per level, and every thread leaves together if any
   // gave up
   for (int q = q0; q < q1; q += 4) {
+    l2_ahead(q + 6);
     prefetch(q + 3, R3);
     run_level(q, R0);
     arm(R2);
     if (__syncthreads_or(aborted) || q + 1 >= q1)
       break;
+    l2_ahead(q + 7);
     prefetch(q + 4, R0);
     run_level(q + 1, R1);
     arm(R3);
     if (__syncthreads_or(aborted) || q + 2 >= q1)
       break;
+    l2_ahead(q + 8);
     prefetch(q + 5, R1);
     run_level(q + 2, R2);
     arm(R0);
     if (__syncthreads_or(aborted) || q + 3 >= q1)
       break;
+    l2_ahead(q + 9);
     prefetch(q + 6, R2);
     run_level(q + 3, R3);
     arm(R1);
