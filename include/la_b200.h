@@ -135,6 +135,24 @@ la_status la_spmv_noalloc(la_spmv_kind kind, int n, int nnz, int base,
                           double alpha, const double *d_x, double beta,
                           double *d_y, la_stream_t stream);
 
+/* Row-block SpMV of a distributed matrix (no reference counterpart; the
+ * reference's ParallelSPMV splits rows over threads by equal nonzero shares,
+ * utils/utils.h:187-222, which is how the blocks are cut across GPUs).  The
+ * plan's matrix is this rank's block of rows with global column indices;
+ * x is not gathered into one array first: it stays split into `nparts`
+ * contiguous slices, slice r holding columns [part_start[r],
+ * part_start[r+1]) at xparts[r], a device pointer that may be another GPU's
+ * memory mapped into this one (peer access or symmetric memory), and the
+ * kernel reads every column from the slice that owns it.  part_start is a
+ * HOST array of nparts + 1 non-decreasing entries from 0 to the matrix's
+ * column count; 1 <= nparts <= LA_SPMV_MAX_XPARTS.  The values of x must be
+ * in place before the call (the caller orders the writers, e.g. by a
+ * barrier across ranks); y = alpha*A*x + beta*y in the dtype of the slices. */
+#define LA_SPMV_MAX_XPARTS 8
+la_status la_spmv_xparts(la_spmv_plan_t plan, double alpha, const void *const *xparts,
+                         const int *part_start, int nparts, double beta, void *y,
+                         la_dtype vector_dtype, la_stream_t stream);
+
 /* Adjoints of y = A x (no reference counterpart; the reference has none).
  * la_spmv_transpose: out = alpha * A^T g + beta * out (dL/dx), through a
  * transposed copy of A built once per plan on first use (the role

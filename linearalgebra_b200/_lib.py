@@ -20,6 +20,7 @@ STATUS_NAMES = {
 }
 LA_F64, LA_F32 = 0, 1
 LA_SPMV_SEGSUM, LA_SPMV_ALBUS = 0, 1
+LA_SPMV_MAX_XPARTS = 8  # include/la_b200.h
 LA_LOWER, LA_UPPER = 0, 1
 LA_CSR_KEEP_F32 = 1
 LA_PCG_FP64, LA_PCG_MIXED = 0, 1
@@ -56,6 +57,7 @@ _SIGS = {
     "la_csr_destroy": [P],
     "la_spmv_plan_create": [P, I, C.POINTER(P)],
     "la_spmv": [P, D, P, D, P, I, P],
+    "la_spmv_xparts": [P, D, P, P, I, D, P, I, P],
     "la_spmv_host": [P, D, P, D, P],
     "la_spmv_plan_destroy": [P],
     "la_spmv_noalloc": [I, I, I, I, P, P, P, D, P, D, P, P],

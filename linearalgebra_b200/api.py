@@ -31,7 +31,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import (LA_CSR_KEEP_F32, LA_F32, LA_F64, LA_LOWER, LA_PCG_FP64,
-                   LA_PCG_MIXED, LA_SPMV_ALBUS, LA_SPMV_SEGSUM, LA_UPPER,
+                   LA_PCG_MIXED, LA_SPMV_ALBUS, LA_SPMV_MAX_XPARTS, LA_SPMV_SEGSUM, LA_UPPER,
                    LAError, PcgInfo, call)
 
 __all__ = [
@@ -131,6 +131,19 @@ class SPMV:
             call("la_spmv_host", self.h, float(alpha), _ptr(b), float(beta),
                  _ptr(x))
         return x
+
+    def xparts(self, slices, starts, y, alpha=1.0, beta=0.0):
+        """y = alpha*A*x + beta*y with x given as contiguous slices: slices[r]
+        holds columns starts[r]..starts[r+1]-1; each entry is a CUDA tensor or a
+        raw device address (e.g. a peer GPU's buffer).  la_spmv_xparts."""
+        import torch
+        ptrs = (C.c_void_p * len(slices))(
+            *[s if isinstance(s, int) else s.data_ptr() for s in slices])
+        st = np.ascontiguousarray(starts, dtype=np.int32)
+        vd = LA_F64 if y.dtype == torch.float64 else LA_F32
+        call("la_spmv_xparts", self.h, float(alpha), C.cast(ptrs, C.c_void_p), _ptr(st),
+             len(slices), float(beta), _ptr(y), vd, _stream(y))
+        return y
 
     def transpose(self, g, out, alpha=1.0, beta=0.0):
         """out = alpha*A^T g + beta*out (device FP64 tensors)."""

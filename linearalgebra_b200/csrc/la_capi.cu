@@ -10,6 +10,9 @@ namespace la {
 la_status spmv_launch(la_spmv_plan_t P, double alpha, const void *x,
                       double beta, void *y, const void *yin, la_dtype vd,
                       cudaStream_t st);
+la_status spmv_xparts_launch(la_spmv_plan_t P, double alpha, const void *const *xparts,
+                             const int *part_start, int nparts, double beta, void *y,
+                             la_dtype vd, cudaStream_t st);
 la_status sddmm_launch(la_spmv_plan_t P, double alpha, const double *g,
                        const double *x, double *dv, cudaStream_t st);
 la_status spmv_noalloc(la_spmv_kind kind, int n, int nnz, int base, const int *ai,
@@ -316,6 +319,22 @@ la_status la_spmv_transpose(la_spmv_plan_t plan, double alpha, const double *g,
   LA_CHECK_ARG(plan && g && out && g != out, "arguments");
   LA_TRY(ensure_transpose(plan));
   return spmv_launch(plan->Atplan, alpha, g, beta, out, out, LA_F64, S(stream));
+}
+
+la_status la_spmv_xparts(la_spmv_plan_t plan, double alpha, const void *const *xparts,
+                         const int *part_start, int nparts, double beta, void *y,
+                         la_dtype vector_dtype, la_stream_t stream) {
+  LA_CHECK_ARG(plan && xparts && part_start && (y || plan->A->n == 0), "arguments");
+  LA_CHECK_ARG(nparts >= 1 && nparts <= LA_SPMV_MAX_XPARTS, "nparts out of range");
+  LA_CHECK_ARG(part_start[0] == 0 && part_start[nparts] == plan->A->ncols,
+               "part_start must run from 0 to the column count");
+  for (int r = 0; r < nparts; r++) {
+    LA_CHECK_ARG(part_start[r] <= part_start[r + 1], "part_start must not decrease");
+    LA_CHECK_ARG(xparts[r] || part_start[r] == part_start[r + 1], "missing x slice");
+  }
+  LA_CHECK_ARG(vector_dtype == LA_F64 || vector_dtype == LA_F32, "vector dtype");
+  return spmv_xparts_launch(plan, alpha, xparts, part_start, nparts, beta, y, vector_dtype,
+                            S(stream));
 }
 
 la_status la_spmv_noalloc(la_spmv_kind kind, int n, int nnz, int base,

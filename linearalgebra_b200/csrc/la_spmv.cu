@@ -42,6 +42,7 @@
 #include <algorithm>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 
 namespace la {
 namespace {
@@ -133,18 +134,41 @@ __device__ __forceinline__ int row_start(const TileRows &T, int base,
   return T.staged ? rp[i] : min(max(__ldg(ai + T.R0 + i) - base - T.s, 0), T.cnt);
 }
 
-// Tile pass of y = alpha*A*x + beta*yin (yin may equal y).
-template <int FORM, typename V, typename X, typename ACC>
+// x split into contiguous slices (la_spmv_xparts): slice r holds columns
+// [start[r], start[r+1]) at p[r], which may be another GPU's memory.
+template <typename X> struct XParts {
+  const X *p[LA_SPMV_MAX_XPARTS];
+  int start[LA_SPMV_MAX_XPARTS + 1];
+  int n;
+};
+
+// Tile pass of y = alpha*A*x + beta*yin (yin may equal y).  With XP the
+// gather reads column j from the slice that owns it (XParts) instead of x.
+template <int FORM, typename V, typename X, typename ACC, bool XP = false>
 __global__ void __launch_bounds__(kThreads, kTileBlocksPerSm)
     spmv_tile_kernel(const int n, const int nnz, const int base,
                      const int *__restrict__ ai, const int *__restrict__ aj,
                      const V *__restrict__ av, const X *__restrict__ x, X *y,
                      const X *yin, const ACC alpha, const ACC beta,
-                     const int *__restrict__ tile_row, ACC *part) {
+                     const int *__restrict__ tile_row, ACC *part,
+                     const XParts<X> xp = XParts<X>{}) {
   __shared__ ACC prod[kTile];
   __shared__ int rp[kRowCap];
   __shared__ int long_rows[kLongCap];
   __shared__ int n_long;
+  __shared__ const X *xp_ptr[XP ? LA_SPMV_MAX_XPARTS : 1];
+  __shared__ int xp_start[XP ? LA_SPMV_MAX_XPARTS + 1 : 1];
+  if (XP) { // constant indices keep the parameter block out of local memory
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int r = 0; r < LA_SPMV_MAX_XPARTS; r++)
+        xp_ptr[r] = xp.p[r];
+#pragma unroll
+      for (int r = 0; r <= LA_SPMV_MAX_XPARTS; r++)
+        xp_start[r] = xp.start[r];
+    }
+    __syncthreads();
+  }
   // let the merge kernel's launch overlap this grid
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const RowOut<FORM, ACC> out{alpha, beta};
@@ -177,8 +201,17 @@ __global__ void __launch_bounds__(kThreads, kTileBlocksPerSm)
   ACC xv[kNpt];
 #pragma unroll
   for (int q = 0; q < kNpt; q++)
-    if (full || q * kThreads + tid < T.cnt)
-      xv[q] = ACC(__ldg(x + jj[q] - base));
+    if (full || q * kThreads + tid < T.cnt) {
+      if (XP) { // owner: the number of slice starts at or below the column
+        const int j = jj[q] - base;
+        int r = 0;
+        for (int k = 1; k < xp.n; k++)
+          r += j >= xp_start[k];
+        xv[q] = ACC(__ldg(xp_ptr[r] + (j - xp_start[r])));
+      } else {
+        xv[q] = ACC(__ldg(x + jj[q] - base));
+      }
+    }
   stage_rows(T, base, ai, rp);
 #pragma unroll
   for (int q = 0; q < kNpt; q++) {
@@ -293,9 +326,10 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-template <int FORM, typename V, typename X, typename ACC>
+template <int FORM, typename V, typename X, typename ACC, bool XP = false>
 la_status launch_form(la_spmv_plan_t P, const V *av, ACC alpha, const X *x,
-                      ACC beta, X *y, const X *yin, cudaStream_t st) {
+                      ACC beta, X *y, const X *yin, cudaStream_t st,
+                      const XParts<X> &xp = XParts<X>{}) {
   const la_csr_t A = P->A;
   if (A->n == 0)
     return LA_OK;
@@ -305,9 +339,9 @@ la_status launch_form(la_spmv_plan_t P, const V *av, ACC alpha, const X *x,
     LA_CUDA_TRY(cudaGetLastError());
     return LA_OK;
   }
-  spmv_tile_kernel<FORM, V, X, ACC><<<P->ntiles, kThreads, 0, st>>>(
+  spmv_tile_kernel<FORM, V, X, ACC, XP><<<P->ntiles, kThreads, 0, st>>>(
       A->n, A->nnz, A->base, A->ai.as<int>(), A->aj.as<int>(), av, x, y, yin, alpha, beta,
-      P->tile_row.as<int>(), P->part.as<ACC>());
+      P->tile_row.as<int>(), P->part.as<ACC>(), xp);
   LA_CUDA_TRY(cudaGetLastError());
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((P->ntiles + 255) / 256);
@@ -356,6 +390,50 @@ la_status spmv_launch(la_spmv_plan_t P, double alpha, const void *x,
                                (const float *)yin, st);
   return launch_form<kSegSum>(P, av, fa, (const float *)x, fb, (float *)y,
                               (const float *)yin, st);
+}
+
+// y = alpha*A*x + beta*y with x given as slices (validated by the caller).
+la_status spmv_xparts_launch(la_spmv_plan_t P, double alpha, const void *const *xparts,
+                             const int *part_start, int nparts, double beta, void *y,
+                             la_dtype vd, cudaStream_t st) {
+  auto fill = [&](auto &xp) {
+    using X = std::remove_cv_t<std::remove_pointer_t<std::remove_cv_t<
+        std::remove_reference_t<decltype(xp.p[0])>>>>;
+    for (int r = 0; r < LA_SPMV_MAX_XPARTS; r++)
+      xp.p[r] = r < nparts ? static_cast<const X *>(xparts[r]) : nullptr;
+    for (int r = 0; r <= LA_SPMV_MAX_XPARTS; r++)
+      xp.start[r] = part_start[std::min(r, nparts)];
+    xp.n = nparts;
+  };
+  const la_csr_t A = P->A;
+  if (vd == LA_F64) {
+    if (A->dtype != LA_F64) {
+      set_error("FP64 SpMV needs an FP64 matrix");
+      return LA_ERR_INVALID_ARG;
+    }
+    XParts<double> xp;
+    fill(xp);
+    const double *av = A->av.as<double>();
+    double *yy = static_cast<double *>(y);
+    if (P->kind == LA_SPMV_ALBUS)
+      return launch_form<kAlbus, double, double, double, true>(P, av, alpha, nullptr, beta, yy,
+                                                                yy, st, xp);
+    return launch_form<kSegSum, double, double, double, true>(P, av, alpha, nullptr, beta, yy,
+                                                               yy, st, xp);
+  }
+  const float *av = static_cast<const float *>(A->values(LA_F32));
+  if (!av) {
+    set_error("FP32 SpMV needs FP32 values (LA_CSR_KEEP_F32 or an FP32 matrix)");
+    return LA_ERR_INVALID_ARG;
+  }
+  XParts<float> xp;
+  fill(xp);
+  float *yy = static_cast<float *>(y);
+  if (P->kind == LA_SPMV_ALBUS)
+    return launch_form<kAlbus, float, float, float, true>(P, av, (float)alpha, nullptr,
+                                                          (float)beta, yy, yy, st, xp);
+  return launch_form<kSegSum, float, float, float, true>(P, av, (float)alpha, nullptr,
+                                                         (float)beta, yy, yy, st, xp);
 }
 
 la_status sddmm_launch(la_spmv_plan_t P, double alpha, const double *g,

@@ -33,6 +33,14 @@ extern "C" {
 int la_ref_max_threads(void) { return omp_get_max_threads(); }
 void la_ref_set_threads(int t) { omp_set_num_threads(t); }
 
+// LoadPrefixBalancedPartitionPos (utils/utils.h:187-222) over the row
+// pointers, as ParallelSPMV calls it: start[t] = first row of part t.
+void la_ref_prefix_partition(int n, const int *ai, int nparts, int *start) {
+  for (int t = 0; t < nparts; t++)
+    start[t] = (int)utils::LoadPrefixBalancedPartitionPos(ai, ai + n, t, nparts).first;
+  start[nparts] = n;
+}
+
 // ---------------------------------------------------------------- SpMV
 // SerialSPMV (sparse_mat_op/spmv.hpp:12-29)
 void la_ref_serial_spmv(int n, int base, const int *ai, const int *aj,

@@ -234,3 +234,38 @@ def test_spmv_adjoints(lab, orc, golden):
         ref = np.empty(len(aj))
         orc.port().oracle_sddmm_pattern(m, 0, P(ai), P(aj), P(g), P(x), P(ref), -1.25)
         assert np.array_equal(dv.cpu().numpy(), ref), name
+
+
+def test_spmv_xparts_emulated_ranks(lab):
+    """The row-block SpMV of a sharded matrix reading x from its owners'
+    slices (la_spmv_xparts), with the ranks emulated as separate device
+    buffers on one GPU: bit-identical to the same block multiplied with the
+    gathered x (la_spmv), for both forms and both precisions."""
+    from linearalgebra_b200 import dist, gen
+    for n, ai, aj, av in (gen.powerlaw(200_000, seed=4), gen.laplacian_3d(32)):
+        x = gen.uniform_vector(n, 2)
+        for world in (1, 3, 8):
+            start = dist.row_blocks_by_nnz(ai, world)
+            for dt in (torch.float64, torch.float32):
+                xd = torch.as_tensor(x).to("cuda", dt)
+                slices = [xd[int(start[r]):int(start[r + 1])].clone() for r in range(world)]
+                for r in range(world):
+                    r0, r1 = int(start[r]), int(start[r + 1])
+                    bai, baj, bav = dist.block_rows(ai, aj, av, r0, r1)
+                    A = lab.CSR(r1 - r0, n, 0, bai, baj, bav, keep_f32=True)
+                    for kind in (lab.api.LA_SPMV_SEGSUM, lab.api.LA_SPMV_ALBUS):
+                        plan = lab.SPMV(A, kind)
+                        y1 = torch.full((r1 - r0,), 0.5, dtype=dt, device="cuda")
+                        y2 = y1.clone()
+                        plan(xd, y1, 1.25, 0.5)
+                        plan.xparts(slices, start, y2, 1.25, 0.5)
+                        assert torch.equal(y1, y2), (n, world, r, dt, kind)
+    # argument checks
+    n, ai, aj, av = gen.laplacian_2d(16)
+    plan = lab.SPMV(lab.CSR(n, n, 0, ai, aj, av))
+    y = torch.empty(n, dtype=torch.float64, device="cuda")
+    xd = torch.zeros(n, dtype=torch.float64, device="cuda")
+    with pytest.raises(lab.LAError):
+        plan.xparts([xd], [0, n - 1], y)          # must end at the column count
+    with pytest.raises(lab.LAError):
+        plan.xparts([xd] * 9, [0] * 9 + [n], y)  # more slices than allowed
