@@ -381,16 +381,28 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
     }
     return v;
   };
+  // The slot reads are issued together (no branch between them), values of
+  // other parts that were not yet published are waited for afterwards (the
+  // rare case), and only then is the row summed in stored order -- an unused
+  // slot adds nothing, so the result is the reference's bit for bit.
   auto solve_row = [&](const PartRow<X, KD> &R, bool armed) {
     const X bi = xs[R.r - P0];
+    X v[KD];
+#pragma unroll
+    for (int s = 0; s < KD; s++) {
+      const int c = R.j[s];
+      v[s] = c < 0 ? xs[-1 - c] : (armed ? R.xr[s] : X(0));
+    }
+#pragma unroll
+    for (int s = 0; s < KD; s++) {
+      const int c = R.j[s];
+      if (c >= 0 && c != kEmptySlot && (!armed || Sentinel<X>::is(v[s])))
+        v[s] = await(c, armed ? v[s] : dev::ld_relaxed(x + c));
+    }
     X sum = X(0);
 #pragma unroll
     for (int s = 0; s < KD; s++)
-      if (R.j[s] != kEmptySlot) {
-        const int c = R.j[s];
-        const X v = c < 0 ? xs[-1 - c] : await(c, armed ? R.xr[s] : dev::ld_relaxed(x + c));
-        sum = add_rn(sum, mul_rn(R.a[s], v));
-      }
+      sum = R.j[s] != kEmptySlot ? add_rn(sum, mul_rn(R.a[s], v[s])) : sum;
     if (tail) {
       const int k1 = __ldg(ai + R.r + 1);
       for (int k = __ldg(ai + R.r) + KD; k < k1; k++) {
@@ -420,14 +432,15 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
   for (int q = q0 + tid; q <= q1; q += T)
     ssb[q - q0] = __ldg(sb + q);
   __syncthreads();
-  // Level q's slices of the row arrays are pulled into L2 six levels ahead
-  // (fire-and-forget bulk prefetches, one array per warp), so the register
-  // fetch three levels ahead reads L2 rather than HBM.
-  auto l2_ahead = [&](int q) {
+  // Slices of the row arrays are pulled into L2 several levels ahead, four
+  // levels per fire-and-forget bulk prefetch, one array per warp, so the
+  // register fetch three levels ahead reads L2 rather than HBM.
+  auto l2_ahead = [&](int q, int qe) { // levels [q, qe) of the part
     const int a = tid >> 5;
-    if ((tid & 31) != 0 || a >= 2 * KD + 2 || q >= q1)
+    qe = min(qe, q1);
+    if ((tid & 31) != 0 || a >= 2 * KD + 2 || q >= qe)
       return;
-    const int s = ssb[q - q0], e = ssb[q - q0 + 1];
+    const int s = ssb[q - q0], e = ssb[qe - q0];
     const char *base_ptr;
     size_t es;
     if (a == 0) {
@@ -455,8 +468,7 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
                  : "memory");
   };
   PartRow<X, KD> R0, R1, R2, R3;
-  for (int q = q0 + 3; q < q0 + 6; q++)
-    l2_ahead(q);
+  l2_ahead(q0 + 3, q0 + 8);
   prefetch(q0, R0);
   prefetch(q0 + 1, R1);
   prefetch(q0 + 2, R2);
@@ -480,32 +492,29 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
   __syncthreads();
   arm(R0);
   arm(R1);
-  // four register sets rotate: level q runs while q+3 is fetched and q+2 is
-  // armed; one barrier per level, and every thread leaves together if any
-  // gave up
+  // four register sets rotate: level q runs, then q+2 is armed and q+3 is
+  // fetched (after the solve, so its loads do not delay the solve's reads);
+  // one barrier per level, and every thread leaves together if any gave up
   for (int q = q0; q < q1; q += 4) {
-    l2_ahead(q + 6);
-    prefetch(q + 3, R3);
     run_level(q, R0);
     arm(R2);
+    l2_ahead(q + 8, q + 12); // four levels per bulk prefetch
+    prefetch(q + 3, R3);
     if (__syncthreads_or(aborted) || q + 1 >= q1)
       break;
-    l2_ahead(q + 7);
-    prefetch(q + 4, R0);
     run_level(q + 1, R1);
     arm(R3);
+    prefetch(q + 4, R0);
     if (__syncthreads_or(aborted) || q + 2 >= q1)
       break;
-    l2_ahead(q + 8);
-    prefetch(q + 5, R1);
     run_level(q + 2, R2);
     arm(R0);
+    prefetch(q + 5, R1);
     if (__syncthreads_or(aborted) || q + 3 >= q1)
       break;
-    l2_ahead(q + 9);
-    prefetch(q + 6, R2);
     run_level(q + 3, R3);
     arm(R1);
+    prefetch(q + 6, R2);
     if (__syncthreads_or(aborted))
       break;
   }
@@ -562,6 +571,8 @@ cudaError_t launch_parts_kd(la_trsv_plan_t P, const X *b, X *x, cudaStream_t st)
 template <typename V, typename X, bool UNIT>
 cudaError_t launch_parts(la_trsv_plan_t P, const X *b, X *x, cudaStream_t st) {
   switch (P->kd) {
+  case 3:
+    return launch_parts_kd<V, X, UNIT, 3>(P, b, x, st);
   case 4:
     return launch_parts_kd<V, X, UNIT, 4>(P, b, x, st);
   case 8:
@@ -689,7 +700,9 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
   int longest = 0;
   for (int i = 0; i < n; i++)
     longest = std::max(longest, ai[i + 1] - ai[i]);
-  const int kd = longest <= 4 ? 4 : longest <= 8 ? 8 : longest <= 16 ? 16 : 0;
+  // (3 slots for the 7-point stencils' IC(0) factors: a fourth would hold four
+  // registers per prefetched row for nothing, and FP64 needs them)
+  const int kd = longest <= 3 ? 3 : longest <= 4 ? 4 : longest <= 8 ? 8 : longest <= 16 ? 16 : 0;
   const int ks = kd ? kd : 16;
   // the device must hold one CTA per part with this much shared memory
   // levels per part (their boundaries are staged in shared memory too)
@@ -709,7 +722,10 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
     return LA_OK;
   const void *fns[2];
   int threads = 0;
-  if (ks == 4) {
+  if (ks == 3) {
+    fns[0] = part_fn<X, X, false, 3>(), fns[1] = part_fn<X, X, true, 3>();
+    threads = part_threads<X, 3>();
+  } else if (ks == 4) {
     fns[0] = part_fn<X, X, false, 4>(), fns[1] = part_fn<X, X, true, 4>();
     threads = part_threads<X, 4>();
   } else if (ks == 8) {
