@@ -220,7 +220,7 @@ def time_device_spmv(la, torch, plan, xd, yd, steps, warmup, alpha=1.0, beta=0.0
 
 
 def extras(la, torch, peak):
-    """Single-GPU extras: Laplacian SpMV rooflines and the PCG comparison."""
+    """Single-GPU extras: Laplacian SpMV rooflines and the PCG comparisons."""
     from linearalgebra_b200 import gen
     out = {"spmv": [], "pcg": None}
     for label, t in (("C1_lap2d_512", gen.laplacian_2d(512)), ("C3_lap3d_128", gen.laplacian_3d(128))):
@@ -252,8 +252,26 @@ def extras(la, torch, peak):
                                     "frac_of_measured_hbm": b / t / 1e9 / peak,
                                     "frac_of_8TBs": b / t / 8e12, "l2": "flushed"})
                 del flush
-    # IC(0)-PCG on the RCM-ordered 128^3 Laplacian, FP64 vs mixed
-    n, ai, aj, av = gen.laplacian_3d(128)
+    # IC(0)-PCG, FP64 vs mixed: the RCM-ordered 128^3 Laplacian (C3) and the
+    # 192^3 anisotropic diffusion (C5, mixed precision at scale)
+    out["pcg"], mats = pcg_case(la, torch, "C3_lap3d_128_rcm", gen.laplacian_3d(128))
+    out["pcg_c5"], _ = pcg_case(la, torch, "C5_aniso7_192_rcm", gen.aniso7(192, seed=0))
+    return out, mats
+
+
+def pcg_iteration_bytes(n, nnz, nnz_tri, vb):
+    """Algorithmic bytes of one PCG iteration with values and vectors of vb
+    bytes: SpMV + two triangular solves (strict triangle, row pointers,
+    execution map, diagonal, b, x) + about ten n-vector reads/writes."""
+    spmv = spmv_bytes(n, nnz, vb, vb)
+    trsv = nnz_tri * (vb + 4) + (n + 1) * 4 + n * 4 + 3 * n * vb
+    return spmv + 2 * trsv + 10 * n * 8
+
+
+def pcg_case(la, torch, label, matrix):
+    """FP64 vs mixed IC(0)-PCG to 1e-10 on an RCM-ordered SPD matrix."""
+    from linearalgebra_b200 import gen
+    n, ai, aj, av = matrix
     t0 = time.perf_counter()
     iperm, perm = la.SerialCM(n, 0, ai, aj)
     b_ai, b_aj, b_av = la.Permute(n, 0, ai, aj, av, iperm, perm)
@@ -267,20 +285,34 @@ def extras(la, torch, peak):
     bd = torch.as_tensor(bvec).to("cuda")
     x64 = torch.empty(n, dtype=torch.float64, device="cuda")
     x32 = torch.empty(n, dtype=torch.float64, device="cuda")
-    s64.solve(bd, x64)  # warm-up
-    s32.solve(bd, x32)
-    r64 = s64.solve(bd, x64)
-    r32 = s32.solve(bd, x32)
+    s64.solve(bd, x64, maxit=20000)  # warm-up
+    s32.solve(bd, x32, maxit=20000)
+    r64 = s64.solve(bd, x64, maxit=20000)
+    r32 = s32.solve(bd, x32, maxit=20000)
     err = float(torch.linalg.norm(x32 - x64) / torch.linalg.norm(x64))
-    out["pcg"] = {"config": "C3_lap3d_128_rcm", "n": n, "nnz": int(ai[-1]), "rtol": 1e-10,
-                  "levels": 382, "setup_s_host": setup_s,
-                  "fp64": {"iterations": r64.iterations, "ms": r64.solve_ms,
-                           "rel_residual": r64.rel_residual},
-                  "mixed": {"inner_iterations": r32.iterations, "outer": r32.outer_iterations,
-                            "ms": r32.solve_ms, "rel_residual": r32.rel_residual,
-                            "rel_err_vs_fp64": err},
-                  "speedup_mixed_vs_fp64": r64.solve_ms / r32.solve_ms}
-    return out, (b_ai, b_aj, b_av, ua, uj, f, bvec, r64)
+    nnz = int(ai[-1])
+    nnz_tri = (nnz - n) // 2
+    _, d, (s_ai, s_aj, s_av) = la.SplitLDU(n, 0, ua, uj, f)
+    t_ai, t_aj, t_av = la.Transpose(n, n, 0, s_ai, s_aj, s_av)
+    sched = {}
+    for name, dt in (("fp64", np.float64), ("fp32", np.float32)):
+        ts = la.OptimizedTriangularSolve("L", dtype=dt).analysis(n, 0, t_ai, t_aj, t_av, d)
+        sched[name] = list(ts.schedule())
+        levels = ts.levels()[0]
+    b64 = pcg_iteration_bytes(n, nnz, nnz_tri, 8)
+    b32 = pcg_iteration_bytes(n, nnz, nnz_tri, 4)
+    res = {"config": label, "n": n, "nnz": nnz, "rtol": 1e-10, "levels": levels,
+           "setup_s_host": setup_s,
+           "fp64": {"iterations": r64.iterations, "ms": r64.solve_ms,
+                    "rel_residual": r64.rel_residual,
+                    "GB/s_algorithmic": b64 * r64.iterations / (r64.solve_ms * 1e-3) / 1e9},
+           "mixed": {"inner_iterations": r32.iterations, "outer": r32.outer_iterations,
+                     "ms": r32.solve_ms, "rel_residual": r32.rel_residual,
+                     "rel_err_vs_fp64": err,
+                     "GB/s_algorithmic": b32 * r32.iterations / (r32.solve_ms * 1e-3) / 1e9},
+           "speedup_mixed_vs_fp64": r64.solve_ms / r32.solve_ms,
+           "trsv_schedules": sched}
+    return res, (b_ai, b_aj, b_av, ua, uj, f, bvec, r64)
 
 
 def cpu_pcg(mats):
