@@ -51,6 +51,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <vector>
 
@@ -647,6 +648,49 @@ la_status trsv_launch(la_trsv_plan_t P, const void *b, void *x,
   return launch_typed<float, float>(P, (const float *)b, (float *)x, st);
 }
 
+// The plans of one preconditioner (L and U = L^T, FP64 and FP32) share one
+// undirected graph, and a partition computed for one of them is valid for
+// all: the solve is correct for any partition, landmark coordinates are
+// monotone whatever the edges' direction, and L's level order is monotone
+// (reversed) for U.  So the last few partitions are kept, keyed by the row
+// count, the part count and an order-independent hash of the graph's edges.
+std::mutex g_part_mu;
+struct PartEntry {
+  int n, nparts;
+  unsigned long long hash;
+  std::vector<int> part;
+};
+std::vector<PartEntry> g_part_cache; // most recent last, at most 4
+
+void cached_partition(int n, const std::vector<int> &xadj, const std::vector<int> &adj,
+                      const int *ai, const int *aj, int base, const std::vector<int> &lvl,
+                      int nparts, std::vector<int> &part) {
+  unsigned long long h = 0x9e3779b97f4a7c15ull * (unsigned long long)(n + 1);
+  for (int i = 0; i < n; i++)
+    for (int k = xadj[i]; k < xadj[i + 1]; k++) {
+      const int j = adj[k];
+      if (j <= i)
+        continue;
+      unsigned long long z = (unsigned long long)i * 0x100000001b3ull ^ (unsigned long long)j;
+      z = (z ^ (z >> 31)) * 0xbf58476d1ce4e5b9ull;
+      h += z ^ (z >> 29); // sum: independent of the edge order
+    }
+  {
+    std::lock_guard<std::mutex> lock(g_part_mu);
+    for (const PartEntry &e : g_part_cache)
+      if (e.n == n && e.nparts == nparts && e.hash == h) {
+        part = e.part;
+        return;
+      }
+  }
+  part.assign(n, 0);
+  monotone_partition(n, xadj.data(), adj.data(), ai, aj, base, lvl.data(), nparts, part.data());
+  std::lock_guard<std::mutex> lock(g_part_mu);
+  if (g_part_cache.size() == 4)
+    g_part_cache.erase(g_part_cache.begin());
+  g_part_cache.push_back({n, nparts, h, part});
+}
+
 // Partitioned layout (schedule 1).  Leaves the plan untouched and reports
 // *ok = false when the parts would not fit in shared memory or the device
 // cannot keep one CTA per part resident.
@@ -685,8 +729,8 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
         adj[fill[j]++] = i;
       }
   }
-  std::vector<int> part(n);
-  monotone_partition(n, xadj.data(), adj.data(), ai, aj, base, lvl.data(), nparts, part.data());
+  std::vector<int> part;
+  cached_partition(n, xadj, adj, ai, aj, base, lvl, nparts, part);
   std::vector<int> pstart(nparts + 1, 0);
   for (int i = 0; i < n; i++)
     pstart[part[i] + 1]++;
