@@ -103,6 +103,8 @@ struct la_spmv_plan_s {
   int ntiles = 0;
   la::DevBuf tile_row; // int[ntiles + 1]: row holding each tile's first nz
   la::DevBuf part;     // double[2 * ntiles]: head / tail partial sums
+  la::DevBuf group_end; // int[ntiles]: end of the merge group a tile starts, else -1
+  bool long_rows = true; // some row is longer than the per-thread row sum limit
   // lazily built transpose for the adjoint
   la_csr_t At = nullptr;
   la_spmv_plan_t Atplan = nullptr;

@@ -144,7 +144,9 @@ template <typename X> struct XParts {
 
 // Tile pass of y = alpha*A*x + beta*yin (yin may equal y).  With XP the
 // gather reads column j from the slice that owns it (XParts) instead of x.
-template <int FORM, typename V, typename X, typename ACC, bool XP = false>
+// LONG = false drops the warp path for in-tile segments longer than kLongRow
+// (and its second barrier); the plan selects it when no row is that long.
+template <int FORM, typename V, typename X, typename ACC, bool XP = false, bool LONG = true>
 __global__ void __launch_bounds__(kThreads, kTileBlocksPerSm)
     spmv_tile_kernel(const int n, const int nnz, const int base,
                      const int *__restrict__ ai, const int *__restrict__ aj,
@@ -174,7 +176,7 @@ __global__ void __launch_bounds__(kThreads, kTileBlocksPerSm)
   const RowOut<FORM, ACC> out{alpha, beta};
   const int t = blockIdx.x, tid = threadIdx.x;
   const TileRows T = tile_rows(t, n, nnz, tile_row);
-  if (tid == 0)
+  if (LONG && tid == 0)
     n_long = 0;
   if (t == 0) // leading empty rows (ai[r + 1] == ai[0]) precede tile 0
     for (int r = tid; r < T.R0; r += kThreads)
@@ -233,7 +235,7 @@ __global__ void __launch_bounds__(kThreads, kTileBlocksPerSm)
   };
   for (int i = tid; i < T.nrows; i += kThreads) {
     const int lo = row_start(T, base, ai, rp, i), hi = row_start(T, base, ai, rp, i + 1);
-    if (hi - lo > kLongRow) {
+    if (LONG && hi - lo > kLongRow) {
       long_rows[atomicAdd(&n_long, 1)] = i;
       continue;
     }
@@ -242,6 +244,8 @@ __global__ void __launch_bounds__(kThreads, kTileBlocksPerSm)
       sum = add_rn(sum, prod[k]);
     emit(T.R0 + i, sum);
   }
+  if (!LONG)
+    return;
   __syncthreads();
   const int lane = tid & 31, warp = tid >> 5;
   for (int li = warp; li < n_long; li += kThreads / 32) {
@@ -260,29 +264,50 @@ __global__ void __launch_bounds__(kThreads, kTileBlocksPerSm)
 
 // Merge pass: one thread per tile f that is the first tile holding its head
 // row R; adds the previous tile's tail partial and the head partials of
-// every tile that starts inside R, in tile order, and writes y[R].
+// every tile that starts inside R, in tile order, and writes y[R].  The
+// tiles of that group are [f, group_end[f]) (group_end[f] = -1 when f is not
+// the first); plan-built groups are constant, so they are read before the
+// wait for the tile pass and the partials' loads do not depend on one
+// another.  Without group_end (the allocation-free path, whose tile rows are
+// computed on the device) the group is found by scanning tile_row.
 template <int FORM, typename X, typename ACC>
 __global__ void __launch_bounds__(256)
     spmv_merge_kernel(const int ntiles, X *y, const X *yin, const ACC beta,
-                      const int *__restrict__ tile_row, const ACC *part) {
+                      const int *__restrict__ tile_row, const ACC *part,
+                      const int *__restrict__ group_end) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  int R = 0, e = -1;
+  if (group_end && f < ntiles) {
+    e = group_end[f];
+    if (e >= 0)
+      R = tile_row[f];
+  }
   // wait until the tile pass has completed and its writes are visible
   asm volatile("griddepcontrol.wait;" ::: "memory");
-  const int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= ntiles)
     return;
-  const int R = tile_row[f];
-  if (f > 0 && tile_row[f - 1] == R)
+  if (!group_end) {
+    R = tile_row[f];
+    if (f > 0 && tile_row[f - 1] == R)
+      return;
+    e = f + 1;
+    while (e < ntiles && tile_row[e] == R)
+      e++;
+  }
+  if (e < 0)
     return;
   if (FORM == kAlbus) { // merge order of spmv.hpp:275-292
     ACC v = beta == ACC(0) ? ACC(0) : mul_rn(beta, ACC(yin[R]));
     if (f > 0)
       v = add_rn(v, part[2 * (f - 1) + 1]);
-    for (int u = f; u < ntiles && tile_row[u] == R; u++)
+#pragma unroll 4
+    for (int u = f; u < e; u++)
       v = add_rn(v, part[2 * u]);
     y[R] = X(v);
   } else { // carry chain of spmv.hpp:118-141, then + beta*x (:171)
     ACC c = f > 0 ? part[2 * (f - 1) + 1] : ACC(0);
-    for (int u = f; u < ntiles && tile_row[u] == R; u++)
+#pragma unroll 4
+    for (int u = f; u < e; u++)
       c = add_rn(part[2 * u], c);
     y[R] = X(beta == ACC(0) ? c : add_rn(c, mul_rn(beta, ACC(yin[R]))));
   }
@@ -339,9 +364,11 @@ la_status launch_form(la_spmv_plan_t P, const V *av, ACC alpha, const X *x,
     LA_CUDA_TRY(cudaGetLastError());
     return LA_OK;
   }
-  spmv_tile_kernel<FORM, V, X, ACC, XP><<<P->ntiles, kThreads, 0, st>>>(
-      A->n, A->nnz, A->base, A->ai.as<int>(), A->aj.as<int>(), av, x, y, yin, alpha, beta,
-      P->tile_row.as<int>(), P->part.as<ACC>(), xp);
+  auto tile = P->long_rows ? spmv_tile_kernel<FORM, V, X, ACC, XP, true>
+                           : spmv_tile_kernel<FORM, V, X, ACC, XP, false>;
+  tile<<<P->ntiles, kThreads, 0, st>>>(A->n, A->nnz, A->base, A->ai.as<int>(),
+                                       A->aj.as<int>(), av, x, y, yin, alpha, beta,
+                                       P->tile_row.as<int>(), P->part.as<ACC>(), xp);
   LA_CUDA_TRY(cudaGetLastError());
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((P->ntiles + 255) / 256);
@@ -355,8 +382,9 @@ la_status launch_form(la_spmv_plan_t P, const V *av, ACC alpha, const X *x,
   const int nt = P->ntiles;
   const int *tr = P->tile_row.as<int>();
   const ACC *pt = P->part.as<ACC>();
+  const int *ge = P->group_end.as<int>();
   LA_CUDA_TRY(cudaLaunchKernelEx(&cfg, spmv_merge_kernel<FORM, X, ACC>, nt, y, yin, beta,
-                                 tr, pt));
+                                 tr, pt, ge));
   return LA_OK;
 }
 
@@ -464,6 +492,20 @@ la_status spmv_plan_build(la_spmv_plan_t P) {
     trow[t] = int(std::upper_bound(ai, ai + n + 1, (int)(k + base)) - ai) - 1;
   }
   LA_TRY(P->tile_row.upload(trow.data(), sizeof(int) * trow.size()));
+  // merge groups: tiles [f, e) share head row trow[f]
+  std::vector<int> gend(ntiles, -1);
+  for (int f = 0; f < ntiles;) {
+    int e = f + 1;
+    while (e < ntiles && trow[e] == trow[f])
+      e++;
+    gend[f] = e;
+    f = e;
+  }
+  LA_TRY(P->group_end.upload(gend.data(), sizeof(int) * gend.size()));
+  int longest = 0;
+  for (int r = 0; r < n; r++)
+    longest = std::max(longest, ai[r + 1] - ai[r]);
+  P->long_rows = longest > kLongRow;
   LA_TRY(P->part.alloc(sizeof(double) * 2 * ntiles));
   LA_CUDA_TRY(cudaMemset(P->part.p, 0, P->part.bytes));
   return LA_OK;
@@ -564,9 +606,9 @@ la_status noalloc_launch(int n, int nnz, int base, const int *ai, const int *aj,
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   const double *yin = y, *pt = part;
-  const int *tr = tile_row;
+  const int *tr = tile_row, *ge = nullptr;
   LA_CUDA_TRY(cudaLaunchKernelEx(&cfg, spmv_merge_kernel<FORM, double, double>, ntiles, y,
-                                 yin, beta, tr, pt));
+                                 yin, beta, tr, pt, ge));
   return LA_OK;
 }
 } // namespace
