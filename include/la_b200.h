@@ -260,11 +260,15 @@ la_status la_trsv_host(la_trsv_plan_t plan, const double *b, double *x);
  * prefix[levels + 1] exactly as TopologicalSort2 returns them. */
 la_status la_trsv_levels(la_trsv_plan_t plan, int *levels, int *iperm,
                          int *prefix);
-/* Schedule the analysis chose (no reference counterpart; both compute the
+/* Schedule the analysis chose (no reference counterpart; all compute the
  * same bits): *schedule = 0 for level order over the whole GPU with per-row
  * readiness, 1 for the partitioned form (*parts co-resident CTAs, each
- * keeping its rows' values in shared memory).  Set LA_TRSV_SCHEDULE=flags or
- * =parts in the environment before the analysis to force one. */
+ * keeping its rows' values in shared memory), 2 for the partitioned form
+ * whose parts are too large for shared memory, which keeps each part's most
+ * recent rows in a shared-memory ring and reads older ones from x.  Set
+ * LA_TRSV_SCHEDULE=flags or =parts in the environment before the analysis to
+ * force level order or a partition; LA_TRSV_RING=<rows> (a power of two, at
+ * least 32) forces a ring of that size onto a partition. */
 la_status la_trsv_schedule(la_trsv_plan_t plan, int *schedule, int *parts);
 la_status la_trsv_plan_destroy(la_trsv_plan_t plan);
 

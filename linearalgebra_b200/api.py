@@ -239,10 +239,11 @@ class OptimizedTriangularSolve:
         return self
 
     def schedule(self):
-        """('levels', 0) or ('parts', number of parts): the analysis's choice."""
+        """('levels', 0), ('parts', number of parts) or ('parts-ring', number of
+        parts): the analysis's choice."""
         s, p = C.c_int(), C.c_int()
         call("la_trsv_schedule", self.h, C.byref(s), C.byref(p))
-        return ("parts" if s.value == 1 else "levels"), p.value
+        return {0: "levels", 1: "parts", 2: "parts-ring"}[s.value], p.value
 
     def levels(self):
         lv = C.c_int()

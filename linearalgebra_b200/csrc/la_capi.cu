@@ -574,7 +574,7 @@ la_status la_trsv_levels(la_trsv_plan_t plan, int *levels, int *iperm,
 
 la_status la_trsv_schedule(la_trsv_plan_t plan, int *schedule, int *parts) {
   LA_CHECK_ARG(plan && schedule && parts, "arguments");
-  *schedule = plan->sched;
+  *schedule = plan->sched == 1 && plan->ring_mask != la::kTrsvNoRing ? 2 : plan->sched;
   *parts = plan->sched == 1 ? plan->nparts : 0;
   return LA_OK;
 }

@@ -77,6 +77,27 @@ __device__ __forceinline__ int ld_relaxed(const int *p) {
   return v;
 }
 
+// Asynchronous 4- or 8-byte copy global -> shared (one element; both
+// addresses aligned to its size), tracked by the issuing thread's groups.
+template <typename T>
+__device__ __forceinline__ void cp_async_shared(T *dst_shared, const T *src) {
+  static_assert(sizeof(T) == 4 || sizeof(T) == 8, "cp.async element size");
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst_shared);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(src),
+               "n"(sizeof(T))
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+// every committed group but the most recent one has landed
+__device__ __forceinline__ void cp_async_wait_all_but_one() {
+  asm volatile("cp.async.wait_group 1;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
 // Segmented-sum pair: f = "a segment boundary occurred", v = running sum
 // since the last boundary.  combine(a, b) = (a.f | b.f, b.f ? b.v : a.v+b.v).
 template <typename ACC> struct SegPair {

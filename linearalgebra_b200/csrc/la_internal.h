@@ -12,6 +12,10 @@
 
 namespace la {
 
+// ring_mask of a partitioned triangular-solve plan whose rows each have
+// their own shared-memory slot
+constexpr int kTrsvNoRing = 0x7fffffff;
+
 // Thread-local last error message (la_last_error_string).
 void set_error(const char *fmt, ...);
 const char *get_error();
@@ -130,6 +134,7 @@ struct la_trsv_plan_s {
   // and aj holds -1 - (position in the part) for a column of the same part.
   int sched = 0, nparts = 0, part_rows = 0;
   size_t part_smem = 0; // x slots of the largest part + its level boundaries
+  int ring_mask = la::kTrsvNoRing; // x slots form a ring of ring_mask + 1 rows
   la::DevBuf pstart, psub, sb;
   la::DevBuf ej, ev; // first slots of every row, slot-major (schedule 1)
   la::DevBuf hb, hx; // staging for the host form

@@ -296,6 +296,7 @@ __global__ void __launch_bounds__(kThreads)
 // No deadlock: every CTA is resident and processes its rows in level order,
 // so the unfinished row of lowest level always has its inputs ready.
 constexpr int kEmptySlot = 0x7fffffff; // column of an unused slot
+constexpr int kNoRing = kTrsvNoRing;   // ring_mask when every row has its own slot
 
 // threads per CTA: four prefetched rows live in registers
 template <typename X, int KD> constexpr int part_threads() {
@@ -326,6 +327,14 @@ template <typename X, int KD> struct PartRow {
 // Entries beyond KD (only when some row is longer than 16) come from the CSR
 // copy, and rows beyond the first per thread in levels wider than the CTA
 // are loaded when reached.
+// Ring mode (ring_mask != kNoRing), for parts whose rows do not all fit in
+// shared memory: the x slots form a ring of ring_mask + 1 rows, row r of the
+// part in slot (r - P0) & ring_mask.  The analysis encodes a dependency on
+// the part's own row as a slot only while that slot cannot yet have been
+// reused (see build_parts); older ones are read from x in global memory,
+// published several barriers earlier.  b is not staged at kernel start:
+// each prefetched row's b is copied into its slot by cp.async when the row
+// is armed (two levels ahead), and the solve waits for that copy first.
 template <typename V, typename X, bool UNIT, int KD>
 __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
     trsv_part_kernel(const int n, const int *__restrict__ pstart,
@@ -334,8 +343,9 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
                      const V *__restrict__ av, const int *__restrict__ ej,
                      const V *__restrict__ ev, const V *__restrict__ diag,
                      const int *__restrict__ exec_row, const X *__restrict__ b, X *x,
-                     int *err, const int tail, const int rows_cap) {
+                     int *err, const int tail, const int rows_cap, const int ring_mask) {
   constexpr int T = part_threads<X, KD>();
+  const bool ring = ring_mask != kNoRing;
   extern __shared__ __align__(16) unsigned char part_smem[];
   X *xs = reinterpret_cast<X *>(part_smem);
   int *ssb = reinterpret_cast<int *>(xs + rows_cap); // level boundaries
@@ -369,7 +379,11 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
       for (int s = 0; s < KD; s++)
         if (R.j[s] >= 0 && R.j[s] != kEmptySlot)
           R.xr[s] = dev::ld_relaxed(x + R.j[s]);
+      if (ring)
+        dev::cp_async_shared(xs + ((R.r - P0) & ring_mask), b + R.i);
     }
+    if (ring) // one group per armed level, empty or not
+      dev::cp_async_commit();
   };
   // a value of another part: wait (bounded) until it stops being the sentinel
   auto await = [&](int c, X v) {
@@ -387,7 +401,8 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
   // rare case), and only then is the row summed in stored order -- an unused
   // slot adds nothing, so the result is the reference's bit for bit.
   auto solve_row = [&](const PartRow<X, KD> &R, bool armed) {
-    const X bi = xs[R.r - P0];
+    const int slot = (R.r - P0) & ring_mask;
+    const X bi = ring && !armed ? __ldg(b + R.i) : xs[slot];
     X v[KD];
 #pragma unroll
     for (int s = 0; s < KD; s++) {
@@ -415,10 +430,12 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
     X xi = sub_rn(bi, sum);
     if (!UNIT)
       xi = div_rn(xi, R.dg);
-    xs[R.r - P0] = xi;
+    xs[slot] = xi;
     dev::st_relaxed(x + R.i, Sentinel<X>::scrub(xi));
   };
   auto run_level = [&](int q, const PartRow<X, KD> &R) {
+    if (ring) // this row's b copy: all but the newest group (level q+1's) are done
+      dev::cp_async_wait_all_but_one();
     if (R.r < 0)
       return;
     solve_row(R, true);
@@ -476,7 +493,7 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
   // b of the part's rows into their x slots, 16 rows per thread per batch
   // (all row indices, then all b values, in flight together)
   constexpr int kStage = 16;
-  for (int r0 = P0 + tid; r0 < P1; r0 += kStage * T) {
+  for (int r0 = P0 + tid; !ring && r0 < P1; r0 += kStage * T) {
     int ii[kStage];
     X bv[kStage];
 #pragma unroll
@@ -519,6 +536,8 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
     if (__syncthreads_or(aborted))
       break;
   }
+  if (ring) // no copy may still be landing when the CTA leaves (an abort)
+    dev::cp_async_wait_all();
 }
 
 template <typename V, typename X, bool UNIT>
@@ -560,11 +579,11 @@ cudaError_t launch_parts_kd(la_trsv_plan_t P, const X *b, X *x, cudaStream_t st)
             *er = P->exec_row.as<int>();
   const V *av = P->av.as<V>(), *ev = P->ev.as<V>(), *dg = P->diag.as<V>();
   int *err = P->err.as<int>();
-  const int cap = P->part_rows;
+  const int cap = P->part_rows, mask = P->ring_mask;
   void *args[] = {(void *)&n,  (void *)&ps, (void *)&pq, (void *)&sb,  (void *)&ai,
                   (void *)&aj, (void *)&av, (void *)&ej, (void *)&ev,  (void *)&dg,
                   (void *)&er, (void *)&b,  (void *)&x,  (void *)&err, (void *)&tail,
-                  (void *)&cap};
+                  (void *)&cap, (void *)&mask};
   return cudaLaunchCooperativeKernel(part_fn<V, X, UNIT, KD>(), dim3(P->nparts),
                                      dim3(part_threads<X, KD>()), args, P->part_smem, st);
 }
@@ -692,8 +711,9 @@ void cached_partition(int n, const std::vector<int> &xadj, const std::vector<int
 }
 
 // Partitioned layout (schedule 1).  Leaves the plan untouched and reports
-// *ok = false when the parts would not fit in shared memory or the device
-// cannot keep one CTA per part resident.
+// *ok = false when the device cannot keep one CTA per part resident, or when
+// a part's rows fit in shared memory neither whole nor as a ring (ring mode
+// needs any three consecutive levels of a part to fit).
 template <typename X>
 la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const double *av,
                       const double *diag, bool force, bool *ok) {
@@ -702,12 +722,9 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
   int dev = 0, optin = 0;
   LA_CUDA_TRY(cudaGetDevice(&dev));
   LA_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  const int cap = (optin - 1024) / (int)sizeof(X);
   int nparts = std::min(sm_count(), std::max(1, (n + 2047) / 2048));
   if (const char *e = std::getenv("LA_TRSV_PARTS")) // tuning override
     nparts = std::max(1, std::min(sm_count(), std::atoi(e)));
-  if ((long long)nparts * cap < (long long)n + n / 16)
-    return LA_OK;
   // rows' levels, and the triangle's graph made undirected
   std::vector<int> lvl(n);
   for (int l = 0; l < P->levels; l++)
@@ -737,8 +754,6 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
   int rows_max = 0;
   for (int p = 0; p < nparts; p++)
     rows_max = std::max(rows_max, pstart[p + 1]);
-  if (rows_max > cap)
-    return LA_OK;
   std::partial_sum(pstart.begin(), pstart.end(), pstart.begin());
   // register slots from the longest row (16 plus the CSR tail beyond)
   int longest = 0;
@@ -748,22 +763,53 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
   // registers per prefetched row for nothing, and FP64 needs them)
   const int kd = longest <= 3 ? 3 : longest <= 4 ? 4 : longest <= 8 ? 8 : longest <= 16 ? 16 : 0;
   const int ks = kd ? kd : 16;
-  // the device must hold one CTA per part with this much shared memory
-  // levels per part (their boundaries are staged in shared memory too)
-  int subs_max = 0;
+  // execution order: part-major, level order inside a part; sb = the
+  // start position of every (part, level), psub = each part's first entry
+  std::vector<int> erow(n), pos(n);
   {
-    std::vector<int> last(nparts, -1), subs(nparts, 0);
+    std::vector<int> fill(pstart.begin(), pstart.end() - 1);
     for (int q = 0; q < n; q++) {
-      const int i = P->h_iperm[q] - base;
-      if (last[part[i]] != lvl[i]) {
-        last[part[i]] = lvl[i];
-        subs_max = std::max(subs_max, ++subs[part[i]]);
-      }
+      const int i = P->h_iperm[q] - base, r = fill[part[i]]++;
+      erow[r] = i;
+      pos[i] = r;
     }
   }
-  const size_t smem = sizeof(X) * (size_t)rows_max + sizeof(int) * ((size_t)subs_max + 1);
-  if (smem + 1024 > (size_t)optin)
-    return LA_OK;
+  std::vector<int> sb, psub(nparts + 1), lvl_at(n);
+  int subs_max = 0;
+  for (int p = 0; p < nparts; p++) {
+    psub[p] = (int)sb.size();
+    for (int r = pstart[p]; r < pstart[p + 1]; r++) {
+      if (r == pstart[p] || lvl[erow[r]] != lvl[erow[r - 1]])
+        sb.push_back(r);
+      lvl_at[r] = (int)sb.size() - 1;
+    }
+    subs_max = std::max(subs_max, (int)sb.size() - psub[p]);
+  }
+  psub[nparts] = (int)sb.size();
+  sb.push_back(n);
+  // end of the level two after the one at sb index g (part p)
+  auto end2 = [&](int p, int g) { return sb[std::min(g + 3, psub[p + 1])]; };
+  // shared memory: every row of the largest part, else a ring (power of two)
+  const size_t sb_bytes = sizeof(int) * ((size_t)subs_max + 1);
+  int ring = 0; // ring rows, 0 = whole parts
+  if (sizeof(X) * (size_t)rows_max + sb_bytes + 1024 > (size_t)optin) {
+    if (sb_bytes + 1024 + sizeof(X) * 1024 > (size_t)optin)
+      return LA_OK;
+    ring = 1024;
+    while (sizeof(X) * (size_t)ring * 2 + sb_bytes + 1024 <= (size_t)optin)
+      ring *= 2;
+  }
+  if (const char *e = std::getenv("LA_TRSV_RING")) { // testing / tuning override
+    const int r = std::atoi(e);
+    if (r >= 32 && (r & (r - 1)) == 0 && sizeof(X) * (size_t)r + sb_bytes + 1024 <= (size_t)optin)
+      ring = r;
+  }
+  if (ring)
+    for (int p = 0; p < nparts; p++)
+      for (int g = psub[p]; g < psub[p + 1]; g++)
+        if (end2(p, g) - sb[g] > ring)
+          return LA_OK; // three consecutive levels must fit in the ring
+  const size_t smem = sizeof(X) * (size_t)(ring ? ring : rows_max) + sb_bytes;
   const void *fns[2];
   int threads = 0;
   if (ks == 3) {
@@ -797,10 +843,14 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
   }
   // Modelled critical path (microseconds; B200 measurements): a part takes
   // ~0.35 us per level it holds plus ~1 us for every further round of rows
-  // in a level wider than its CTA, and a value crossing parts arrives
-  // ~1.5 us after it is written; the level-order schedule takes ~2 us per
-  // level.  The partition is used when it models at most 0.8 of that.
+  // in a level wider than its CTA, both 1.5x for FP64 (a part's level step
+  // measured 1.24 us FP64 against 0.80 us FP32 on the 128^3 IC(0) factor,
+  // while the level order costs about the same in both), and a value
+  // crossing parts arrives ~1.5 us after it is written; the level-order
+  // schedule takes ~2 us per level.  The partition is used when it models
+  // at most 0.8 of that.
   if (!force) {
+    const double f = sizeof(X) == 8 ? 1.5 : 1.0;
     std::vector<double> ready(n), last(nparts, 0.0), fin(nparts, 0.0);
     std::vector<int> width(nparts, 0), touched;
     for (int l = 0; l < P->levels; l++) {
@@ -819,7 +869,7 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
         fin[pi] = std::max(fin[pi], t);
       }
       for (int p : touched)
-        fin[p] += 0.35 + 1.0 * ((width[p] + threads - 1) / threads - 1);
+        fin[p] += f * (0.35 + 1.0 * ((width[p] + threads - 1) / threads - 1));
       for (int q = P->h_prefix[l]; q < P->h_prefix[l + 1]; q++) {
         const int i = P->h_iperm[q] - base;
         ready[i] = fin[part[i]];
@@ -835,27 +885,12 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
     if (est > 0.8 * 2.0 * P->levels)
       return LA_OK;
   }
-  // execution order: part-major, level order inside a part
-  std::vector<int> erow(n), pos(n);
-  {
-    std::vector<int> fill(pstart.begin(), pstart.end() - 1);
-    for (int p = 0; p < n; p++) {
-      const int i = P->h_iperm[p] - base, r = fill[part[i]]++;
-      erow[r] = i;
-      pos[i] = r;
-    }
-  }
-  std::vector<int> sb, psub(nparts + 1);
-  for (int p = 0; p < nparts; p++) {
-    psub[p] = (int)sb.size();
-    for (int r = pstart[p]; r < pstart[p + 1]; r++)
-      if (r == pstart[p] || lvl[erow[r]] != lvl[erow[r - 1]])
-        sb.push_back(r);
-  }
-  psub[nparts] = (int)sb.size();
-  sb.push_back(n);
-  // encoded columns (-1 - position in the part for the part's own rows),
-  // first ks entries slot-major, all entries in CSR for rows beyond ks
+  // encoded columns (-1 - x slot for the part's own rows), first ks entries
+  // slot-major, all entries in CSR for rows beyond ks.  In ring mode a row r
+  // of level g reads its part's row d from the ring only if d >= end of level
+  // g + 2 minus the ring size: d's slot is refilled by row d + ring, whose b
+  // is copied in while level (d + ring's level) - 2 is still being solved, so
+  // d + ring must lie beyond level g + 2.  Older rows are read from x.
   const size_t cells = (size_t)ks * n;
   std::vector<int> ej(cells, kEmptySlot);
   std::vector<double> ev(cells, 0.0), ediag(n, 1.0);
@@ -873,7 +908,14 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
       ediag[r] = diag[i];
     for (int k = ai[i] - base, s = 0; k < ai[i + 1] - base; k++, s++, w++) {
       const int j = aj[k] - base;
-      const int c = part[j] == pi ? -1 - (pos[j] - pstart[pi]) : j;
+      int c = j;
+      if (part[j] == pi) {
+        const int d = pos[j];
+        if (!ring)
+          c = -1 - (d - pstart[pi]);
+        else if (d >= end2(pi, lvl_at[r]) - ring)
+          c = -1 - ((d - pstart[pi]) & (ring - 1));
+      }
       if (s < ks) {
         ej[(size_t)s * n + r] = c;
         ev[(size_t)s * n + r] = av[k];
@@ -911,7 +953,8 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
   }
   P->kd = kd;
   P->nparts = nparts;
-  P->part_rows = rows_max;
+  P->part_rows = ring ? ring : rows_max;
+  P->ring_mask = ring ? ring - 1 : kNoRing;
   P->part_smem = smem;
   P->sched = 1;
   *ok = true;

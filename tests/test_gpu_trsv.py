@@ -236,6 +236,63 @@ def test_trsv_schedules_bit_identical(lab, orc, monkeypatch, schedule):
             assert np.array_equal(x32, y32), (n, uplo, "fp32 schedules differ")
 
 
+def _chain_with_skips(n, seed):
+    """Strict lower triangle: row i reads rows i-1, i-500 and i-1500 (when
+    they exist) -- one row per level, and dependencies far older than the
+    levels just before."""
+    r = np.random.default_rng(seed)
+    cols = [[j for j in (i - 1500, i - 500, i - 1) if j >= 0] for i in range(n)]
+    ai = np.concatenate([[0], np.cumsum([len(c) for c in cols])]).astype(np.int32)
+    aj = np.concatenate([np.array(c, np.int64) for c in cols]).astype(np.int32)
+    return ai, aj, r.uniform(-0.3, 0.3, int(ai[-1]))
+
+
+def test_trsv_ring_bit_identical(lab, orc, monkeypatch):
+    """The partitioned schedule with each part's x slots as a shared-memory
+    ring (the form taken when a part's rows do not fit in shared memory),
+    forced onto small cases: bit-identical to the oracle in both triangles
+    and both precisions.  Cases: IC(0) factors with the default parts; the
+    40^3 factor on 2 parts, whose levels are wider than a CTA (rows beyond
+    the first per thread read b directly); a chain with skips on 3 parts and
+    a 32-row ring, whose dependencies 500 and 1500 rows back are older than
+    the ring and are read from x."""
+    from linearalgebra_b200 import gen
+    P = orc.ptr
+    monkeypatch.setenv("LA_TRSV_SCHEDULE", "parts")
+    cases = []
+    for n, ai, aj, av in (gen.laplacian_3d(40), gen.aniso7(28, seed=3)):
+        _, lt, ut, d = _ic_factor_rcm(lab, n, ai, aj, av)
+        cases += [(n, "L", lt, d, None, ("1024", "2048", "4096")),
+                  (n, "U", ut, d, None, ("1024", "2048", "4096"))]
+        if n == 64_000:
+            cases.append((n, "L", lt, d, "2", ("2048", "4096", "8192")))
+    n = 3000
+    cases.append((n, "L", _chain_with_skips(n, 4), np.random.default_rng(5).uniform(1, 2, n),
+                  "3", ("32",)))
+    for n, uplo, (c_ai, c_aj, c_av), d, parts, rings in cases:
+        if parts:
+            monkeypatch.setenv("LA_TRSV_PARTS", parts)
+        else:
+            monkeypatch.delenv("LA_TRSV_PARTS", raising=False)
+        b = np.random.default_rng(n + 1).uniform(-1, 1, n)
+        for ring in rings:  # the smallest ring that holds three levels
+            monkeypatch.setenv("LA_TRSV_RING", ring)
+            ts, x = solve(lab, uplo, n, c_ai, c_aj, c_av, d, b)
+            if ts.schedule()[0] == "parts-ring":
+                break
+        assert ts.schedule()[0] == "parts-ring", (n, uplo, parts, ts.schedule())
+        lv, ip, pf = ts.levels()
+        ref = np.zeros(n)
+        orc.port().oracle_level_solve(lv, P(ip), P(pf), 0, P(c_ai), P(c_aj), P(c_av),
+                                      P(d), P(b), P(ref))
+        assert np.array_equal(x, ref), (n, uplo, parts, ring)
+        ts32, x32 = solve(lab, uplo, n, c_ai, c_aj, c_av, d, b, dtype=np.float32)
+        assert ts32.schedule()[0] == "parts-ring", (n, uplo, ts32.schedule())
+        monkeypatch.delenv("LA_TRSV_RING")
+        _, y32 = solve(lab, uplo, n, c_ai, c_aj, c_av, d, b, dtype=np.float32)
+        assert np.array_equal(x32, y32), (n, uplo, "fp32 ring differs from whole parts")
+
+
 def test_trsv_partitioned_is_chosen_for_3d_ic0(lab):
     """The analysis picks the partitioned schedule for the RCM-ordered IC(0)
     factor of the 128^3 Laplacian (the preconditioner of the PCG workload)."""
