@@ -266,7 +266,68 @@ def extras(la, torch, peak):
     # 192^3 anisotropic diffusion (C5, mixed precision at scale)
     out["pcg"], mats = pcg_case(la, torch, "C3_lap3d_128_rcm", gen.laplacian_3d(128))
     out["pcg_c5"], _ = pcg_case(la, torch, "C5_aniso7_192_rcm", gen.aniso7(192, seed=0))
+    out["adjoint_c4"] = adjoint_case(la, torch, peak)
     return out, mats
+
+
+def adjoint_case(la, torch, peak):
+    """Differentiation configuration: SPD 27-point stencil on a 96^3 grid, FP64;
+    L = 1/2 ||u - u*||^2 with u = A^-1 b.  Times the forward IC(0)-PCG, the
+    adjoint solve with dL/dvalues (la_pcg_adjoint), and the SpMV adjoints --
+    transpose SpMV (dL/dx) and the sampled outer product over the pattern
+    (dL/dvalues) -- each to 1e-10.  Gradient parity (finite differences on 64
+    entries, FP64 CPU gradient) is tests/test_gpu_adjoint.py's job."""
+    from linearalgebra_b200 import gen
+    n, ai, aj, av = gen.stencil27(96, seed=0)
+    nnz = int(ai[-1])
+    t0 = time.perf_counter()
+    ua, uj, uv = gen.upper_with_diag(n, ai, aj, av)
+    f = la.ICCLevelNumeric0(n, 0, ua, uj, uv)
+    A = la.CSR(n, n, 0, ai, aj, av)
+    s = la.PCG(A, ua, uj, f)
+    plan = la.SPMV(A)
+    setup_s = time.perf_counter() - t0
+    rng = np.random.default_rng(0)
+    us = torch.as_tensor(rng.standard_normal(n)).cuda()
+    b = torch.as_tensor(rng.standard_normal(n)).cuda()
+    u = torch.empty_like(b)
+    db = torch.empty_like(b)
+    dv = torch.empty(nnz, dtype=torch.float64, device="cuda")
+    dx = torch.empty_like(b)
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps, out
+
+    fwd_ms, rf = timed(lambda: s.solve(b, u, rtol=1e-10), 3)
+    g = u - us
+    adj_ms, ra = timed(lambda: s.adjoint(g, u, db, dv, rtol=1e-10), 3)
+    tr_ms, _ = timed(lambda: plan.transpose(g, dx), 50)
+    sd_ms, _ = timed(lambda: plan.sddmm(g, u, dv), 50)
+    spmv_b = spmv_bytes(n, nnz)
+    sddmm_b = nnz * 12 + n * 8 * 2 + (n + 1) * 4
+    _, d, (s_ai, s_aj, s_av) = la.SplitLDU(n, 0, ua, uj, f)
+    t_ai, t_aj, t_av = la.Transpose(n, n, 0, s_ai, s_aj, s_av)
+    ts = la.OptimizedTriangularSolve("L").analysis(n, 0, t_ai, t_aj, t_av, d)
+    return {"config": "C4_stencil27_96_fp64", "n": n, "nnz": nnz, "rtol": 1e-10,
+            "setup_s_host": setup_s, "levels": ts.levels()[0],
+            "trsv_schedule": list(ts.schedule()),
+            "forward_pcg": {"iterations": rf.iterations, "ms": fwd_ms,
+                            "rel_residual": rf.rel_residual},
+            "adjoint_pcg_and_dvalues": {"iterations": ra.iterations, "ms": adj_ms,
+                                        "rel_residual": ra.rel_residual},
+            "spmv_transpose": {"us": tr_ms * 1e3, "GB/s": spmv_b / (tr_ms * 1e-3) / 1e9,
+                               "frac_of_measured_hbm": spmv_b / (tr_ms * 1e-3) / 1e9 / peak},
+            "sddmm_pattern": {"us": sd_ms * 1e3, "GB/s": sddmm_b / (sd_ms * 1e-3) / 1e9,
+                              "frac_of_measured_hbm": sddmm_b / (sd_ms * 1e-3) / 1e9 / peak},
+            "timing": "back to back after one warm-up call; inputs larger than L2 except x/g"}
 
 
 def pcg_iteration_bytes(n, nnz, nnz_tri, vb):
