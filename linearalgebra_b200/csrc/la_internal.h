@@ -135,6 +135,7 @@ struct la_trsv_plan_s {
   int sched = 0, nparts = 0, part_rows = 0;
   size_t part_smem = 0; // x slots of the largest part + its level boundaries
   int ring_mask = la::kTrsvNoRing; // x slots form a ring of ring_mask + 1 rows
+  bool w2 = false; // partitioned kernel with the second-row register sets
   la::DevBuf pstart, psub, sb;
   la::DevBuf ej, ev; // first slots of every row, slot-major (schedule 1)
   la::DevBuf hb, hx; // staging for the host form

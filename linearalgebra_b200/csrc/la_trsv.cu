@@ -335,7 +335,12 @@ template <typename X, int KD> struct PartRow {
 // published several barriers earlier.  b is not staged at kernel start:
 // each prefetched row's b is copied into its slot by cp.async when the row
 // is armed (two levels ahead), and the solve waits for that copy first.
-template <typename V, typename X, bool UNIT, int KD>
+// W2 (FP32, short rows): levels wider than the CTA are common in large parts;
+// two more register sets hold each thread's second row of a level, fetched
+// at the start of the level before (L2, pulled in by the bulk prefetch) and
+// its other parts' values requested at the start of its own level, so the
+// second round of a wide level costs no global round trip of its own.
+template <typename V, typename X, bool UNIT, int KD, bool W2 = false>
 __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
     trsv_part_kernel(const int n, const int *__restrict__ pstart,
                      const int *__restrict__ psub, const int *__restrict__ sb,
@@ -400,9 +405,11 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
   // other parts that were not yet published are waited for afterwards (the
   // rare case), and only then is the row summed in stored order -- an unused
   // slot adds nothing, so the result is the reference's bit for bit.
-  auto solve_row = [&](const PartRow<X, KD> &R, bool armed) {
+  // b_in_slot: b was staged at kernel start (whole parts) or copied in when
+  // the row was armed (ring mode); otherwise it is read here
+  auto solve_row = [&](const PartRow<X, KD> &R, bool armed, bool b_in_slot) {
     const int slot = (R.r - P0) & ring_mask;
-    const X bi = ring && !armed ? __ldg(b + R.i) : xs[slot];
+    const X bi = b_in_slot ? xs[slot] : __ldg(b + R.i);
     X v[KD];
 #pragma unroll
     for (int s = 0; s < KD; s++) {
@@ -433,17 +440,44 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
     xs[slot] = xi;
     dev::st_relaxed(x + R.i, Sentinel<X>::scrub(xi));
   };
-  auto run_level = [&](int q, const PartRow<X, KD> &R) {
+  // W2: a thread's second row of level q (r = level start + T + tid)
+  auto prefetch2 = [&](int q, PartRow<X, KD> &S) {
+    S.r = -1;
+    if (q < q1) {
+      const int r = ssb[q - q0] + T + tid;
+      if (r < ssb[q - q0 + 1])
+        load_row(r, S);
+    }
+  };
+  auto arm2 = [&](PartRow<X, KD> &S) {
+    if (S.r >= 0) {
+#pragma unroll
+      for (int s = 0; s < KD; s++)
+        if (S.j[s] >= 0 && S.j[s] != kEmptySlot)
+          S.xr[s] = dev::ld_relaxed(x + S.j[s]);
+    }
+  };
+  auto run_level = [&](int q, const PartRow<X, KD> &R, PartRow<X, KD> &Sc,
+                       PartRow<X, KD> &Sn) {
     if (ring) // this row's b copy: all but the newest group (level q+1's) are done
       dev::cp_async_wait_all_but_one();
+    if (W2) {
+      prefetch2(q + 1, Sn);
+      arm2(Sc);
+    }
     if (R.r < 0)
       return;
-    solve_row(R, true);
+    solve_row(R, true, true);
     const int e = ssb[q - q0 + 1];
-    for (int r = R.r + T; r < e; r += T) { // levels wider than the CTA
+    int r = R.r + T;
+    if (W2 && Sc.r >= 0) {
+      solve_row(Sc, true, !ring);
+      r += T;
+    }
+    for (; r < e; r += T) { // levels wider than the CTA
       PartRow<X, KD> S;
       load_row(r, S);
-      solve_row(S, false);
+      solve_row(S, false, !ring);
     }
   };
 
@@ -486,6 +520,8 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
                  : "memory");
   };
   PartRow<X, KD> R0, R1, R2, R3;
+  PartRow<X, KD> S0, S1; // W2 only
+  S0.r = S1.r = -1;
   l2_ahead(q0 + 3, q0 + 8);
   prefetch(q0, R0);
   prefetch(q0 + 1, R1);
@@ -510,27 +546,29 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
   __syncthreads();
   arm(R0);
   arm(R1);
+  if (W2)
+    prefetch2(q0, S0);
   // four register sets rotate: level q runs, then q+2 is armed and q+3 is
   // fetched (after the solve, so its loads do not delay the solve's reads);
   // one barrier per level, and every thread leaves together if any gave up
   for (int q = q0; q < q1; q += 4) {
-    run_level(q, R0);
+    run_level(q, R0, S0, S1);
     arm(R2);
     l2_ahead(q + 8, q + 12); // four levels per bulk prefetch
     prefetch(q + 3, R3);
     if (__syncthreads_or(aborted) || q + 1 >= q1)
       break;
-    run_level(q + 1, R1);
+    run_level(q + 1, R1, S1, S0);
     arm(R3);
     prefetch(q + 4, R0);
     if (__syncthreads_or(aborted) || q + 2 >= q1)
       break;
-    run_level(q + 2, R2);
+    run_level(q + 2, R2, S0, S1);
     arm(R0);
     prefetch(q + 5, R1);
     if (__syncthreads_or(aborted) || q + 3 >= q1)
       break;
-    run_level(q + 3, R3);
+    run_level(q + 3, R3, S1, S0);
     arm(R1);
     prefetch(q + 6, R2);
     if (__syncthreads_or(aborted))
@@ -566,12 +604,12 @@ void launch_kernel(la_trsv_plan_t P, const X *b, X *x, cudaStream_t st) {
   }
 }
 
-template <typename V, typename X, bool UNIT, int KD>
+template <typename V, typename X, bool UNIT, int KD, bool W2 = false>
 const void *part_fn() {
-  return (const void *)trsv_part_kernel<V, X, UNIT, KD>;
+  return (const void *)trsv_part_kernel<V, X, UNIT, KD, W2>;
 }
 
-template <typename V, typename X, bool UNIT, int KD>
+template <typename V, typename X, bool UNIT, int KD, bool W2 = false>
 cudaError_t launch_parts_kd(la_trsv_plan_t P, const X *b, X *x, cudaStream_t st) {
   const int n = P->n, tail = P->kd == 0;
   const int *ps = P->pstart.as<int>(), *pq = P->psub.as<int>(), *sb = P->sb.as<int>(),
@@ -584,12 +622,15 @@ cudaError_t launch_parts_kd(la_trsv_plan_t P, const X *b, X *x, cudaStream_t st)
                   (void *)&aj, (void *)&av, (void *)&ej, (void *)&ev,  (void *)&dg,
                   (void *)&er, (void *)&b,  (void *)&x,  (void *)&err, (void *)&tail,
                   (void *)&cap, (void *)&mask};
-  return cudaLaunchCooperativeKernel(part_fn<V, X, UNIT, KD>(), dim3(P->nparts),
+  return cudaLaunchCooperativeKernel(part_fn<V, X, UNIT, KD, W2>(), dim3(P->nparts),
                                      dim3(part_threads<X, KD>()), args, P->part_smem, st);
 }
 
 template <typename V, typename X, bool UNIT>
 cudaError_t launch_parts(la_trsv_plan_t P, const X *b, X *x, cudaStream_t st) {
+  if constexpr (sizeof(X) == 4)
+    if (P->w2 && P->kd == 3)
+      return launch_parts_kd<V, X, UNIT, 3, true>(P, b, x, st);
   switch (P->kd) {
   case 3:
     return launch_parts_kd<V, X, UNIT, 3>(P, b, x, st);
@@ -812,7 +853,21 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
   const size_t smem = sizeof(X) * (size_t)(ring ? ring : rows_max) + sb_bytes;
   const void *fns[2];
   int threads = 0;
-  if (ks == 3) {
+  // second-row register sets when some level of a part is wider than the
+  // CTA (FP32 3-slot rows: the only variant whose registers allow them)
+  int widest = 0;
+  for (int g = 0; g < psub[nparts]; g++)
+    widest = std::max(widest, sb[g + 1] - sb[g]);
+  bool w2 = false;
+  if constexpr (sizeof(X) == 4) {
+    w2 = ks == 3 && widest > part_threads<X, 3>();
+    if (w2) {
+      fns[0] = part_fn<X, X, false, 3, true>(), fns[1] = part_fn<X, X, true, 3, true>();
+      threads = part_threads<X, 3>();
+    }
+  }
+  if (w2) {
+  } else if (ks == 3) {
     fns[0] = part_fn<X, X, false, 3>(), fns[1] = part_fn<X, X, true, 3>();
     threads = part_threads<X, 3>();
   } else if (ks == 4) {
@@ -843,7 +898,8 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
   }
   // Modelled critical path (microseconds; B200 measurements): a part takes
   // ~0.35 us per level it holds plus ~1 us for every further round of rows
-  // in a level wider than its CTA, both 1.5x for FP64 (a part's level step
+  // in a level wider than its CTA (~0.3 us for the second round when it is
+  // held in registers, W2), both 1.5x for FP64 (a part's level step
   // measured 1.24 us FP64 against 0.80 us FP32 on the 128^3 IC(0) factor,
   // while the level order costs about the same in both), and a value
   // crossing parts arrives ~1.5 us after it is written; the level-order
@@ -868,8 +924,11 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
         }
         fin[pi] = std::max(fin[pi], t);
       }
-      for (int p : touched)
-        fin[p] += f * (0.35 + 1.0 * ((width[p] + threads - 1) / threads - 1));
+      for (int p : touched) {
+        const int extra = (width[p] + threads - 1) / threads - 1;
+        const double rounds = w2 && extra > 0 ? 0.3 + 1.0 * (extra - 1) : 1.0 * extra;
+        fin[p] += f * (0.35 + rounds);
+      }
       for (int q = P->h_prefix[l]; q < P->h_prefix[l + 1]; q++) {
         const int i = P->h_iperm[q] - base;
         ready[i] = fin[part[i]];
@@ -955,6 +1014,7 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
   P->nparts = nparts;
   P->part_rows = ring ? ring : rows_max;
   P->ring_mask = ring ? ring - 1 : kNoRing;
+  P->w2 = w2;
   P->part_smem = smem;
   P->sched = 1;
   *ok = true;
