@@ -148,9 +148,11 @@ struct la_pcg_s {
   la_spmv_plan_t Ap = nullptr;
   la_trsv_plan_t L = nullptr, U = nullptr;
   la::DevBuf r, z, p, q, t;        // FP64 work vectors
-  la::DevBuf r32, z32, p32, q32, t32, d32; // FP32 inner vectors (mixed)
+  la::DevBuf r32, z32, p32, q32, t32, d32, p32b; // FP32 inner vectors (mixed)
   la::DevBuf scal, partials, ticket;
   la::DevBuf hb, hx;
   int dot_blocks = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double *h_rr = nullptr;       // pinned host copy of the residual norm
+  cudaEvent_t ev_rr = nullptr;  // marks its arrival
 };

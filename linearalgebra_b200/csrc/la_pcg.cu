@@ -24,6 +24,7 @@
 #include "la_internal.h"
 
 #include <cmath>
+#include <utility>
 
 namespace la {
 
@@ -43,7 +44,7 @@ namespace {
 constexpr int kDotThreads = 512;
 
 // Scalar slots in device memory.
-enum { S_RZ = 0, S_PQ, S_RR, S_ALPHA, S_BETA, S_DOT, S_COUNT };
+enum { S_RZ = 0, S_PQ, S_RR, S_ALPHA, S_BETA, S_DOT, S_RZ0, S_COUNT };
 
 // Deterministic FP64 dot with a fused finaliser: every block writes its
 // partial sum, the last block to finish (atomic ticket after a fence) adds
@@ -88,6 +89,7 @@ __global__ void __launch_bounds__(kDotThreads)
     scal[S_ALPHA] = scal[S_RZ] / t;
   } else if (op == OP_BETA) { // beta = (r, z)_new / (r, z)_old
     scal[S_BETA] = t / scal[S_RZ];
+    scal[S_RZ0] = scal[S_RZ]; // kept so that a discarded step can be redone
     scal[S_RZ] = t;
   }
 }
@@ -102,6 +104,16 @@ __global__ void xr_update_kernel(const int n, X *x, X *r, const X *p,
     x[i] = X(double(x[i]) + al * double(p[i]));
     r[i] = X(double(r[i]) - al * double(q[i]));
   }
+}
+
+// pn = z + beta p (out of place: the mixed loop may discard the result)
+template <typename X>
+__global__ void p_next_kernel(const int n, X *pn, const X *p, const X *z,
+                              const double *scal) {
+  const double be = scal[S_BETA];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x)
+    pn[i] = X(double(z[i]) + be * double(p[i]));
 }
 
 // p = z + beta p
@@ -207,8 +219,19 @@ la_status pcg_run(la_pcg_t S, const X *rhs, X *y, X *r, X *z, X *p, X *q,
     LA_TRY(dot(S, p, q, OP_ALPHA, st));
     xr_update_kernel<X><<<g, 256, 0, st>>>(n, y, r, p, q, S->scal.as<double>());
     LA_TRY(dot(S, r, r, OP_STORE, st));
-    double rr;
-    LA_TRY(read_scalar(S, S_DOT, &rr, st));
+    // ||r||^2 travels to the host while the next iteration's preconditioner
+    // and direction update are already queued behind it, so the GPU does
+    // not idle through the host's check.  They write only t, z, p and the
+    // rz scalar: when this iteration is the last, y and r are untouched.
+    LA_CUDA_TRY(cudaMemcpyAsync(S->h_rr, S->scal.as<double>() + S_DOT, sizeof(double),
+                                cudaMemcpyDeviceToHost, st));
+    LA_CUDA_TRY(cudaEventRecord(S->ev_rr, st));
+    LA_TRY(trsv_launch(S->L, r, t, st));
+    LA_TRY(trsv_launch(S->U, t, z, st));
+    LA_TRY(dot(S, r, z, OP_BETA, st));
+    p_update_kernel<X><<<g, 256, 0, st>>>(n, p, z, S->scal.as<double>());
+    LA_CUDA_TRY(cudaEventSynchronize(S->ev_rr));
+    const double rr = *S->h_rr;
     *iters = it;
     const double rel = std::sqrt(rr) / r0;
     *rel_out = rel;
@@ -225,10 +248,6 @@ la_status pcg_run(la_pcg_t S, const X *rhs, X *y, X *r, X *z, X *p, X *q,
       if (trel < tol)
         return LA_OK;
     }
-    LA_TRY(trsv_launch(S->L, r, t, st));
-    LA_TRY(trsv_launch(S->U, t, z, st));
-    LA_TRY(dot(S, r, z, OP_BETA, st));
-    p_update_kernel<X><<<g, 256, 0, st>>>(n, p, z, S->scal.as<double>());
   }
   LA_TRY(trsv_check(S->L, st));
   LA_TRY(trsv_check(S->U, st));
@@ -251,7 +270,8 @@ la_status pcg_mixed(la_pcg_t S, const double *b, double *x, double bn, double rt
                     int maxit, la_pcg_info *loc, cudaStream_t st) {
   const int n = S->n, g = vec_grid(n);
   float *r32 = S->r32.as<float>(), *z32 = S->z32.as<float>(), *p32 = S->p32.as<float>(),
-        *q32 = S->q32.as<float>(), *t32 = S->t32.as<float>(), *d32 = S->d32.as<float>();
+        *q32 = S->q32.as<float>(), *t32 = S->t32.as<float>(), *d32 = S->d32.as<float>(),
+        *pn32 = S->p32b.as<float>();
   double *r64 = S->r.as<double>();
   zero_kernel<<<g, 256, 0, st>>>(n, x);
   LA_CUDA_TRY(cudaMemsetAsync(d32, 0, sizeof(float) * n, st));
@@ -262,16 +282,38 @@ la_status pcg_mixed(la_pcg_t S, const double *b, double *x, double bn, double rt
   LA_TRY(dot(S, r32, z32, OP_STORE, st));
   LA_CUDA_TRY(cudaMemcpyAsync(S->scal.as<double>() + S_RZ, S->scal.as<double>() + S_DOT,
                               sizeof(double), cudaMemcpyDeviceToDevice, st));
-  double rmax = bn, rel = 1.0;
+  double rmax = bn, rel = 1.0, rn_prev = bn;
   int updates = 0, it;
   for (it = 1; it <= maxit; it++) {
     LA_TRY(spmv_launch(S->Ap, 1.0, p32, 0.0, q32, q32, LA_F32, st));
     LA_TRY(dot(S, p32, q32, OP_ALPHA, st));
     xr_update_kernel<float><<<g, 256, 0, st>>>(n, d32, r32, p32, q32, S->scal.as<double>());
     LA_TRY(dot(S, r32, r32, OP_STORE, st));
-    double rr;
-    LA_TRY(read_scalar(S, S_DOT, &rr, st));
+    // As in pcg_run: ||r||^2 travels to the host while the next step's
+    // preconditioner and direction are queued -- when the last residual was
+    // well above the reliable-update threshold, so that no update is likely
+    // now (one iteration in about twenty has one, and a discarded step costs
+    // two triangular solves).  The queued step writes t, z, the next
+    // direction pn and the rz / beta scalars; if an update is due after all,
+    // rz is restored and the step is redone on the new residual.
+    LA_CUDA_TRY(cudaMemcpyAsync(S->h_rr, S->scal.as<double>() + S_DOT, sizeof(double),
+                                cudaMemcpyDeviceToHost, st));
+    LA_CUDA_TRY(cudaEventRecord(S->ev_rr, st));
+    const bool ahead = rn_prev > 0.13 * rmax && rn_prev > 2.0 * rtol * bn;
+    auto precondition = [&]() -> la_status {
+      LA_TRY(trsv_launch(S->L, r32, t32, st));
+      LA_TRY(trsv_launch(S->U, t32, z32, st));
+      LA_TRY(dot(S, r32, z32, OP_BETA, st));
+      p_next_kernel<float><<<g, 256, 0, st>>>(n, pn32, p32, z32, S->scal.as<double>());
+      return LA_OK;
+    };
+    if (ahead)
+      LA_TRY(precondition());
+    LA_CUDA_TRY(cudaEventSynchronize(S->ev_rr));
+    const double rr = *S->h_rr;
     const double rn = std::sqrt(rr);
+    rn_prev = rn;
+    bool updated = false;
     if (!std::isfinite(rn)) {
       set_error("mixed PCG breakdown: non-finite residual at iteration %d", it);
       loc->iterations = it;
@@ -290,11 +332,14 @@ la_status pcg_mixed(la_pcg_t S, const double *b, double *x, double bn, double rt
       if (rel < rtol)
         break;
       scale_copy_kernel<float, double><<<g, 256, 0, st>>>(n, r32, r64, 1.0);
+      updated = true;
     }
-    LA_TRY(trsv_launch(S->L, r32, t32, st));
-    LA_TRY(trsv_launch(S->U, t32, z32, st));
-    LA_TRY(dot(S, r32, z32, OP_BETA, st));
-    p_update_kernel<float><<<g, 256, 0, st>>>(n, p32, z32, S->scal.as<double>());
+    if (ahead && updated) // the queued step used the old residual: redo it
+      LA_CUDA_TRY(cudaMemcpyAsync(S->scal.as<double>() + S_RZ, S->scal.as<double>() + S_RZ0,
+                                  sizeof(double), cudaMemcpyDeviceToDevice, st));
+    if (!ahead || updated)
+      LA_TRY(precondition());
+    std::swap(p32, pn32);
   }
   loc->iterations = std::min(it, maxit);
   loc->outer_iterations = updates;
@@ -315,6 +360,8 @@ la_status pcg_mixed(la_pcg_t S, const double *b, double *x, double bn, double rt
 
 } // namespace
 
+void pcg_destroy(la_pcg_t S);
+
 la_status pcg_create(la_csr_t A, const int *u_ai, const int *u_aj,
                      const double *icc_av, la_pcg_mode mode, la_pcg_t *out) {
   auto *S = new la_pcg_s();
@@ -322,7 +369,7 @@ la_status pcg_create(la_csr_t A, const int *u_ai, const int *u_aj,
   S->mode = mode;
   const int n = S->n = A->n, base = A->base;
   auto fail = [&](la_status s) {
-    delete S;
+    pcg_destroy(S);
     return s;
   };
   // Preconditioner factors: strict U + diag, and strict L = U^T (same diag).
@@ -374,7 +421,7 @@ la_status pcg_create(la_csr_t A, const int *u_ai, const int *u_aj,
     if ((s = b->alloc(v8)) != LA_OK)
       return fail(s);
   if (mode == LA_PCG_MIXED)
-    for (DevBuf *b : {&S->r32, &S->z32, &S->p32, &S->q32, &S->t32, &S->d32})
+    for (DevBuf *b : {&S->r32, &S->z32, &S->p32, &S->q32, &S->t32, &S->d32, &S->p32b})
       if ((s = b->alloc(v4)) != LA_OK)
         return fail(s);
   S->dot_blocks = std::max(1, std::min(2 * sm_count(), (n + kDotThreads - 1) / kDotThreads));
@@ -383,7 +430,9 @@ la_status pcg_create(la_csr_t A, const int *u_ai, const int *u_aj,
       (s = S->ticket.alloc(sizeof(unsigned))) != LA_OK)
     return fail(s);
   if (cudaMemset(S->ticket.p, 0, sizeof(unsigned)) != cudaSuccess ||
-      cudaEventCreate(&S->ev0) != cudaSuccess || cudaEventCreate(&S->ev1) != cudaSuccess) {
+      cudaEventCreate(&S->ev0) != cudaSuccess || cudaEventCreate(&S->ev1) != cudaSuccess ||
+      cudaEventCreateWithFlags(&S->ev_rr, cudaEventDisableTiming) != cudaSuccess ||
+      cudaMallocHost((void **)&S->h_rr, sizeof(double)) != cudaSuccess) {
     set_error("PCG setup: CUDA error");
     return fail(LA_ERR_CUDA);
   }
@@ -454,6 +503,10 @@ void pcg_destroy(la_pcg_t S) {
     cudaEventDestroy(S->ev0);
   if (S->ev1)
     cudaEventDestroy(S->ev1);
+  if (S->ev_rr)
+    cudaEventDestroy(S->ev_rr);
+  if (S->h_rr)
+    cudaFreeHost(S->h_rr);
   delete S->L;
   delete S->U;
   delete S->Ap;
