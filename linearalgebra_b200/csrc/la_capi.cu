@@ -19,6 +19,8 @@ la_status spmv_noalloc(la_spmv_kind kind, int n, int nnz, int base, const int *a
                        const int *aj, const double *av, double alpha, const double *x,
                        double beta, double *y, cudaStream_t st);
 la_status spmv_plan_build(la_spmv_plan_t P);
+la_status spmv_host_chunked(la_spmv_plan_t P, double alpha, const double *x, double beta,
+                            double *y);
 la_status trsv_launch(la_trsv_plan_t P, const void *b, void *x,
                       cudaStream_t st);
 la_status trsv_build(la_trsv_plan_t P, const int *ai, const int *aj,
@@ -256,18 +258,7 @@ la_status la_spmv(la_spmv_plan_t plan, double alpha, const void *x,
 la_status la_spmv_host(la_spmv_plan_t plan, double alpha, const double *x,
                        double beta, double *y) {
   LA_CHECK_ARG(plan && x && y, "arguments");
-  const la_csr_t A = plan->A;
-  if (!plan->hx.p) {
-    LA_TRY(plan->hx.alloc(sizeof(double) * std::max(A->ncols, 1)));
-    LA_TRY(plan->hy.alloc(sizeof(double) * std::max(A->n, 1)));
-  }
-  LA_CUDA_TRY(cudaMemcpy(plan->hx.p, x, sizeof(double) * A->ncols, cudaMemcpyHostToDevice));
-  if (beta != 0.0)
-    LA_CUDA_TRY(cudaMemcpy(plan->hy.p, y, sizeof(double) * A->n, cudaMemcpyHostToDevice));
-  LA_TRY(spmv_launch(plan, alpha, plan->hx.p, beta, plan->hy.p, plan->hy.p,
-                     LA_F64, nullptr));
-  LA_CUDA_TRY(cudaMemcpy(y, plan->hy.p, sizeof(double) * A->n, cudaMemcpyDeviceToHost));
-  return LA_OK;
+  return spmv_host_chunked(plan, alpha, x, beta, y);
 }
 
 la_status la_spmv_plan_destroy(la_spmv_plan_t plan) {

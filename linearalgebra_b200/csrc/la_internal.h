@@ -112,8 +112,21 @@ struct la_spmv_plan_s {
   // lazily built transpose for the adjoint
   la_csr_t At = nullptr;
   la_spmv_plan_t Atplan = nullptr;
-  // host staging for la_spmv_host
+  std::vector<int> h_tile_row, h_group_end; // host copies (chunked host-pointer calls)
+  // host staging for la_spmv_host: device copies of x and y, a stream for the
+  // tile chunks, one for copying finished rows out, an event per chunk
   la::DevBuf hx, hy;
+  cudaStream_t hst = nullptr, hcp = nullptr;
+  cudaEvent_t hev[8] = {};
+  ~la_spmv_plan_s() {
+    for (cudaEvent_t e : hev)
+      if (e)
+        cudaEventDestroy(e);
+    if (hst)
+      cudaStreamDestroy(hst);
+    if (hcp)
+      cudaStreamDestroy(hcp);
+  }
 };
 
 struct la_trsv_plan_s {

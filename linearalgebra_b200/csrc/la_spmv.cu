@@ -146,14 +146,17 @@ template <typename X> struct XParts {
 // gather reads column j from the slice that owns it (XParts) instead of x.
 // LONG = false drops the warp path for in-tile segments longer than kLongRow
 // (and its second barrier); the plan selects it when no row is that long.
-template <int FORM, typename V, typename X, typename ACC, bool XP = false, bool LONG = true>
+// CHUNK: the grid covers tiles [tile0, tile0 + grid) (chunked host-pointer
+// calls); otherwise tile0 is not read, which keeps the kernel's schedule.
+template <int FORM, typename V, typename X, typename ACC, bool XP = false, bool LONG = true,
+          bool CHUNK = false>
 __global__ void __launch_bounds__(kThreads, kTileBlocksPerSm)
     spmv_tile_kernel(const int n, const int nnz, const int base,
                      const int *__restrict__ ai, const int *__restrict__ aj,
                      const V *__restrict__ av, const X *__restrict__ x, X *y,
                      const X *yin, const ACC alpha, const ACC beta,
                      const int *__restrict__ tile_row, ACC *part,
-                     const XParts<X> xp = XParts<X>{}) {
+                     const XParts<X> xp = XParts<X>{}, const int tile0 = 0) {
   __shared__ ACC prod[kTile];
   __shared__ int rp[kRowCap];
   __shared__ int long_rows[kLongCap];
@@ -174,7 +177,7 @@ __global__ void __launch_bounds__(kThreads, kTileBlocksPerSm)
   // let the merge kernel's launch overlap this grid
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const RowOut<FORM, ACC> out{alpha, beta};
-  const int t = blockIdx.x, tid = threadIdx.x;
+  const int t = CHUNK ? blockIdx.x + tile0 : blockIdx.x, tid = threadIdx.x;
   const TileRows T = tile_rows(t, n, nnz, tile_row);
   if (LONG && tid == 0)
     n_long = 0;
@@ -270,15 +273,21 @@ __global__ void __launch_bounds__(kThreads, kTileBlocksPerSm)
 // wait for the tile pass and the partials' loads do not depend on one
 // another.  Without group_end (the allocation-free path, whose tile rows are
 // computed on the device) the group is found by scanning tile_row.
-template <int FORM, typename X, typename ACC>
+// After the tile pass over tiles [t0, t1) only (a chunk of a host-pointer
+// call), the groups whose last tile lies in that range are merged; threads
+// start at f0, the first tile of the group holding tile t0.
+template <int FORM, typename X, typename ACC, bool CHUNK = false>
 __global__ void __launch_bounds__(256)
     spmv_merge_kernel(const int ntiles, X *y, const X *yin, const ACC beta,
                       const int *__restrict__ tile_row, const ACC *part,
-                      const int *__restrict__ group_end) {
-  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+                      const int *__restrict__ group_end, const int f0 = 0, const int t0 = 0,
+                      const int t1 = 0) {
+  const int f = (CHUNK ? f0 : 0) + blockIdx.x * blockDim.x + threadIdx.x;
   int R = 0, e = -1;
   if (group_end && f < ntiles) {
     e = group_end[f];
+    if (CHUNK && (e - 1 < t0 || e - 1 >= t1)) // a head whose group ends elsewhere
+      e = -1;
     if (e >= 0)
       R = tile_row[f];
   }
@@ -351,10 +360,12 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// Tiles [tile0, tile1) only when tile1 >= 0 (a chunk of a host-pointer call:
+// the plan's host copies of tile_row and group_end give the merge range).
 template <int FORM, typename V, typename X, typename ACC, bool XP = false>
 la_status launch_form(la_spmv_plan_t P, const V *av, ACC alpha, const X *x,
                       ACC beta, X *y, const X *yin, cudaStream_t st,
-                      const XParts<X> &xp = XParts<X>{}) {
+                      const XParts<X> &xp = XParts<X>{}, int tile0 = 0, int tile1 = -1) {
   const la_csr_t A = P->A;
   if (A->n == 0)
     return LA_OK;
@@ -364,14 +375,24 @@ la_status launch_form(la_spmv_plan_t P, const V *av, ACC alpha, const X *x,
     LA_CUDA_TRY(cudaGetLastError());
     return LA_OK;
   }
-  auto tile = P->long_rows ? spmv_tile_kernel<FORM, V, X, ACC, XP, true>
-                           : spmv_tile_kernel<FORM, V, X, ACC, XP, false>;
-  tile<<<P->ntiles, kThreads, 0, st>>>(A->n, A->nnz, A->base, A->ai.as<int>(),
-                                       A->aj.as<int>(), av, x, y, yin, alpha, beta,
-                                       P->tile_row.as<int>(), P->part.as<ACC>(), xp);
+  const bool chunk = tile1 >= 0;
+  auto tile = chunk ? (P->long_rows ? spmv_tile_kernel<FORM, V, X, ACC, XP, true, true>
+                                    : spmv_tile_kernel<FORM, V, X, ACC, XP, false, true>)
+                    : (P->long_rows ? spmv_tile_kernel<FORM, V, X, ACC, XP, true>
+                                    : spmv_tile_kernel<FORM, V, X, ACC, XP, false>);
+  if (tile1 < 0)
+    tile1 = P->ntiles;
+  int f0 = 0;
+  if (tile0 > 0)
+    for (f0 = tile0; f0 > 0 && P->h_group_end[f0] < 0;)
+      f0--;
+  tile<<<tile1 - tile0, kThreads, 0, st>>>(A->n, A->nnz, A->base, A->ai.as<int>(),
+                                           A->aj.as<int>(), av, x, y, yin, alpha, beta,
+                                           P->tile_row.as<int>(), P->part.as<ACC>(), xp,
+                                           tile0);
   LA_CUDA_TRY(cudaGetLastError());
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((P->ntiles + 255) / 256);
+  cfg.gridDim = dim3((tile1 - f0 + 255) / 256);
   cfg.blockDim = dim3(256);
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
@@ -383,8 +404,12 @@ la_status launch_form(la_spmv_plan_t P, const V *av, ACC alpha, const X *x,
   const int *tr = P->tile_row.as<int>();
   const ACC *pt = P->part.as<ACC>();
   const int *ge = P->group_end.as<int>();
-  LA_CUDA_TRY(cudaLaunchKernelEx(&cfg, spmv_merge_kernel<FORM, X, ACC>, nt, y, yin, beta,
-                                 tr, pt, ge));
+  if (chunk)
+    LA_CUDA_TRY(cudaLaunchKernelEx(&cfg, spmv_merge_kernel<FORM, X, ACC, true>, nt, y, yin,
+                                   beta, tr, pt, ge, f0, tile0, tile1));
+  else
+    LA_CUDA_TRY(cudaLaunchKernelEx(&cfg, spmv_merge_kernel<FORM, X, ACC>, nt, y, yin, beta,
+                                   tr, pt, ge, f0, tile0, tile1));
   return LA_OK;
 }
 
@@ -502,6 +527,8 @@ la_status spmv_plan_build(la_spmv_plan_t P) {
     f = e;
   }
   LA_TRY(P->group_end.upload(gend.data(), sizeof(int) * gend.size()));
+  P->h_tile_row = trow;
+  P->h_group_end = gend;
   int longest = 0;
   for (int r = 0; r < n; r++)
     longest = std::max(longest, ai[r + 1] - ai[r]);
@@ -512,6 +539,58 @@ la_status spmv_plan_build(la_spmv_plan_t P) {
 }
 
 int spmv_tile_nnz() { return kTile; }
+
+// la_spmv_host, FP64: x in, the tiles in up to 8 chunks on one stream, and
+// after each chunk the rows it finished -- those below the next chunk's first
+// tile row; that row may still get partials -- copied out on a second stream,
+// so the copy of y overlaps the rest of the computation.  The same tiles,
+// partials and merge order as one launch: bit-identical to la_spmv.
+la_status spmv_host_chunked(la_spmv_plan_t P, double alpha, const double *x, double beta,
+                            double *y) {
+  const la_csr_t A = P->A;
+  const int n = A->n;
+  if (!P->hx.p) {
+    LA_TRY(P->hx.alloc(sizeof(double) * std::max(A->ncols, 1)));
+    LA_TRY(P->hy.alloc(sizeof(double) * std::max(n, 1)));
+    // blocking streams: ordered after work on the legacy default stream, as
+    // the synchronous copies of this call always were
+    LA_CUDA_TRY(cudaStreamCreate(&P->hst));
+    LA_CUDA_TRY(cudaStreamCreate(&P->hcp));
+    for (cudaEvent_t &e : P->hev)
+      LA_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  double *hx = P->hx.as<double>(), *hy = P->hy.as<double>();
+  LA_CUDA_TRY(cudaMemcpyAsync(hx, x, sizeof(double) * A->ncols, cudaMemcpyHostToDevice, P->hst));
+  if (beta != 0.0)
+    LA_CUDA_TRY(cudaMemcpyAsync(hy, y, sizeof(double) * n, cudaMemcpyHostToDevice, P->hst));
+  const int nt = P->ntiles, chunks = std::min(8, nt);
+  if (chunks <= 1 || A->dtype != LA_F64) {
+    LA_TRY(spmv_launch(P, alpha, hx, beta, hy, hy, LA_F64, P->hst));
+    LA_CUDA_TRY(cudaMemcpyAsync(y, hy, sizeof(double) * n, cudaMemcpyDeviceToHost, P->hst));
+    LA_CUDA_TRY(cudaStreamSynchronize(P->hst));
+    return LA_OK;
+  }
+  const double *av = A->av.as<double>();
+  for (int c = 0; c < chunks; c++) {
+    const int t0 = (int)((long long)nt * c / chunks), t1 = (int)((long long)nt * (c + 1) / chunks);
+    la_status s = P->kind == LA_SPMV_ALBUS
+                      ? launch_form<kAlbus>(P, av, alpha, (const double *)hx, beta, hy,
+                                            (const double *)hy, P->hst, XParts<double>{}, t0, t1)
+                      : launch_form<kSegSum>(P, av, alpha, (const double *)hx, beta, hy,
+                                             (const double *)hy, P->hst, XParts<double>{}, t0,
+                                             t1);
+    LA_TRY(s);
+    const int r0 = c == 0 ? 0 : P->h_tile_row[t0], r1 = c == chunks - 1 ? n : P->h_tile_row[t1];
+    LA_CUDA_TRY(cudaEventRecord(P->hev[c], P->hst));
+    LA_CUDA_TRY(cudaStreamWaitEvent(P->hcp, P->hev[c], 0));
+    if (r1 > r0)
+      LA_CUDA_TRY(cudaMemcpyAsync(y + r0, hy + r0, sizeof(double) * (r1 - r0),
+                                  cudaMemcpyDeviceToHost, P->hcp));
+  }
+  LA_CUDA_TRY(cudaStreamSynchronize(P->hcp));
+  LA_CUDA_TRY(cudaStreamSynchronize(P->hst));
+  return LA_OK;
+}
 
 // ---------------------------------------------------------------------------
 // Allocation-free SpMV (la_spmv_noalloc).  The per-call scratch of the tile
@@ -607,8 +686,9 @@ la_status noalloc_launch(int n, int nnz, int base, const int *ai, const int *aj,
   cfg.numAttrs = 1;
   const double *yin = y, *pt = part;
   const int *tr = tile_row, *ge = nullptr;
+  const int f0 = 0, t0 = 0, t1 = ntiles;
   LA_CUDA_TRY(cudaLaunchKernelEx(&cfg, spmv_merge_kernel<FORM, double, double>, ntiles, y,
-                                 yin, beta, tr, pt, ge));
+                                 yin, beta, tr, pt, ge, f0, t0, t1));
   return LA_OK;
 }
 } // namespace

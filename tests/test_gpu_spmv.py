@@ -163,6 +163,30 @@ def test_spmv_edge_cases(lab, orc, kind):
 
 
 @pytest.mark.parametrize("kind", KINDS)
+def test_spmv_host_path_chunks_bit_identical(lab, kind):
+    """The host-pointer call runs the plan's tiles in up to 8 chunks and copies
+    each chunk's finished rows out while the next runs: bit for bit the
+    device call's result, including rows that span chunk edges (power-law
+    rows up to 20,000 long; one 20,000-long row among tiny ones), empty rows
+    on tile edges, and beta != 0 with y in place."""
+    from linearalgebra_b200 import gen
+    rng = np.random.default_rng(5)
+    n, ai, aj, av = gen.powerlaw(200_000, seed=3)
+    mats = [("powerlaw_200k", n, n, ai, aj, av)] + _edge_matrices()
+    for name, m, n, ai, aj, av in mats:
+        A = lab.CSR(m, n, 0, ai, aj, av)
+        plan = lab.SPMV(A, kind_id(lab, kind))
+        x = rng.uniform(-1, 1, n)
+        y0 = rng.uniform(-1, 1, m)
+        for alpha, beta in ((1.0, 0.0), (-1.5, 0.5)):
+            yd = dev(y0)
+            plan(dev(x), yd, alpha, beta)
+            yh = y0.copy()
+            plan(x, yh, alpha, beta)
+            assert np.array_equal(yh, yd.cpu().numpy()), (name, kind, alpha, beta)
+
+
+@pytest.mark.parametrize("kind", KINDS)
 def test_spmv_beta_zero_does_not_read_y_and_base1(lab, orc, golden, kind):
     ai, aj, av = golden["rdist1/ai"], golden["rdist1/aj"], golden["rdist1/av"]
     n = len(ai) - 1
