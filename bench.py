@@ -420,6 +420,23 @@ def run_case(case):
         y = torch.empty_like(x)
         for _ in range(3):
             P(x, y)
+    elif case == "trsv-c5-f32":
+        # FP32 lower solve of the RCM-ordered 192^3 anisotropic IC(0) factor:
+        # the partitioned kernel with second-row register sets
+        n, ai, aj, av = gen.aniso7(192, seed=0)
+        iperm, perm = la.SerialCM(n, 0, ai, aj)
+        b_ai, b_aj, b_av = la.Permute(n, 0, ai, aj, av, iperm, perm)
+        ua, uj, uv = gen.upper_with_diag(n, b_ai, b_aj, b_av)
+        f = la.ICCLevelNumeric0(n, 0, ua, uj, uv)
+        _, d, (s_ai, s_aj, s_av) = la.SplitLDU(n, 0, ua, uj, f)
+        t_ai, t_aj, t_av = la.Transpose(n, n, 0, s_ai, s_aj, s_av)
+        ts = la.OptimizedTriangularSolve("L", dtype=np.float32).analysis(n, 0, t_ai, t_aj,
+                                                                        t_av, d)
+        b = torch.as_tensor(gen.uniform_vector(n, 0)).to("cuda", torch.float32)
+        x = torch.empty_like(b)
+        for _ in range(3):
+            ts(b, x)
+        print("schedule", ts.schedule())
     else:
         n, ai, aj, av = gen.laplacian_3d(128)
         iperm, perm = la.SerialCM(n, 0, ai, aj)
@@ -451,7 +468,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-cpu-pcg", action="store_true")
     ap.add_argument("--case", default=None,
-                    choices=["spmv-powerlaw", "spmv-lap3d", "trsv-lap3d", "pcg-lap3d"],
+                    choices=["spmv-powerlaw", "spmv-lap3d", "trsv-lap3d", "trsv-c5-f32",
+                             "pcg-lap3d"],
                     help="run one kernel workload a few times and exit (for ncu)")
     args = ap.parse_args()
     args.steps_given = args.steps is not None
