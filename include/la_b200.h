@@ -242,6 +242,19 @@ la_status la_trsv_analysis_levels(la_uplo uplo, int n, int base,
                                   la_dtype dtype, const int *iperm,
                                   const int *prefix, int nlevels,
                                   la_trsv_plan_t *out);
+/* The transposed solve: a plan that solves with T^T, given the CSR of the
+ * strict triangle T (`uplo` names T's triangle; the plan's is the other).
+ * With diag = NULL and T strict upper this is ForwardSubstitutionT
+ * (triangle_solve.hpp:87-98: the unit lower solve with L = U^T, which the
+ * reference runs as a column scatter); with a diag, (T^T + D) x = b.  T^T
+ * is formed on the host once (ParallelTranspose2 order, matrix_utils.hpp:
+ * 311-390), then planned as la_trsv_analysis does.  The scatter subtracts
+ * each product from x_j in turn while the plan sums a row first: FP64
+ * results agree to rounding, not bit for bit. */
+la_status la_trsv_analysis_transposed(la_uplo uplo, int n, int base, const int *ai,
+                                      const int *aj, const double *av,
+                                      const double *diag, la_dtype dtype,
+                                      la_trsv_plan_t *out);
 /* x = T^-1 b (triangle_solve.tpp:115-155 operator()/BarrierOp): b, x device
  * arrays of the plan's dtype; b and x must not alias.  LA_ERR_TIMEOUT if a
  * dependency wait exceeded its bound (x is then undefined). */

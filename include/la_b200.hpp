@@ -170,6 +170,23 @@ private:
   la_trsv_plan_t _plan{nullptr};
 };
 
+// ForwardSubstitutionT (triangle_solve.hpp:87-98): x = (I + U^T)^-1 b for the
+// strict upper triangle U given as CSR, host arrays.  Plans the transposed
+// solve on the GPU (la_trsv_analysis_transposed) and runs it once; FP64
+// results agree with the reference's column scatter to rounding.
+template <typename ROWTYPE, typename COLTYPE, typename VALTYPE>
+void ForwardSubstitutionT(const COLTYPE size, const int base, ROWTYPE const *ai,
+                          COLTYPE const *aj, VALTYPE const *av,
+                          VALTYPE const *const b, VALTYPE *const x) {
+  require_int_double<ROWTYPE, COLTYPE, VALTYPE>();
+  la_trsv_plan_t plan = nullptr;
+  check(la_trsv_analysis_transposed(LA_UPPER, size, base, ai, aj, av, nullptr, LA_F64, &plan),
+        "la_trsv_analysis_transposed");
+  const la_status s = la_trsv_host(plan, b, x);
+  la_trsv_plan_destroy(plan);
+  check(s, "la_trsv_host");
+}
+
 // TopologicalSort2<TS> (matrix_utils.hpp:637-675), bit-identical output.
 template <TriangularMatrix TS = L, typename ROWTYPE, typename COLTYPE,
           typename VEC>

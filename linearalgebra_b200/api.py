@@ -38,7 +38,7 @@ __all__ = [
     "CSR", "SPMV", "SegSumSPMV", "ALBUSSPMV", "OptimizedTriangularSolve",
     "TopologicalSort2", "SplitLDU", "SplitTriangle", "Transpose", "Permute",
     "ValidCSR", "ICCLevelNumeric0", "ICCShifted", "SerialCM", "PCG", "LAError",
-    "spmv_transpose", "sddmm_pattern",
+    "spmv_transpose", "sddmm_pattern", "ForwardSubstitutionT",
 ]
 
 
@@ -224,6 +224,21 @@ class OptimizedTriangularSolve:
         self.n = int(rows)
         return self
 
+    def analysis_transposed(self, rows, base, ai, aj, av, diag=None):
+        """Plan the solve with T^T, given the CSR of the strict triangle T of
+        the other kind (strict U for an "L" solver); the role
+        ForwardSubstitutionT (triangle_solve.hpp:87-98) plays."""
+        ai, aj, av = _i32(ai), _i32(aj), _f64(av)
+        d = None if diag is None else _f64(diag)
+        h = C.c_void_p()
+        t_uplo = LA_UPPER if self.uplo == LA_LOWER else LA_LOWER
+        call("la_trsv_analysis_transposed", t_uplo, int(rows), int(base), _ptr(ai),
+             _ptr(aj), _ptr(av), _ptr(d),
+             LA_F64 if self.dtype == np.float64 else LA_F32, C.byref(h))
+        self.h = h
+        self.n = int(rows)
+        return self
+
     def analysis_levels(self, rows, base, ai, aj, av, iperm, prefix, diag=None):
         """analysis() with a caller-built level structure (iperm, prefix)."""
         ai, aj, av = _i32(ai), _i32(aj), _f64(av)
@@ -277,6 +292,15 @@ class OptimizedTriangularSolve:
 
 
 # --------------------------------------------------------- host analysis
+def ForwardSubstitutionT(size, base, ai, aj, av, b, x):
+    """``ForwardSubstitutionT`` (triangle_solve.hpp:87-98): x = (I + U^T)^-1 b
+    for the strict upper triangle U given as CSR; host arrays, x written in
+    place.  Plans the transposed solve on the GPU and runs it once."""
+    ts = OptimizedTriangularSolve("L").analysis_transposed(size, base, ai, aj, av)
+    ts(np.ascontiguousarray(b, np.float64), x)
+    return x
+
+
 def TopologicalSort2(uplo, nodes, base, ai, aj):
     """Level sets (matrix_utils.hpp:637-675): returns (levels, iperm, prefix)."""
     ai, aj = _i32(ai), _i32(aj)

@@ -518,6 +518,25 @@ la_status la_trsv_analysis_levels(la_uplo uplo, int n, int base, const int *ai,
                             nlevels, out);
 }
 
+la_status la_trsv_analysis_transposed(la_uplo uplo, int n, int base, const int *ai,
+                                      const int *aj, const double *av,
+                                      const double *diag, la_dtype dtype,
+                                      la_trsv_plan_t *out) {
+  LA_CHECK_ARG(out && ai && n >= 0, "arguments");
+  LA_CHECK_ARG(uplo == LA_LOWER || uplo == LA_UPPER, "uplo");
+  std::string why;
+  if (!valid_csr(n, n, base, ai, aj, &why)) {
+    set_error("invalid CSR: %s", why.c_str());
+    return LA_ERR_BAD_CSR;
+  }
+  const int nnz = ai[n] - base;
+  std::vector<int> tai(n + 1), taj(std::max(nnz, 1));
+  std::vector<double> tav(std::max(nnz, 1));
+  transpose(n, n, base, ai, aj, av, tai.data(), taj.data(), tav.data());
+  return trsv_analysis_impl(uplo == LA_LOWER ? LA_UPPER : LA_LOWER, n, base, tai.data(),
+                            taj.data(), tav.data(), diag, dtype, nullptr, nullptr, 0, out);
+}
+
 la_status la_trsv(la_trsv_plan_t plan, const void *b, void *x,
                   la_stream_t stream) {
   LA_CHECK_ARG(plan && ((b && x) || plan->n == 0), "arguments");
