@@ -867,6 +867,7 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
     }
   }
   if (w2) {
+    // fns and threads set above
   } else if (ks == 3) {
     fns[0] = part_fn<X, X, false, 3>(), fns[1] = part_fn<X, X, true, 3>();
     threads = part_threads<X, 3>();
