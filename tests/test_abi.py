@@ -63,3 +63,24 @@ def test_invalid_csr_rejected_before_device(lab):
         lab.CSR(2, 2, 0, np.array([0, 2, 3], np.int32), np.array([1, 0, 1], np.int32),
                 np.ones(3))
     assert e.value.name == "LA_ERR_BAD_CSR"
+
+
+def test_transposed_solve_analysis_checks_before_device(lab):
+    """la_trsv_analysis_transposed validates T's CSR on the host before it
+    needs a GPU (unsorted columns -> LA_ERR_BAD_CSR); a strict upper triangle
+    it accepts, and without a GPU it then fails loudly (LA_ERR_NO_DEVICE)."""
+    ts = lab.OptimizedTriangularSolve("L")
+    with pytest.raises(lab.LAError) as e:
+        ts.analysis_transposed(3, 0, np.array([0, 2, 3, 3], np.int32),
+                               np.array([2, 1, 2], np.int32), np.ones(3))
+    assert e.value.name == "LA_ERR_BAD_CSR"
+    # T upper -> T^T lower: an entry of T below its diagonal is not allowed
+    with pytest.raises(lab.LAError) as e:
+        ts.analysis_transposed(2, 0, np.array([0, 0, 1], np.int32),
+                               np.array([0], np.int32), np.ones(1))
+    assert e.value.name == "LA_ERR_INVALID_ARG"
+    if not gpu_available():
+        with pytest.raises(lab.LAError) as e:
+            ts.analysis_transposed(3, 0, np.array([0, 2, 3, 3], np.int32),
+                                   np.array([1, 2, 2], np.int32), np.ones(3))
+        assert e.value.name == "LA_ERR_NO_DEVICE"
