@@ -170,6 +170,69 @@ private:
   la_trsv_plan_t _plan{nullptr};
 };
 
+// The reference's free solve functions (triangle_solve.hpp:32-145), host
+// arrays, same signatures.  Each call plans the triangle on the GPU, solves
+// once and releases the plan; for repeated solves keep an
+// OptimizedTriangularSolve.  Results are bit-identical to the reference's
+// (per row: the sum in stored order, then b - sum, / diag).
+namespace detail {
+inline void solve_with(la_trsv_plan_t plan, la_status made, const double *b, double *x) {
+  check(made, "la_trsv_analysis");
+  const la_status s = la_trsv_host(plan, b, x);
+  la_trsv_plan_destroy(plan);
+  check(s, "la_trsv_host");
+}
+} // namespace detail
+
+// ForwardSubstitution (triangle_solve.hpp:32-43): unit lower, strict L CSR.
+template <typename ROWTYPE, typename COLTYPE, typename VALTYPE>
+void ForwardSubstitution(const COLTYPE size, const int base, ROWTYPE const *ai,
+                         COLTYPE const *aj, VALTYPE const *av, VALTYPE const *const b,
+                         VALTYPE *const x) {
+  require_int_double<ROWTYPE, COLTYPE, VALTYPE>();
+  la_trsv_plan_t p = nullptr;
+  const la_status s = la_trsv_analysis(LA_LOWER, size, base, ai, aj, av, nullptr, LA_F64, &p);
+  detail::solve_with(p, s, b, x);
+}
+
+// BackwardSubstitution (triangle_solve.hpp:59-71): strict U CSR + diag.
+template <typename ROWTYPE, typename COLTYPE, typename VALTYPE>
+void BackwardSubstitution(const COLTYPE size, const int base, ROWTYPE const *ai,
+                          COLTYPE const *aj, VALTYPE const *av, VALTYPE const *diag,
+                          VALTYPE const *const b, VALTYPE *const x) {
+  require_int_double<ROWTYPE, COLTYPE, VALTYPE>();
+  la_trsv_plan_t p = nullptr;
+  const la_status s = la_trsv_analysis(LA_UPPER, size, base, ai, aj, av, diag, LA_F64, &p);
+  detail::solve_with(p, s, b, x);
+}
+
+// LevelScheduleForward/BackwardSubstitution (triangle_solve.hpp:100-145):
+// the caller's level structure (iperm with base, zero-based prefix).
+template <typename ROWTYPE, typename COLTYPE, typename VALTYPE>
+void LevelScheduleForwardSubstitution(COLTYPE const *iperm, COLTYPE const *prefix,
+                                      const COLTYPE lvls, const COLTYPE rows, const int base,
+                                      ROWTYPE const *ai, COLTYPE const *aj, VALTYPE const *av,
+                                      VALTYPE const *const b, VALTYPE *const x) {
+  require_int_double<ROWTYPE, COLTYPE, VALTYPE>();
+  la_trsv_plan_t p = nullptr;
+  const la_status s = la_trsv_analysis_levels(LA_LOWER, rows, base, ai, aj, av, nullptr,
+                                              LA_F64, iperm, prefix, lvls, &p);
+  detail::solve_with(p, s, b, x);
+}
+
+template <typename ROWTYPE, typename COLTYPE, typename VALTYPE>
+void LevelScheduleBackwardSubstitution(COLTYPE const *iperm, COLTYPE const *prefix,
+                                       const COLTYPE lvls, const COLTYPE rows, const int base,
+                                       ROWTYPE const *ai, COLTYPE const *aj, VALTYPE const *av,
+                                       VALTYPE const *diag, VALTYPE const *const b,
+                                       VALTYPE *const x) {
+  require_int_double<ROWTYPE, COLTYPE, VALTYPE>();
+  la_trsv_plan_t p = nullptr;
+  const la_status s = la_trsv_analysis_levels(LA_UPPER, rows, base, ai, aj, av, diag,
+                                              LA_F64, iperm, prefix, lvls, &p);
+  detail::solve_with(p, s, b, x);
+}
+
 // ForwardSubstitutionT (triangle_solve.hpp:87-98): x = (I + U^T)^-1 b for the
 // strict upper triangle U given as CSR, host arrays.  Plans the transposed
 // solve on the GPU (la_trsv_analysis_transposed) and runs it once; FP64

@@ -38,7 +38,9 @@ __all__ = [
     "CSR", "SPMV", "SegSumSPMV", "ALBUSSPMV", "OptimizedTriangularSolve",
     "TopologicalSort2", "SplitLDU", "SplitTriangle", "Transpose", "Permute",
     "ValidCSR", "ICCLevelNumeric0", "ICCShifted", "SerialCM", "PCG", "LAError",
-    "spmv_transpose", "sddmm_pattern", "ForwardSubstitutionT",
+    "spmv_transpose", "sddmm_pattern", "ForwardSubstitutionT", "ForwardSubstitution",
+    "BackwardSubstitution", "LevelScheduleForwardSubstitution",
+    "LevelScheduleBackwardSubstitution",
 ]
 
 
@@ -292,6 +294,36 @@ class OptimizedTriangularSolve:
 
 
 # --------------------------------------------------------- host analysis
+def ForwardSubstitution(size, base, ai, aj, av, b, x):
+    """``ForwardSubstitution`` (triangle_solve.hpp:32-43): unit lower solve with
+    the strict lower CSR, host arrays, x written in place (one GPU plan and
+    solve per call; keep an OptimizedTriangularSolve for repeated solves)."""
+    OptimizedTriangularSolve("L").analysis(size, base, ai, aj, av)(_f64(b), x)
+    return x
+
+
+def BackwardSubstitution(size, base, ai, aj, av, diag, b, x):
+    """``BackwardSubstitution`` (triangle_solve.hpp:59-71): strict upper CSR
+    plus diag, host arrays, x written in place."""
+    OptimizedTriangularSolve("U").analysis(size, base, ai, aj, av, diag)(_f64(b), x)
+    return x
+
+
+def LevelScheduleForwardSubstitution(iperm, prefix, lvls, rows, base, ai, aj, av, b, x):
+    """``LevelScheduleForwardSubstitution`` (triangle_solve.hpp:100-122) with the
+    caller's levels (iperm with base, zero-based prefix[lvls + 1])."""
+    OptimizedTriangularSolve("L").analysis_levels(
+        rows, base, ai, aj, av, iperm, _i32(prefix)[:int(lvls) + 1])(_f64(b), x)
+    return x
+
+
+def LevelScheduleBackwardSubstitution(iperm, prefix, lvls, rows, base, ai, aj, av, diag, b, x):
+    """``LevelScheduleBackwardSubstitution`` (triangle_solve.hpp:124-145)."""
+    OptimizedTriangularSolve("U").analysis_levels(
+        rows, base, ai, aj, av, iperm, _i32(prefix)[:int(lvls) + 1], diag)(_f64(b), x)
+    return x
+
+
 def ForwardSubstitutionT(size, base, ai, aj, av, b, x):
     """``ForwardSubstitutionT`` (triangle_solve.hpp:87-98): x = (I + U^T)^-1 b
     for the strict upper triangle U given as CSR; host arrays, x written in

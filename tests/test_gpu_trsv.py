@@ -236,6 +236,53 @@ def test_trsv_schedules_bit_identical(lab, orc, monkeypatch, schedule):
             assert np.array_equal(x32, y32), (n, uplo, "fp32 schedules differ")
 
 
+def test_reference_free_solves_bit_exact(lab, orc, golden):
+    """The reference's free functions with their host-array signatures --
+    ForwardSubstitution, BackwardSubstitution and the two level-scheduled
+    forms (triangle_solve.hpp:32-145) -- each planned and solved on the GPU:
+    bit for bit the compiled reference's results (the oracle's where the
+    reference library is absent)."""
+    P = orc.ptr
+    rf = orc.ref()
+    port = orc.port()
+    checked = 0
+    for name, m, n, ai, aj, av in golden_matrices(golden):
+        if m != n:
+            continue
+        l_ai, l_aj, l_av = strict_triangle(n, ai, aj, av, True)
+        u_ai, u_aj, u_av = strict_triangle(n, ai, aj, av, False)
+        rng = np.random.default_rng(n + 3)
+        b = rng.uniform(-1, 1, n)
+        d = rng.uniform(1, 2, n)
+        want = np.zeros(n)
+        (rf.la_ref_forward_substitution if rf else port.oracle_forward_substitution)(
+            n, 0, P(l_ai), P(l_aj), P(l_av), P(b), P(want))
+        got = lab.ForwardSubstitution(n, 0, l_ai, l_aj, l_av, b, np.zeros(n))
+        assert np.array_equal(got, want, equal_nan=True), (name, "forward")
+        want = np.zeros(n)
+        (rf.la_ref_backward_substitution if rf else port.oracle_backward_substitution)(
+            n, 0, P(u_ai), P(u_aj), P(u_av), P(d), P(b), P(want))
+        got = lab.BackwardSubstitution(n, 0, u_ai, u_aj, u_av, d, b, np.zeros(n))
+        assert np.array_equal(got, want, equal_nan=True), (name, "backward")
+        if rf:
+            lv, ip, pf = lab.TopologicalSort2("L", n, 0, l_ai, l_aj)
+            want = np.zeros(n)
+            rf.la_ref_level_forward(4, P(ip), P(pf), lv, n, 0, P(l_ai), P(l_aj), P(l_av),
+                                    P(b), P(want))
+            got = lab.LevelScheduleForwardSubstitution(ip, pf, lv, n, 0, l_ai, l_aj, l_av, b,
+                                                       np.zeros(n))
+            assert np.array_equal(got, want, equal_nan=True), (name, "level forward")
+            lv, ip, pf = lab.TopologicalSort2("U", n, 0, u_ai, u_aj)
+            want = np.zeros(n)
+            rf.la_ref_level_backward(4, P(ip), P(pf), lv, n, 0, P(u_ai), P(u_aj), P(u_av),
+                                     P(d), P(b), P(want))
+            got = lab.LevelScheduleBackwardSubstitution(ip, pf, lv, n, 0, u_ai, u_aj, u_av,
+                                                        d, b, np.zeros(n))
+            assert np.array_equal(got, want, equal_nan=True), (name, "level backward")
+        checked += 1
+    assert checked >= 5
+
+
 def test_forward_substitution_t(lab, orc, golden):
     """ForwardSubstitutionT (triangle_solve.hpp:87-98): the unit lower solve
     with L = U^T given as the CSR of the strict upper triangle U.  The GPU
