@@ -154,3 +154,65 @@ def test_oracle_pcg_matches_reference_composed_pcg(orc, golden):
         assert it1 > 0 and abs(it1 - it2) <= 1, (name, it1, it2)
         assert r1[0] < 1e-10 and r2[0] < 1e-10
         assert np.linalg.norm(x1 - x2) <= 1e-9 * np.linalg.norm(x1)
+
+
+def _random_triangle(n, seed, lower, base):
+    """Strict triangle with 0-6 entries per row, columns sorted, values in
+    [-0.4, 0.4] (so unit solves stay bounded), indices carrying `base`."""
+    r = np.random.default_rng(seed)
+    rows = []
+    for i in range(n):
+        pool = i if lower else n - 1 - i
+        k = min(int(r.integers(0, 7)), pool)
+        c = r.choice(pool, k, replace=False) if k else np.zeros(0, np.int64)
+        rows.append(np.sort(c if lower else c + i + 1))
+    ai = np.concatenate([[0], np.cumsum([len(c) for c in rows])]).astype(np.int32) + base
+    aj = (np.concatenate(rows) if ai[-1] > base else np.zeros(0)).astype(np.int32) + base
+    return ai, aj, r.uniform(-0.4, 0.4, int(ai[-1] - base))
+
+
+def test_oracle_triangular_solves_match_live_reference(orc):
+    """The oracle's restatements of the reference's triangular solves --
+    ForwardSubstitution, BackwardSubstitution, ForwardSubstitutionT and the
+    level-scheduled forms (triangle_solve.hpp:32-145) -- against the compiled
+    reference on seeded random triangles, base 0 and 1, several thread
+    counts for the level forms: bit for bit."""
+    rf = orc.ref()
+    if rf is None:
+        pytest.skip("oracle/_ref not built (reference tree absent)")
+    P = orc.ptr
+    po = orc.port()
+    for seed, n in ((0, 1), (1, 37), (2, 2000), (3, 9000)):
+        for base in (0, 1):
+            b = np.random.default_rng(seed + 100).uniform(-1, 1, n)
+            d = np.random.default_rng(seed + 200).uniform(1, 2, n)
+            l_ai, l_aj, l_av = _random_triangle(n, seed, True, base)
+            u_ai, u_aj, u_av = _random_triangle(n, seed + 50, False, base)
+            x1, x2 = np.zeros(n), np.zeros(n)
+            rf.la_ref_forward_substitution(n, base, P(l_ai), P(l_aj), P(l_av), P(b), P(x1))
+            po.oracle_forward_substitution(n, base, P(l_ai), P(l_aj), P(l_av), P(b), P(x2))
+            assert np.array_equal(x1, x2), (seed, base, "forward")
+            rf.la_ref_backward_substitution(n, base, P(u_ai), P(u_aj), P(u_av), P(d), P(b),
+                                            P(x1))
+            po.oracle_backward_substitution(n, base, P(u_ai), P(u_aj), P(u_av), P(d), P(b),
+                                            P(x2))
+            assert np.array_equal(x1, x2), (seed, base, "backward")
+            rf.la_ref_forward_substitution_t(n, base, P(u_ai), P(u_aj), P(u_av), P(b), P(x1))
+            po.oracle_forward_substitution_t(n, base, P(u_ai), P(u_aj), P(u_av), P(b), P(x2))
+            assert np.array_equal(x1, x2), (seed, base, "forward T")
+            for uplo, (t_ai, t_aj, t_av), diag in ((0, (l_ai, l_aj, l_av), None),
+                                                   (1, (u_ai, u_aj, u_av), d)):
+                ip = np.empty(n, np.int32)
+                pf = np.empty(n + 1, np.int32)
+                lv = po.oracle_topological_sort2(uplo, n, base, P(t_ai), P(t_aj), P(ip), P(pf))
+                po.oracle_level_solve(lv, P(ip), P(pf), base, P(t_ai), P(t_aj), P(t_av),
+                                      P(diag), P(b), P(x2))
+                for T in (1, 3, 8):
+                    x1 = np.zeros(n)
+                    if uplo == 0:
+                        rf.la_ref_level_forward(T, P(ip), P(pf), lv, n, base, P(t_ai), P(t_aj),
+                                                P(t_av), P(b), P(x1))
+                    else:
+                        rf.la_ref_level_backward(T, P(ip), P(pf), lv, n, base, P(t_ai), P(t_aj),
+                                                 P(t_av), P(diag), P(b), P(x1))
+                    assert np.array_equal(x1, x2), (seed, base, uplo, T, "level")
