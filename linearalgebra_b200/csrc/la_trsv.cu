@@ -282,8 +282,9 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // ---------------------------------------------------------------- parts
-// Partitioned schedule.  The rows are split into compact parts (recursive
-// BFS bisection of the triangle's graph), one CTA per part, all CTAs
+// Partitioned schedule.  The rows are split into compact parts (value cuts
+// on coordinates monotone along the dependencies, la_partition.cpp, so the
+// parts' dependency graph is acyclic), one CTA per part, all CTAs
 // co-resident (cooperative launch).  A CTA walks the levels present in its
 // part in increasing order, one __syncthreads per level, and keeps the x
 // values of its own rows in shared memory: a dependency inside the part costs
