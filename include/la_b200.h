@@ -255,6 +255,16 @@ la_status la_trsv_analysis_transposed(la_uplo uplo, int n, int base, const int *
                                       const int *aj, const double *av,
                                       const double *diag, la_dtype dtype,
                                       la_trsv_plan_t *out);
+/* The row partition the partitioned schedule cuts for this strict triangle
+ * (no reference counterpart; host only, needs no GPU): part[n] in
+ * [0, nparts), from value cuts on coordinates monotone along the
+ * dependencies, so that a row never reads a row of a higher-numbered part
+ * (part[j] <= part[i] whenever row i reads row j); *coords (may be NULL)
+ * receives the number of cut coordinates found (3 for a 7-point grid, 1 --
+ * the level alone -- when no other is monotone).  The analysis uses this
+ * partition with nparts = one per SM when its cost model prefers it. */
+la_status la_trsv_partition(la_uplo uplo, int n, int base, const int *ai, const int *aj,
+                            int nparts, int *part, int *coords);
 /* x = T^-1 b (triangle_solve.tpp:115-155 operator()/BarrierOp): b, x device
  * arrays of the plan's dtype; b and x must not alias.  LA_ERR_TIMEOUT if a
  * dependency wait exceeded its bound (x is then undefined). */

@@ -40,7 +40,7 @@ __all__ = [
     "ValidCSR", "ICCLevelNumeric0", "ICCShifted", "SerialCM", "PCG", "LAError",
     "spmv_transpose", "sddmm_pattern", "ForwardSubstitutionT", "ForwardSubstitution",
     "BackwardSubstitution", "LevelScheduleForwardSubstitution",
-    "LevelScheduleBackwardSubstitution",
+    "LevelScheduleBackwardSubstitution", "trsv_partition",
 ]
 
 
@@ -294,6 +294,17 @@ class OptimizedTriangularSolve:
 
 
 # --------------------------------------------------------- host analysis
+def trsv_partition(uplo, n, base, ai, aj, nparts):
+    """(part[n], coordinates used): the row partition the partitioned solve
+    schedule cuts for this strict triangle (host only)."""
+    ai, aj = _i32(ai), _i32(aj)
+    part = np.empty(max(n, 1), np.int32)
+    c = C.c_int()
+    call("la_trsv_partition", LA_LOWER if uplo in ("L", 0, LA_LOWER) else LA_UPPER, int(n),
+         int(base), _ptr(ai), _ptr(aj), int(nparts), _ptr(part), C.byref(c))
+    return part[:n], c.value
+
+
 def ForwardSubstitution(size, base, ai, aj, av, b, x):
     """``ForwardSubstitution`` (triangle_solve.hpp:32-43): unit lower solve with
     the strict lower CSR, host arrays, x written in place (one GPU plan and

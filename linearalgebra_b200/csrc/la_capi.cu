@@ -453,14 +453,9 @@ la_status la_icc0_shifted(int n, int base, const int *u_ai, const int *u_aj,
 }
 
 // ------------------------------------------------------------------ trsv
-static la_status trsv_analysis_impl(la_uplo uplo, int n, int base, const int *ai,
-                                    const int *aj, const double *av,
-                                    const double *diag, la_dtype dtype,
-                                    const int *iperm, const int *prefix,
-                                    int nlevels, la_trsv_plan_t *out) {
-  LA_CHECK_ARG(out && ai && n >= 0, "arguments");
-  LA_CHECK_ARG(uplo == LA_LOWER || uplo == LA_UPPER, "uplo");
-  LA_CHECK_ARG(dtype == LA_F64 || dtype == LA_F32, "dtype");
+// A valid CSR whose entries all lie in the strict `uplo` triangle.
+static la_status check_strict_triangle(la_uplo uplo, int n, int base, const int *ai,
+                                       const int *aj) {
   std::string why;
   if (!valid_csr(n, n, base, ai, aj, &why)) {
     set_error("invalid CSR: %s", why.c_str());
@@ -475,6 +470,18 @@ static la_status trsv_analysis_impl(la_uplo uplo, int n, int base, const int *ai
         return LA_ERR_INVALID_ARG;
       }
     }
+  return LA_OK;
+}
+
+static la_status trsv_analysis_impl(la_uplo uplo, int n, int base, const int *ai,
+                                    const int *aj, const double *av,
+                                    const double *diag, la_dtype dtype,
+                                    const int *iperm, const int *prefix,
+                                    int nlevels, la_trsv_plan_t *out) {
+  LA_CHECK_ARG(out && ai && n >= 0, "arguments");
+  LA_CHECK_ARG(uplo == LA_LOWER || uplo == LA_UPPER, "uplo");
+  LA_CHECK_ARG(dtype == LA_F64 || dtype == LA_F32, "dtype");
+  LA_TRY(check_strict_triangle(uplo, n, base, ai, aj));
   if (iperm) {
     LA_CHECK_ARG(prefix && nlevels >= 0 && prefix[0] == 0 && prefix[nlevels] == n,
                  "level prefix must start at 0 and end at n");
@@ -535,6 +542,28 @@ la_status la_trsv_analysis_transposed(la_uplo uplo, int n, int base, const int *
   transpose(n, n, base, ai, aj, av, tai.data(), taj.data(), tav.data());
   return trsv_analysis_impl(uplo == LA_LOWER ? LA_UPPER : LA_LOWER, n, base, tai.data(),
                             taj.data(), tav.data(), diag, dtype, nullptr, nullptr, 0, out);
+}
+
+la_status la_trsv_partition(la_uplo uplo, int n, int base, const int *ai, const int *aj,
+                           int nparts, int *part, int *coords) {
+  LA_CHECK_ARG(ai && part && n >= 0 && nparts >= 1, "arguments");
+  LA_CHECK_ARG(uplo == LA_LOWER || uplo == LA_UPPER, "uplo");
+  LA_TRY(check_strict_triangle(uplo, n, base, ai, aj));
+  int used = 0;
+  if (n > 0) {
+    std::vector<int> iperm(n), prefix(n + 1), lvl(n);
+    const int levels = topological_sort2(uplo, n, base, ai, aj, iperm.data(), prefix.data());
+    for (int l = 0; l < levels; l++)
+      for (int p = prefix[l]; p < prefix[l + 1]; p++)
+        lvl[iperm[p] - base] = l;
+    std::vector<int> xadj, adj;
+    undirected_pattern(n, base, ai, aj, xadj, adj);
+    used = monotone_partition(n, xadj.data(), adj.data(), ai, aj, base, lvl.data(), nparts,
+                              part);
+  }
+  if (coords)
+    *coords = used;
+  return LA_OK;
 }
 
 la_status la_trsv(la_trsv_plan_t plan, const void *b, void *x,

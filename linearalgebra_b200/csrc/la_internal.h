@@ -89,6 +89,10 @@ void rcm(int n, int base, const int *ai, const int *aj, int *iperm, int *perm);
 // graph; lvl: the rows' levels.  Returns the number of coordinates used.
 int monotone_partition(int n, const int *xadj, const int *adj, const int *dep_ptr,
                        const int *dep_col, int base, const int *lvl, int nparts, int *part);
+// The triangle's pattern made undirected and 0-based (both directions of
+// every stored entry), the graph monotone_partition walks.
+void undirected_pattern(int n, int base, const int *ai, const int *aj, std::vector<int> &xadj,
+                        std::vector<int> &adj);
 
 } // namespace la
 

@@ -58,6 +58,25 @@ void bfs_dist(int n, const int *xadj, const int *adj, int src, std::vector<int> 
 
 } // namespace
 
+void undirected_pattern(int n, int base, const int *ai, const int *aj, std::vector<int> &xadj,
+                        std::vector<int> &adj) {
+  xadj.assign(n + 1, 0);
+  adj.resize(2 * (size_t)(ai[n] - base));
+  for (int i = 0; i < n; i++)
+    for (int k = ai[i] - base; k < ai[i + 1] - base; k++) {
+      xadj[i + 1]++;
+      xadj[aj[k] - base + 1]++;
+    }
+  std::partial_sum(xadj.begin(), xadj.end(), xadj.begin());
+  std::vector<int> fill(xadj.begin(), xadj.end() - 1);
+  for (int i = 0; i < n; i++)
+    for (int k = ai[i] - base; k < ai[i + 1] - base; k++) {
+      const int j = aj[k] - base;
+      adj[fill[i]++] = j;
+      adj[fill[j]++] = i;
+    }
+}
+
 int monotone_partition(int n, const int *xadj, const int *adj, const int *dep_ptr,
                        const int *dep_col, int base, const int *lvl, int nparts, int *part) {
   if (n == 0)

@@ -772,22 +772,8 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
   for (int l = 0; l < P->levels; l++)
     for (int p = P->h_prefix[l]; p < P->h_prefix[l + 1]; p++)
       lvl[P->h_iperm[p] - base] = l;
-  std::vector<int> xadj(n + 1, 0), adj(2 * (size_t)nnz);
-  for (int i = 0; i < n; i++)
-    for (int k = ai[i] - base; k < ai[i + 1] - base; k++) {
-      xadj[i + 1]++;
-      xadj[aj[k] - base + 1]++;
-    }
-  std::partial_sum(xadj.begin(), xadj.end(), xadj.begin());
-  {
-    std::vector<int> fill(xadj.begin(), xadj.end() - 1);
-    for (int i = 0; i < n; i++)
-      for (int k = ai[i] - base; k < ai[i + 1] - base; k++) {
-        const int j = aj[k] - base;
-        adj[fill[i]++] = j;
-        adj[fill[j]++] = i;
-      }
-  }
+  std::vector<int> xadj, adj;
+  undirected_pattern(n, base, ai, aj, xadj, adj);
   std::vector<int> part;
   cached_partition(n, xadj, adj, ai, aj, base, lvl, nparts, part);
   std::vector<int> pstart(nparts + 1, 0);

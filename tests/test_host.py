@@ -155,3 +155,60 @@ def test_valid_csr_rejects_bad_input(lab):
     assert not lab.ValidCSR(2, 2, 0, ai, np.array([0, 1, 2], np.int32))   # out of range
     assert not lab.ValidCSR(2, 2, 1, ai, np.array([0, 1, 1], np.int32))   # ai[0] != base
     assert not lab.ValidCSR(2, 2, 0, np.array([0, 2, 1], np.int32), np.array([0, 1], np.int32))
+
+
+def _strict(n, ai, aj, lower):
+    rows = np.repeat(np.arange(n), np.diff(ai))
+    keep = (aj < rows) if lower else (aj > rows)
+    t_ai = np.zeros(n + 1, np.int32)
+    np.cumsum(np.bincount(rows[keep], minlength=n), out=t_ai[1:])
+    return t_ai, aj[keep].astype(np.int32)
+
+
+def test_trsv_partition_never_reads_a_later_part(lab):
+    """The partitioned solve's row partition (la_trsv_partition, host only):
+    every part index in range, and no row reads a row of a higher-numbered
+    part -- the property that makes the parts' dependency graph acyclic --
+    for grids in natural and RCM order, both triangles, a 27-point stencil,
+    random triangles with base 1, and 1, 3 or 148 parts.  A 7-point grid
+    yields three cut coordinates and balanced parts; the 27-point stencil
+    only the level (its documented limitation)."""
+    from linearalgebra_b200 import gen
+    cases = []
+    n, ai, aj, av = gen.laplacian_3d(20)
+    cases.append(("lap3d_20", n, ai, aj, 0, 3))
+    iperm, perm = lab.SerialCM(n, 0, ai, aj)
+    b_ai, b_aj, _ = lab.Permute(n, 0, ai, aj, av, iperm, perm)
+    cases.append(("lap3d_20_rcm", n, b_ai, b_aj, 0, 3))
+    n2, ai2, aj2, _ = gen.stencil27(10)
+    cases.append(("st27_10", n2, ai2, aj2, 0, 1))
+    n3, ai3, aj3, _ = gen.aniso7(14, seed=1)
+    cases.append(("aniso7_14", n3, ai3, aj3, 0, None))
+    rng = np.random.default_rng(7)
+    m = 3000
+    rows = [np.sort(rng.choice(m, min(m, 5), replace=False)) for _ in range(m)]
+    r_ai = np.concatenate([[0], np.cumsum([len(c) for c in rows])]).astype(np.int32)
+    r_aj = np.concatenate(rows).astype(np.int32)
+    cases.append(("random_base1", m, r_ai + 1, r_aj + 1, 1, None))
+    for name, n, ai, aj, base, want_coords in cases:
+        a0, j0 = (ai - base, aj - base)
+        for lower in (True, False):
+            t_ai, t_aj = _strict(n, a0, j0, lower)
+            for nparts in (1, 3, 148):
+                part, coords = lab.trsv_partition("L" if lower else "U", n, base,
+                                                  t_ai + base, t_aj + base, nparts)
+                assert part.shape == (n,) and part.min() >= 0 and part.max() < nparts, name
+                r = np.repeat(np.arange(n), np.diff(t_ai))
+                assert not np.any(part[t_aj] > part[r]), (name, lower, nparts)
+                if nparts == 148 and want_coords is not None:
+                    assert coords == want_coords, (name, lower, coords)
+                if nparts == 148 and want_coords == 3:
+                    sizes = np.bincount(part, minlength=nparts)
+                    assert sizes.min() > 0 and sizes.max() <= 2 * n / nparts, (name, sizes.max())
+    # edge cases and argument checks
+    assert lab.trsv_partition("L", 0, 0, np.zeros(1, np.int32), np.zeros(0, np.int32), 4)[0].size == 0
+    part, _ = lab.trsv_partition("L", 1, 0, np.zeros(2, np.int32), np.zeros(0, np.int32), 4)
+    assert part.tolist() == [0]
+    with pytest.raises(lab.LAError) as e:
+        lab.trsv_partition("L", 2, 0, np.array([0, 0, 1], np.int32), np.array([1], np.int32), 2)
+    assert e.value.name == "LA_ERR_INVALID_ARG"
