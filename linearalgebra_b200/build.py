@@ -22,7 +22,7 @@ BUILD = PKG / "_build"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr",
-    "-Xcompiler", "-fPIC,-O3", "-Xptxas", "-O3",
+    "-Xcompiler", "-fPIC,-O3,-fopenmp", "-Xptxas", "-O3",
 ] + ARCH
 
 
@@ -70,7 +70,8 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> Path:
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 2)) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose_ptxas), srcs))
     tmp = OUT.with_suffix(".so.tmp")
-    cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs)]
+    # host threads (OpenMP) for the analysis' graph searches and row sorts
+    cmd = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fopenmp", "-o", str(tmp), *map(str, objs)]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")

@@ -107,23 +107,30 @@ void permute(int n, int base, const int *ai, const int *aj, const double *av,
     const int src = iperm ? iperm[i] - base : i;
     p_ai[i + 1] = p_ai[i] + (ai[src + 1] - ai[src]);
   }
-  std::vector<std::pair<int, double>> row;
-  for (int i = 0; i < n; i++) {
-    const int src = iperm ? iperm[i] - base : i;
-    const int o = p_ai[i] - base, s = ai[src] - base, len = ai[src + 1] - ai[src];
-    if (!perm) {
-      std::memcpy(p_aj + o, aj + s, sizeof(int) * len);
-      std::memcpy(p_av + o, av + s, sizeof(double) * len);
-      continue;
-    }
-    row.resize(len);
-    for (int q = 0; q < len; q++)
-      row[q] = {perm[aj[s + q] - base], av[s + q]};
-    std::sort(row.begin(), row.end(),
-              [](const auto &a, const auto &b) { return a.first < b.first; });
-    for (int q = 0; q < len; q++) {
-      p_aj[o + q] = row[q].first;
-      p_av[o + q] = row[q].second;
+  // rows are independent once their starts are known: the host's threads
+  // fill them (each row sorted on its own, so the result does not depend
+  // on the threads)
+#pragma omp parallel
+  {
+    std::vector<std::pair<int, double>> row;
+#pragma omp for schedule(dynamic, 4096)
+    for (int i = 0; i < n; i++) {
+      const int src = iperm ? iperm[i] - base : i;
+      const int o = p_ai[i] - base, s = ai[src] - base, len = ai[src + 1] - ai[src];
+      if (!perm) {
+        std::memcpy(p_aj + o, aj + s, sizeof(int) * len);
+        std::memcpy(p_av + o, av + s, sizeof(double) * len);
+        continue;
+      }
+      row.resize(len);
+      for (int q = 0; q < len; q++)
+        row[q] = {perm[aj[s + q] - base], av[s + q]};
+      std::sort(row.begin(), row.end(),
+                [](const auto &a, const auto &b) { return a.first < b.first; });
+      for (int q = 0; q < len; q++) {
+        p_aj[o + q] = row[q].first;
+        p_av[o + q] = row[q].second;
+      }
     }
   }
 }

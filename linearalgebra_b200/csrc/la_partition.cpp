@@ -37,23 +37,48 @@
 namespace la {
 namespace {
 
-// breadth-first distances from src; -1 where unreachable
-void bfs_dist(int n, const int *xadj, const int *adj, int src, std::vector<int> &d,
-              std::vector<int> &queue) {
+// Breadth-first distances from src (-1 where unreachable); returns the
+// number of vertices reached.  Level-synchronous: the host's threads split
+// each frontier and claim a vertex by a compare-and-swap on its distance, so
+// the distances are those of the sequential search whatever the threads'
+// order (only the order of a frontier varies, and nothing reads it).
+int bfs_dist(int n, const int *xadj, const int *adj, int src, std::vector<int> &d) {
   d.assign(n, -1);
-  queue.clear();
   d[src] = 0;
-  queue.push_back(src);
-  for (size_t h = 0; h < queue.size(); h++) {
-    const int u = queue[h];
-    for (int k = xadj[u]; k < xadj[u + 1]; k++) {
-      const int v = adj[k];
-      if (d[v] < 0) {
-        d[v] = d[u] + 1;
-        queue.push_back(v);
+  std::vector<int> frontier{src}, next;
+  int reached = 1;
+  for (int level = 1; !frontier.empty(); level++) {
+    next.clear();
+    const int fs = (int)frontier.size();
+    if (fs < 4096) { // small frontier: no threads
+      for (int f = 0; f < fs; f++)
+        for (int k = xadj[frontier[f]]; k < xadj[frontier[f] + 1]; k++)
+          if (d[adj[k]] < 0) {
+            d[adj[k]] = level;
+            next.push_back(adj[k]);
+          }
+    } else {
+#pragma omp parallel
+      {
+        std::vector<int> mine;
+#pragma omp for schedule(static) nowait
+        for (int f = 0; f < fs; f++)
+          for (int k = xadj[frontier[f]]; k < xadj[frontier[f] + 1]; k++) {
+            int *dv = &d[adj[k]];
+            int expect = -1;
+            if (__atomic_load_n(dv, __ATOMIC_RELAXED) < 0 &&
+                __atomic_compare_exchange_n(dv, &expect, level, false, __ATOMIC_RELAXED,
+                                            __ATOMIC_RELAXED))
+              mine.push_back(adj[k]);
+          }
+#pragma omp critical
+        next.insert(next.end(), mine.begin(), mine.end());
       }
     }
+    reached += (int)next.size();
+    frontier.swap(next);
   }
+  return reached;
 }
 
 } // namespace
@@ -91,7 +116,6 @@ int monotone_partition(int n, const int *xadj, const int *adj, const int *dep_pt
   std::vector<Cand> cands;
   std::vector<std::vector<int>> dist;
   {
-    std::vector<int> queue;
     int dmin = INT_MAX;
     for (int v = 0; v < n; v++)
       dmin = std::min(dmin, xadj[v + 1] - xadj[v]);
@@ -100,8 +124,7 @@ int monotone_partition(int n, const int *xadj, const int *adj, const int *dep_pt
       if (xadj[v + 1] - xadj[v] == dmin)
         low.push_back(v);
     std::vector<int> d, mind;
-    bfs_dist(n, xadj, adj, low[0], d, queue);
-    bool connected = (int)queue.size() == n;
+    bool connected = bfs_dist(n, xadj, adj, low[0], d) == n;
     if (connected) {
       dist.push_back(d);
       mind = d;
@@ -112,34 +135,48 @@ int monotone_partition(int n, const int *xadj, const int *adj, const int *dep_pt
             best = v;
         if (best < 0 || mind[best] == 0)
           break;
-        bfs_dist(n, xadj, adj, best, d, queue);
+        bfs_dist(n, xadj, adj, best, d);
         dist.push_back(d);
         for (int v = 0; v < n; v++)
           mind[v] = std::min(mind[v], d[v]);
       }
     }
+    // landmark pairs, checked on the host's threads (integer work: the same
+    // candidates, kept in pair order, whatever the threads)
     const int L = (int)dist.size();
+    std::vector<std::pair<int, int>> pairs;
     for (int a = 0; a < L; a++)
-      for (int b = a + 1; b < L; b++) {
-        const std::vector<int> &da = dist[a], &db = dist[b];
-        long long pos = 0, neg = 0;
-        for (int i = 0; i < n && !(pos && neg); i++)
-          for (int k = dep_ptr[i] - base; k < dep_ptr[i + 1] - base; k++) {
-            const int j = dep_col[k] - base;
-            const int df = (da[i] - db[i]) - (da[j] - db[j]);
-            pos += df > 0;
-            neg += df < 0;
-          }
-        if ((pos == 0) == (neg == 0))
-          continue; // not monotone, or constant along every edge
-        int lo = INT_MAX, hi = INT_MIN;
-        for (int v = 0; v < n; v++) {
-          const int f = da[v] - db[v];
-          lo = std::min(lo, f);
-          hi = std::max(hi, f);
+      for (int b = a + 1; b < L; b++)
+        pairs.push_back({a, b});
+    const int np = (int)pairs.size();
+    std::vector<Cand> found(np);
+    std::vector<char> keep(np, 0);
+#pragma omp parallel for schedule(dynamic)
+    for (int q = 0; q < np; q++) {
+      const int a = pairs[q].first, b = pairs[q].second;
+      const std::vector<int> &da = dist[a], &db = dist[b];
+      long long pos = 0, neg = 0;
+      for (int i = 0; i < n && !(pos && neg); i++)
+        for (int k = dep_ptr[i] - base; k < dep_ptr[i + 1] - base; k++) {
+          const int j = dep_col[k] - base;
+          const int df = (da[i] - db[i]) - (da[j] - db[j]);
+          pos += df > 0;
+          neg += df < 0;
         }
-        cands.push_back({a, b, pos > 0 ? 1 : -1, (long long)hi - lo});
+      if ((pos == 0) == (neg == 0))
+        continue; // not monotone, or constant along every edge
+      int lo = INT_MAX, hi = INT_MIN;
+      for (int v = 0; v < n; v++) {
+        const int f = da[v] - db[v];
+        lo = std::min(lo, f);
+        hi = std::max(hi, f);
       }
+      found[q] = {a, b, pos > 0 ? 1 : -1, (long long)hi - lo};
+      keep[q] = 1;
+    }
+    for (int q = 0; q < np; q++)
+      if (keep[q])
+        cands.push_back(found[q]);
     int lo = INT_MAX, hi = INT_MIN;
     for (int v = 0; v < n; v++) {
       lo = std::min(lo, lvl[v]);
