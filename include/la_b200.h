@@ -165,6 +165,16 @@ la_status la_sddmm_pattern(la_spmv_plan_t plan, double alpha, const double *g,
                            const double *x, double *dv, la_stream_t stream);
 
 /* ------------------------------------------------------- host analysis */
+/* TopologicalSort<L|U> (matrix_utils.hpp:583-635, Kahn's breadth-first
+ * order), bit-identical output: the same level sets as TopologicalSort2,
+ * rows of a level in breadth-first order (level 0 ascending for L,
+ * descending for U; then the readers of each row as its level is walked).
+ * *result is the reference's return value -- the index of the last level
+ * (levels - 1; 0 for n == 0) -- and prefix receives *result + 2 zero-based
+ * entries (caller provides n + 2 ints); iperm values carry the base.
+ * LA_ERR_INVALID_ARG if the entries form a cycle (the reference loops). */
+la_status la_topological_sort(la_uplo uplo, int n, int base, const int *ai, const int *aj,
+                              int *iperm, int *prefix, int *result);
 /* TopologicalSort2<L|U> (matrix_utils.hpp:637-675), bit-identical output:
  * iperm[n] (values i + base, ordered by level then row) and zero-based
  * prefix[levels + 1] (caller provides n + 1 ints).  Returns the level

@@ -250,6 +250,23 @@ void ForwardSubstitutionT(const COLTYPE size, const int base, ROWTYPE const *ai,
   check(s, "la_trsv_host");
 }
 
+// TopologicalSort<TS> (matrix_utils.hpp:583-635, Kahn's breadth-first
+// order), bit-identical output, including the return value (the last level's
+// index) and prefix's length (that + 2).
+template <TriangularMatrix TS = L, typename ROWTYPE, typename COLTYPE,
+          typename VEC>
+COLTYPE TopologicalSort(const COLTYPE nodes, const int base, ROWTYPE const *ai,
+                        COLTYPE const *aj, VEC &iperm, VEC &prefix) {
+  iperm.resize(nodes);
+  prefix.resize(nodes + 2);
+  int result = 0;
+  check(la_topological_sort(TS == L ? LA_LOWER : LA_UPPER, nodes, base, ai, aj,
+                            iperm.data(), prefix.data(), &result),
+        "la_topological_sort");
+  prefix.resize(result + 2);
+  return result;
+}
+
 // TopologicalSort2<TS> (matrix_utils.hpp:637-675), bit-identical output.
 template <TriangularMatrix TS = L, typename ROWTYPE, typename COLTYPE,
           typename VEC>

@@ -76,6 +76,7 @@ _SIGS = {
     "la_trsv_analysis_levels": [I, I, I, P, P, P, P, I, P, P, I, C.POINTER(P)],
     "la_trsv_analysis_transposed": [I, I, I, P, P, P, P, I, C.POINTER(P)],
     "la_trsv_partition": [I, I, I, P, P, I, P, P],
+    "la_topological_sort": [I, I, I, P, P, P, P, P],
     "la_trsv": [P, P, P, P],
     "la_trsv_launch": [P, P, P, P],
     "la_trsv_status": [P, P],

@@ -40,7 +40,7 @@ __all__ = [
     "ValidCSR", "ICCLevelNumeric0", "ICCShifted", "SerialCM", "PCG", "LAError",
     "spmv_transpose", "sddmm_pattern", "ForwardSubstitutionT", "ForwardSubstitution",
     "BackwardSubstitution", "LevelScheduleForwardSubstitution",
-    "LevelScheduleBackwardSubstitution", "trsv_partition",
+    "LevelScheduleBackwardSubstitution", "trsv_partition", "TopologicalSort",
 ]
 
 
@@ -342,6 +342,18 @@ def ForwardSubstitutionT(size, base, ai, aj, av, b, x):
     ts = OptimizedTriangularSolve("L").analysis_transposed(size, base, ai, aj, av)
     ts(np.ascontiguousarray(b, np.float64), x)
     return x
+
+
+def TopologicalSort(uplo, nodes, base, ai, aj):
+    """``TopologicalSort`` (matrix_utils.hpp:583-635, Kahn's order): returns
+    (the reference's return value = last level index, iperm, prefix)."""
+    ai, aj = _i32(ai), _i32(aj)
+    iperm = np.empty(max(nodes, 1), np.int32)
+    prefix = np.empty(nodes + 2, np.int32)
+    r = C.c_int()
+    call("la_topological_sort", LA_LOWER if uplo in ("L", 0) else LA_UPPER, int(nodes),
+         int(base), _ptr(ai), _ptr(aj), _ptr(iperm), _ptr(prefix), C.byref(r))
+    return r.value, iperm[:nodes], prefix[: r.value + 2].copy()
 
 
 def TopologicalSort2(uplo, nodes, base, ai, aj):

@@ -357,6 +357,24 @@ la_status la_topological_sort2(la_uplo uplo, int n, int base, const int *ai,
   return LA_OK;
 }
 
+la_status la_topological_sort(la_uplo uplo, int n, int base, const int *ai, const int *aj,
+                              int *iperm, int *prefix, int *result) {
+  LA_CHECK_ARG(ai && iperm && prefix && result && n >= 0, "arguments");
+  LA_CHECK_ARG(uplo == LA_LOWER || uplo == LA_UPPER, "uplo");
+  std::string why;
+  if (!valid_csr(n, n, base, ai, aj, &why)) {
+    set_error("invalid CSR: %s", why.c_str());
+    return LA_ERR_BAD_CSR;
+  }
+  const int r = topological_sort_kahn(uplo, n, base, ai, aj, iperm, prefix);
+  if (r < 0) {
+    set_error("la_topological_sort: the dependencies form a cycle");
+    return LA_ERR_INVALID_ARG;
+  }
+  *result = r;
+  return LA_OK;
+}
+
 la_status la_rcm(int n, int base, const int *ai, const int *aj, int *iperm,
                  int *perm) {
   LA_CHECK_ARG(ai && iperm && perm && n >= 0, "arguments");

@@ -47,6 +47,61 @@ bool valid_csr(int rows, int cols, int base, const int *ai, const int *aj,
   return true;
 }
 
+// matrix_utils.hpp:583-635 TopologicalSort (Kahn's breadth-first order):
+// the same level sets as TopologicalSort2, another order inside a level.
+// Level 0 holds the rows without entries, ascending (L) or descending (U);
+// each later level lists, for the rows of the level before in their order,
+// the rows that read them (ascending, the order of a stable transpose) as
+// the last of their entries is consumed.  Returns the reference's value: the
+// index of the last level (levels - 1, 0 for n == 0); prefix gets that + 2
+// entries.  -1 when a level adds no row before all are placed (a cycle: not
+// a triangle), where the reference would not stop.
+int topological_sort_kahn(int uplo, int n, int base, const int *ai, const int *aj, int *iperm,
+                          int *prefix) {
+  std::vector<int> pending(n);
+  int placed = 0, np = 2;
+  prefix[0] = 0;
+  prefix[1] = 0;
+  for (int t = 0; t < n; t++) {
+    const int i = uplo == 0 ? t : n - 1 - t;
+    pending[i] = ai[i + 1] - ai[i];
+    if (pending[i] == 0) {
+      iperm[placed++] = i + base;
+      prefix[1]++;
+    }
+  }
+  // readers of each row, ascending
+  const int nnz = ai[n] - base;
+  std::vector<int> r_ptr(n + 1, 0), r_row(std::max(nnz, 1));
+  for (int k = 0; k < nnz; k++)
+    r_ptr[aj[k] - base + 1]++;
+  for (int i = 0; i < n; i++)
+    r_ptr[i + 1] += r_ptr[i];
+  {
+    std::vector<int> fill(r_ptr.begin(), r_ptr.end() - 1);
+    for (int i = 0; i < n; i++)
+      for (int k = ai[i] - base; k < ai[i + 1] - base; k++)
+        r_row[fill[aj[k] - base]++] = i;
+  }
+  int level = 0;
+  while (placed != n) {
+    prefix[np] = prefix[np - 1];
+    np++;
+    for (int p = prefix[level]; p < prefix[level + 1]; p++) {
+      const int row = iperm[p] - base;
+      for (int k = r_ptr[row]; k < r_ptr[row + 1]; k++)
+        if (--pending[r_row[k]] == 0) {
+          iperm[placed++] = r_row[k] + base;
+          prefix[np - 1]++;
+        }
+    }
+    if (prefix[np - 1] == prefix[np - 2])
+      return -1;
+    level++;
+  }
+  return level;
+}
+
 // matrix_utils.hpp:637-675 TopologicalSort2.  depth(i) = max over stored
 // entries j of depth(j) + 1, rows visited ascending (L) or descending (U);
 // iperm lists rows by (level, ascending row) with values i + base; prefix is

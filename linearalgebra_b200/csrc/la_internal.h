@@ -69,6 +69,8 @@ bool valid_csr(int rows, int cols, int base, const int *ai, const int *aj,
                std::string *why);
 int topological_sort2(int uplo, int n, int base, const int *ai, const int *aj,
                       int *iperm, int *prefix);
+int topological_sort_kahn(int uplo, int n, int base, const int *ai, const int *aj, int *iperm,
+                          int *prefix);
 void transpose(int rows, int cols, int base, const int *ai, const int *aj,
                const double *av, int *t_ai, int *t_aj, double *t_av);
 void permute(int n, int base, const int *ai, const int *aj, const double *av,

@@ -212,3 +212,50 @@ def test_trsv_partition_never_reads_a_later_part(lab):
     with pytest.raises(lab.LAError) as e:
         lab.trsv_partition("L", 2, 0, np.array([0, 0, 1], np.int32), np.array([1], np.int32), 2)
     assert e.value.name == "LA_ERR_INVALID_ARG"
+
+
+def test_topological_sort_kahn_bit_exact(lab, orc, golden):
+    """TopologicalSort (matrix_utils.hpp:583-635, Kahn's order) against the
+    compiled reference: iperm, prefix and the return value (the last level's
+    index) bit for bit, both triangles, base 0 and 1, the golden matrices and
+    seeded random triangles; the level sets equal TopologicalSort2's; a cycle
+    is reported instead of looping."""
+    rf = orc.ref()
+    if rf is None:
+        pytest.skip("oracle/_ref not built (reference tree absent)")
+    P = orc.ptr
+    mats = [(name, n, ai, aj) for name, m, n, ai, aj, av in golden_matrices(golden) if m == n]
+    rng = np.random.default_rng(11)
+    for k, n in enumerate((1, 50, 3000)):
+        rows = [np.sort(rng.choice(n, min(n, 4), replace=False)) for _ in range(n)]
+        ai = np.concatenate([[0], np.cumsum([len(c) for c in rows])]).astype(np.int32)
+        mats.append((f"random{k}", n, ai, np.concatenate(rows).astype(np.int32)))
+    checked = 0
+    for name, n, ai, aj in mats:
+        for lower in (True, False):
+            t_ai, t_aj, _ = strict_triangle(n, ai, aj, np.zeros(len(aj)), lower)
+            for base in (0, 1):
+                uplo = "L" if lower else "U"
+                b_ai = np.ascontiguousarray(t_ai + base, np.int32)  # kept alive for the call
+                b_aj = np.ascontiguousarray(t_aj + base, np.int32)
+                r, ip, pf = lab.TopologicalSort(uplo, n, base, b_ai, b_aj)
+                ip_ref = np.empty(n, np.int32)
+                pf_ref = np.empty(n + 2, np.int32)
+                r_ref = rf.la_ref_topological_sort(0 if lower else 1, n, base, P(b_ai), P(b_aj),
+                                                   P(ip_ref), P(pf_ref))
+                assert r == r_ref, (name, uplo, base)
+                assert np.array_equal(ip, ip_ref), (name, uplo, base)
+                assert np.array_equal(pf, pf_ref[: r_ref + 2]), (name, uplo, base)
+                lv2, ip2, pf2 = lab.TopologicalSort2(uplo, n, base, b_ai, b_aj)
+                assert lv2 == r + 1 and np.array_equal(pf, pf2), (name, uplo, base)
+                for l in range(lv2):  # same rows per level, another order inside it
+                    seg = slice(pf2[l], pf2[l + 1])
+                    assert np.array_equal(np.sort(ip[seg]), np.sort(ip2[seg])), (name, l)
+            checked += 1
+    assert checked >= 10
+    # n == 0, and a cycle (row 0 reads row 1, row 1 reads row 0)
+    r, ip, pf = lab.TopologicalSort("L", 0, 0, np.zeros(1, np.int32), np.zeros(0, np.int32))
+    assert r == 0 and pf.tolist() == [0, 0]
+    with pytest.raises(lab.LAError) as e:
+        lab.TopologicalSort("L", 2, 0, np.array([0, 1, 2], np.int32), np.array([1, 0], np.int32))
+    assert e.value.name == "LA_ERR_INVALID_ARG"
