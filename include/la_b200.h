@@ -186,6 +186,21 @@ la_status la_topological_sort2(la_uplo uplo, int n, int base, const int *ai,
  * bit-identical iperm/perm (values carry the base). */
 la_status la_rcm(int n, int base, const int *ai, const int *aj, int *iperm,
                  int *perm);
+/* permuteVec (matrix_utils.hpp:562-576): out[i] = v[iperm[i] - base], or a
+ * copy when iperm is NULL. */
+la_status la_permute_vec(int n, int base, const double *v, const int *iperm, double *out);
+/* inversePermute (utils/utils.cpp:101-108): iperm[perm[i] - base] = i + base;
+ * LA_ERR_INVALID_ARG unless perm is a permutation. */
+la_status la_inverse_permute(int n, int base, const int *perm, int *iperm);
+/* Diagonal (matrix_utils.hpp:677-704): per row the position (with base) of
+ * the diagonal entry in diagpos and its value in diag (either may be NULL;
+ * with invert != 0, 1/value, 0 giving 1); *all_present = the reference's
+ * bool (0 when some row has no diagonal entry: its position is then where
+ * the entry would go and its value what is stored there, 0 past the last
+ * entry, where the reference reads beyond its arrays).  Rows' columns must
+ * be sorted (LA_ERR_BAD_CSR otherwise). */
+la_status la_diagonal(int n, int base, const int *ai, const int *aj, const double *av,
+                      int *diagpos, double *diag, int invert, int *all_present);
 /* permute (matrix_utils.hpp:429-472): B(i,:) = A(iperm[i],:), columns mapped
  * through perm (may be NULL: rows only, permuteRow :474-480) and re-sorted. */
 la_status la_permute(int n, int base, const int *ai, const int *aj,

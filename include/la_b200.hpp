@@ -250,6 +250,50 @@ void ForwardSubstitutionT(const COLTYPE size, const int base, ROWTYPE const *ai,
   check(s, "la_trsv_host");
 }
 
+// permute / permuteRow / permuteVec (matrix_utils.hpp:429-480, 562-576),
+// Diagonal (:677-704) and inversePermute (utils/utils.cpp:101-108): host
+// functions, bit-identical to the reference.
+template <typename ROWTYPE, typename COLTYPE, typename VALTYPE>
+void permute(const COLTYPE rows, const int base, ROWTYPE const *ai, COLTYPE const *aj,
+             VALTYPE const *av, COLTYPE const *iperm, COLTYPE const *perm,
+             ROWTYPE *permed_ai, COLTYPE *permed_aj, VALTYPE *permed_av) {
+  require_int_double<ROWTYPE, COLTYPE, VALTYPE>();
+  check(la_permute(rows, base, ai, aj, av, iperm, perm, permed_ai, permed_aj, permed_av),
+        "la_permute");
+}
+
+template <typename ROWTYPE, typename COLTYPE, typename VALTYPE>
+void permuteRow(const COLTYPE rows, const int base, ROWTYPE const *ai, COLTYPE const *aj,
+                VALTYPE const *av, COLTYPE const *iperm, ROWTYPE *permed_ai,
+                COLTYPE *permed_aj, VALTYPE *permed_av) {
+  permute(rows, base, ai, aj, av, iperm, (COLTYPE const *)nullptr, permed_ai, permed_aj,
+          permed_av);
+}
+
+template <typename COLTYPE, typename VALTYPE>
+void permuteVec(const COLTYPE rows, const int base, VALTYPE const *const v,
+                COLTYPE const *const iperm, VALTYPE *const permed_v) {
+  require_int_double<COLTYPE, COLTYPE, VALTYPE>();
+  check(la_permute_vec(rows, base, v, iperm, permed_v), "la_permute_vec");
+}
+
+template <typename ROWTYPE, typename COLTYPE, typename VALTYPE>
+bool Diagonal(const COLTYPE rows, const int base, ROWTYPE const *ai, COLTYPE const *aj,
+              VALTYPE const *av, ROWTYPE *diagpos, VALTYPE *diag, const bool invert = false) {
+  require_int_double<ROWTYPE, COLTYPE, VALTYPE>();
+  int all = 0;
+  check(la_diagonal(rows, base, ai, aj, av, diagpos, diag, invert ? 1 : 0, &all),
+        "la_diagonal");
+  return all != 0;
+}
+
+template <typename VEC>
+void inversePermute(VEC &iperm, const VEC &perm, const int base) {
+  iperm.resize(perm.size());
+  check(la_inverse_permute((int)perm.size(), base, perm.data(), iperm.data()),
+        "la_inverse_permute");
+}
+
 // TopologicalSort<TS> (matrix_utils.hpp:583-635, Kahn's breadth-first
 // order), bit-identical output, including the return value (the last level's
 // index) and prefix's length (that + 2).

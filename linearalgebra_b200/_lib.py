@@ -77,6 +77,9 @@ _SIGS = {
     "la_trsv_analysis_transposed": [I, I, I, P, P, P, P, I, C.POINTER(P)],
     "la_trsv_partition": [I, I, I, P, P, I, P, P],
     "la_topological_sort": [I, I, I, P, P, P, P, P],
+    "la_permute_vec": [I, I, P, P, P],
+    "la_inverse_permute": [I, I, P, P],
+    "la_diagonal": [I, I, P, P, P, P, P, I, P],
     "la_trsv": [P, P, P, P],
     "la_trsv_launch": [P, P, P, P],
     "la_trsv_status": [P, P],

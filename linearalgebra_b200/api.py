@@ -41,6 +41,7 @@ __all__ = [
     "spmv_transpose", "sddmm_pattern", "ForwardSubstitutionT", "ForwardSubstitution",
     "BackwardSubstitution", "LevelScheduleForwardSubstitution",
     "LevelScheduleBackwardSubstitution", "trsv_partition", "TopologicalSort",
+    "PermuteVec", "InversePermute", "Diagonal",
 ]
 
 
@@ -388,6 +389,35 @@ def Permute(n, base, ai, aj, av, iperm, perm=None):
     call("la_permute", int(n), int(base), _ptr(ai), _ptr(aj), _ptr(av),
          _ptr(iperm), _ptr(perm), _ptr(p_ai), _ptr(p_aj), _ptr(p_av))
     return p_ai, p_aj[:nnz], p_av[:nnz]
+
+
+def PermuteVec(rows, base, v, iperm=None):
+    """``permuteVec`` (matrix_utils.hpp:562-576): v[iperm[i] - base]."""
+    v = _f64(v)
+    out = np.empty(rows, np.float64)
+    ip = None if iperm is None else _i32(iperm)
+    call("la_permute_vec", int(rows), int(base), _ptr(v), _ptr(ip), _ptr(out))
+    return out
+
+
+def InversePermute(perm, base=0):
+    """``inversePermute`` (utils.cpp:101-108): iperm[perm[i] - base] = i + base."""
+    perm = _i32(perm)
+    iperm = np.empty(len(perm), np.int32)
+    call("la_inverse_permute", len(perm), int(base), _ptr(perm), _ptr(iperm))
+    return iperm
+
+
+def Diagonal(rows, base, ai, aj, av, invert=False):
+    """``Diagonal`` (matrix_utils.hpp:677-704): (all diagonal entries present,
+    diagpos with base, diag values)."""
+    ai, aj, av = _i32(ai), _i32(aj), _f64(av)
+    pos = np.empty(rows, np.int32)
+    d = np.empty(rows, np.float64)
+    ok = C.c_int()
+    call("la_diagonal", int(rows), int(base), _ptr(ai), _ptr(aj), _ptr(av), _ptr(pos),
+         _ptr(d), 1 if invert else 0, C.byref(ok))
+    return bool(ok.value), pos, d
 
 
 def Transpose(rows, cols, base, ai, aj, av=None):

@@ -401,6 +401,38 @@ la_status la_permute(int n, int base, const int *ai, const int *aj,
   return LA_OK;
 }
 
+la_status la_permute_vec(int n, int base, const double *v, const int *iperm, double *out) {
+  LA_CHECK_ARG(v && out && n >= 0, "arguments");
+  permute_vec(n, base, v, iperm, out);
+  return LA_OK;
+}
+
+la_status la_inverse_permute(int n, int base, const int *perm, int *iperm) {
+  LA_CHECK_ARG(perm && iperm && n >= 0, "arguments");
+  std::vector<char> seen(n, 0);
+  for (int i = 0; i < n; i++) {
+    const int p = perm[i] - base;
+    LA_CHECK_ARG(p >= 0 && p < n && !seen[p], "perm must be a permutation");
+    seen[p] = 1;
+  }
+  inverse_permute(n, base, perm, iperm);
+  return LA_OK;
+}
+
+la_status la_diagonal(int n, int base, const int *ai, const int *aj, const double *av,
+                      int *diagpos, double *diag, int invert, int *all_present) {
+  LA_CHECK_ARG(ai && (aj || ai[n] == base) && (av || !diag) && n >= 0, "arguments");
+  std::string why;
+  if (!valid_csr(n, n, base, ai, aj, &why)) {
+    set_error("invalid CSR: %s", why.c_str());
+    return LA_ERR_BAD_CSR;
+  }
+  const bool all = diagonal(n, base, ai, aj, av, diagpos, diag, invert != 0);
+  if (all_present)
+    *all_present = all ? 1 : 0;
+  return LA_OK;
+}
+
 la_status la_transpose(int rows, int cols, int base, const int *ai,
                        const int *aj, const double *av, int *t_ai, int *t_aj,
                        double *t_av) {

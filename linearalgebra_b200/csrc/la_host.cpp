@@ -190,6 +190,49 @@ void permute(int n, int base, const int *ai, const int *aj, const double *av,
   }
 }
 
+// matrix_utils.hpp:562-576 permuteVec: out[i] = v[iperm[i] - base] (a copy
+// without iperm).
+void permute_vec(int n, int base, const double *v, const int *iperm, double *out) {
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; i++)
+    out[i] = v[iperm ? iperm[i] - base : i];
+}
+
+// utils.cpp:101-108 inversePermute: iperm[perm[i] - base] = i + base.
+void inverse_permute(int n, int base, const int *perm, int *iperm) {
+  for (int i = 0; i < n; i++)
+    iperm[perm[i] - base] = i + base;
+}
+
+// matrix_utils.hpp:677-704 Diagonal: per row the first stored column not
+// below the row (a binary search over the row's sorted columns); diagpos
+// gets its position (with base), diag its value (inverted when asked, 0
+// becoming 1).  Returns false when some row has no diagonal entry; that
+// row's position is where the diagonal would go, and its value is what is
+// stored there -- 0 past the last entry, where the reference reads beyond
+// its arrays.
+bool diagonal(int n, int base, const int *ai, const int *aj, const double *av, int *diagpos,
+              double *diag, bool invert) {
+  const int nnz = ai[n] - base;
+  bool all = true;
+  for (int i = 0; i < n; i++) {
+    const int *lo = aj + ai[i] - base, *hi = aj + ai[i + 1] - base;
+    const int *at = std::lower_bound(lo, hi, i + base);
+    const int k = (int)(at - aj);
+    if (at == hi || *at != i + base)
+      all = false;
+    if (diagpos)
+      diagpos[i] = k + base;
+    if (diag) {
+      double v = k < nnz ? av[k] : 0.0;
+      if (invert)
+        v = v == 0 ? 1.0 : 1.0 / v;
+      diag[i] = v;
+    }
+  }
+  return all;
+}
+
 // matrix_utils.hpp:720-803 SplitLDU: strict lower, diagonal (0 when
 // missing), strict upper; entries keep their column order.
 void split_ldu(int n, int base, const int *ai, const int *aj, const double *av,

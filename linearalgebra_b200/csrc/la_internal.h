@@ -71,6 +71,10 @@ int topological_sort2(int uplo, int n, int base, const int *ai, const int *aj,
                       int *iperm, int *prefix);
 int topological_sort_kahn(int uplo, int n, int base, const int *ai, const int *aj, int *iperm,
                           int *prefix);
+void permute_vec(int n, int base, const double *v, const int *iperm, double *out);
+void inverse_permute(int n, int base, const int *perm, int *iperm);
+bool diagonal(int n, int base, const int *ai, const int *aj, const double *av, int *diagpos,
+              double *diag, bool invert);
 void transpose(int rows, int cols, int base, const int *ai, const int *aj,
                const double *av, int *t_ai, int *t_aj, double *t_av);
 void permute(int n, int base, const int *ai, const int *aj, const double *av,

@@ -72,6 +72,9 @@ _REF_SIGS = {
     "la_ref_transpose": ([I, I, I, P, P, P, P, P, P], None),
     "la_ref_permute": ([I, I, P, P, P, P, P, P, P, P], None),
     "la_ref_valid_csr": ([I, I, I, P, P], I),
+    "la_ref_permute_vec": ([I, I, P, P, P], None),
+    "la_ref_inverse_permute": ([I, I, P, P], None),
+    "la_ref_diagonal": ([I, I, P, P, P, P, P, I], I),
     "la_ref_icc0": ([I, I, P, P, P, D, P], I),
     "la_ref_serial_cm": ([I, I, P, P, P, P], None),
     "la_ref_pcg_create": ([I, I, I, P, P, P, P, P, P], P),

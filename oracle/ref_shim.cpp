@@ -265,6 +265,24 @@ void la_ref_permute(int n, int base, const int *ai, const int *aj,
   permute(n, base, ai, aj, av, iperm, perm, p_ai, p_aj, p_av);
 }
 
+// permuteVec (matrix_utils.hpp:562-576)
+void la_ref_permute_vec(int n, int base, const double *v, const int *iperm, double *out) {
+  permuteVec(n, base, v, iperm, out);
+}
+
+// inversePermute (utils/utils.cpp:101-108)
+void la_ref_inverse_permute(int n, int base, const int *perm, int *iperm) {
+  std::vector<MKL_INT> p(perm, perm + n), ip;
+  utils::inversePermute(ip, p, base);
+  std::memcpy(iperm, ip.data(), sizeof(int) * ip.size());
+}
+
+// Diagonal (matrix_utils.hpp:677-704); returns its bool
+int la_ref_diagonal(int n, int base, const int *ai, const int *aj, const double *av,
+                    int *diagpos, double *diag, int invert) {
+  return Diagonal(n, base, ai, aj, av, diagpos, diag, invert != 0) ? 1 : 0;
+}
+
 // ValidCSR (matrix_utils.hpp:985-1014)
 int la_ref_valid_csr(int rows, int cols, int base, const int *ai,
                      const int *aj) {

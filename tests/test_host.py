@@ -259,3 +259,61 @@ def test_topological_sort_kahn_bit_exact(lab, orc, golden):
     with pytest.raises(lab.LAError) as e:
         lab.TopologicalSort("L", 2, 0, np.array([0, 1, 2], np.int32), np.array([1, 0], np.int32))
     assert e.value.name == "LA_ERR_INVALID_ARG"
+
+
+def test_permute_vec_inverse_permute_diagonal_bit_exact(lab, orc, golden):
+    """permuteVec, inversePermute and Diagonal (matrix_utils.hpp:562-576,
+    677-704; utils.cpp:101-108) against the compiled reference, base 0 and 1:
+    bit for bit, Diagonal's bool included (the golden matrices without a full
+    diagonal report false, the positions where the entry would go); rows only
+    (permuteRow) is la_permute with no column permutation."""
+    rf = orc.ref()
+    if rf is None:
+        pytest.skip("oracle/_ref not built (reference tree absent)")
+    P = orc.ptr
+    checked = 0
+    for name, m, n, ai, aj, av in golden_matrices(golden):
+        if m != n:
+            continue
+        rng = np.random.default_rng(n)
+        for base in (0, 1):
+            perm = (rng.permutation(n) + base).astype(np.int32)
+            ip = lab.InversePermute(perm, base)
+            ip_ref = np.empty(n, np.int32)
+            rf.la_ref_inverse_permute(n, base, P(perm), P(ip_ref))
+            assert np.array_equal(ip, ip_ref), (name, base)
+            v = rng.standard_normal(n)
+            out_ref = np.empty(n)
+            rf.la_ref_permute_vec(n, base, P(v), P(ip), P(out_ref))
+            assert np.array_equal(lab.PermuteVec(n, base, v, ip), out_ref), (name, base)
+            b_ai = np.ascontiguousarray(ai + base, np.int32)
+            b_aj = np.ascontiguousarray(aj + base, np.int32)
+            # the reference reads one value (and one column) past the row when
+            # the last row lacks its diagonal: give it padded copies to read
+            av_pad = np.append(av, 0.0)
+            aj_pad = np.append(b_aj, np.int32(-1)).astype(np.int32)
+            for invert in (False, True):
+                ok, pos, d = lab.Diagonal(n, base, b_ai, b_aj, av, invert)
+                pos_ref = np.empty(n, np.int32)
+                d_ref = np.empty(n)
+                ok_ref = rf.la_ref_diagonal(n, base, P(b_ai), P(aj_pad), P(av_pad), P(pos_ref),
+                                            P(d_ref), int(invert))
+                assert ok == bool(ok_ref), (name, base, invert)
+                assert np.array_equal(pos, pos_ref), (name, base)
+                full = np.ones(n, bool)
+                if not ok:  # values past the last entry are undefined in the reference
+                    full = pos - base < len(av)
+                assert np.array_equal(d[full], d_ref[full]), (name, base, invert)
+            # permuteRow: la_permute with rows only
+            p_ai, p_aj, p_av = lab.Permute(n, base, b_ai, b_aj, av, ip, None)
+            r_ai = np.empty(n + 1, np.int32)
+            r_aj = np.empty(len(aj), np.int32)
+            r_av = np.empty(len(aj))
+            rf.la_ref_permute(n, base, P(b_ai), P(b_aj), P(av), P(ip), None, P(r_ai), P(r_aj),
+                              P(r_av))
+            assert np.array_equal(p_ai, r_ai) and np.array_equal(p_aj, r_aj), (name, base)
+            assert np.array_equal(p_av, r_av), (name, base)
+        checked += 1
+    assert checked >= 5
+    with pytest.raises(lab.LAError):
+        lab.InversePermute(np.array([0, 0, 2], np.int32))
