@@ -8,6 +8,8 @@
 
 #include "la_internal.h"
 
+#include <omp.h>
+
 #include <algorithm>
 #include <climits>
 #include <cmath>
@@ -357,21 +359,56 @@ struct Bfs {
   const int *ai, *aj;
   int base;
   std::vector<int> level, queue;
-  // BFS from src over its component; returns the level count.
+  std::vector<std::vector<int>> found; // per-thread finds of one frontier
+  // BFS from src over its component; returns the level count.  Level by
+  // level: a large frontier is split over the host's threads, which claim a
+  // vertex by a compare-and-swap on its level.  The levels, and the set of
+  // vertices on each, are those of the sequential search; only the order
+  // inside a level may differ, and rcm() never depends on it.  Only the
+  // vertices the previous run reached are reset, so a pattern with many
+  // components is not O(n) per component.
   int run(int n, int src) {
-    level.assign(n, -1);
+    if ((int)level.size() != n)
+      level.assign(n, -1);
+    else
+      for (int v : queue)
+        level[v] = -1;
     queue.clear();
     queue.push_back(src);
     level[src] = 0;
-    for (size_t h = 0; h < queue.size(); h++) {
-      const int u = queue[h];
-      for (int k = ai[u] - base; k < ai[u + 1] - base; k++) {
-        const int v = aj[k] - base;
-        if (level[v] < 0) {
-          level[v] = level[u] + 1;
-          queue.push_back(v);
-        }
+    for (size_t head = 0; head < queue.size();) {
+      const size_t begin = head, end = queue.size();
+      const int lev = level[queue[begin]] + 1;
+      head = end;
+      if (end - begin < 4096) {
+        for (size_t h = begin; h < end; h++)
+          for (int k = ai[queue[h]] - base; k < ai[queue[h] + 1] - base; k++) {
+            const int v = aj[k] - base;
+            if (level[v] < 0) {
+              level[v] = lev;
+              queue.push_back(v);
+            }
+          }
+        continue;
       }
+#pragma omp parallel
+      {
+#pragma omp single
+        found.assign(omp_get_num_threads(), {});
+        std::vector<int> &mine = found[omp_get_thread_num()];
+#pragma omp for schedule(static)
+        for (long long h = (long long)begin; h < (long long)end; h++)
+          for (int k = ai[queue[h]] - base; k < ai[queue[h] + 1] - base; k++) {
+            int *lv = &level[aj[k] - base];
+            int expect = -1;
+            if (__atomic_load_n(lv, __ATOMIC_RELAXED) < 0 &&
+                __atomic_compare_exchange_n(lv, &expect, lev, false, __ATOMIC_RELAXED,
+                                            __ATOMIC_RELAXED))
+              mine.push_back(aj[k] - base);
+          }
+      }
+      for (const std::vector<int> &f : found)
+        queue.insert(queue.end(), f.begin(), f.end());
     }
     return level[queue.back()] + 1;
   }
