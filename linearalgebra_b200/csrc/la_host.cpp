@@ -419,7 +419,7 @@ void rcm(int n, int base, const int *ai, const int *aj, int *iperm, int *perm) {
   std::vector<int> deg(n);
   for (int i = 0; i < n; i++)
     deg[i] = ai[i + 1] - ai[i];
-  Bfs bfs{ai, aj, base, {}, {}};
+  Bfs bfs{ai, aj, base, {}, {}, {}};
 
   // components, ordered by their largest node; members ascending
   std::vector<int> comp(n, -1), comp_max;
