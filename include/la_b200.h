@@ -186,6 +186,16 @@ la_status la_topological_sort2(la_uplo uplo, int n, int base, const int *ai,
  * bit-identical iperm/perm (values carry the base). */
 la_status la_rcm(int n, int base, const int *ai, const int *aj, int *iperm,
                  int *perm);
+/* ILU(0) on A's own pattern, from scratch (no reference counterpart: the
+ * reference factors ILU through MKL, and its level-0 path never fills the
+ * upper-part positions, incomplete_lu.cpp:166 / :267-269).  lu_av (A's
+ * pattern) receives L strictly below the diagonal (unit diagonal implied)
+ * and U on and above it, so that (L U)_ij = A_ij on the pattern; split it
+ * with la_split_ldu and apply it with a unit-lower and an upper la_trsv plan,
+ * as incomplete_lu.cpp:36-48 does.  Rows' columns sorted, every diagonal
+ * stored (LA_ERR_INVALID_ARG otherwise); LA_ERR_BREAKDOWN on a zero pivot. */
+la_status la_ilu0(int n, int base, const int *ai, const int *aj, const double *av,
+                  double *lu_av);
 /* permuteVec (matrix_utils.hpp:562-576): out[i] = v[iperm[i] - base], or a
  * copy when iperm is NULL. */
 la_status la_permute_vec(int n, int base, const double *v, const int *iperm, double *out);

@@ -78,6 +78,7 @@ _SIGS = {
     "la_trsv_partition": [I, I, I, P, P, I, P, P],
     "la_topological_sort": [I, I, I, P, P, P, P, P],
     "la_permute_vec": [I, I, P, P, P],
+    "la_ilu0": [I, I, P, P, P, P],
     "la_inverse_permute": [I, I, P, P],
     "la_diagonal": [I, I, P, P, P, P, P, I, P],
     "la_trsv": [P, P, P, P],

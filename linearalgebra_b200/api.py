@@ -41,7 +41,7 @@ __all__ = [
     "spmv_transpose", "sddmm_pattern", "ForwardSubstitutionT", "ForwardSubstitution",
     "BackwardSubstitution", "LevelScheduleForwardSubstitution",
     "LevelScheduleBackwardSubstitution", "trsv_partition", "TopologicalSort",
-    "PermuteVec", "InversePermute", "Diagonal",
+    "PermuteVec", "InversePermute", "Diagonal", "ILU0",
 ]
 
 
@@ -389,6 +389,15 @@ def Permute(n, base, ai, aj, av, iperm, perm=None):
     call("la_permute", int(n), int(base), _ptr(ai), _ptr(aj), _ptr(av),
          _ptr(iperm), _ptr(perm), _ptr(p_ai), _ptr(p_aj), _ptr(p_av))
     return p_ai, p_aj[:nnz], p_av[:nnz]
+
+
+def ILU0(n, base, ai, aj, av):
+    """ILU(0) on A's pattern (host): L strictly below the diagonal (unit
+    diagonal implied) and U on and above it, in A's pattern."""
+    ai, aj, av = _i32(ai), _i32(aj), _f64(av)
+    lu = np.empty(max(len(av), 1), np.float64)
+    call("la_ilu0", int(n), int(base), _ptr(ai), _ptr(aj), _ptr(av), _ptr(lu))
+    return lu[: len(av)]
 
 
 def PermuteVec(rows, base, v, iperm=None):

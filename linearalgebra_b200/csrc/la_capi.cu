@@ -401,6 +401,26 @@ la_status la_permute(int n, int base, const int *ai, const int *aj,
   return LA_OK;
 }
 
+la_status la_ilu0(int n, int base, const int *ai, const int *aj, const double *av,
+                  double *lu_av) {
+  LA_CHECK_ARG(ai && aj && av && lu_av && n >= 0, "arguments");
+  std::string why;
+  if (!valid_csr(n, n, base, ai, aj, &why)) {
+    set_error("invalid CSR: %s", why.c_str());
+    return LA_ERR_BAD_CSR;
+  }
+  const int r = ilu0(n, base, ai, aj, av, lu_av);
+  if (r == -2) {
+    set_error("la_ilu0: a row has no diagonal entry");
+    return LA_ERR_INVALID_ARG;
+  }
+  if (r >= 0) {
+    set_error("la_ilu0: zero pivot in row %d", r);
+    return LA_ERR_BREAKDOWN;
+  }
+  return LA_OK;
+}
+
 la_status la_permute_vec(int n, int base, const double *v, const int *iperm, double *out) {
   LA_CHECK_ARG(v && out && n >= 0, "arguments");
   permute_vec(n, base, v, iperm, out);

@@ -235,6 +235,51 @@ bool diagonal(int n, int base, const int *ai, const int *aj, const double *av, i
   return all;
 }
 
+// ILU(0) on A's own pattern (no reference routine: the reference factors ILU
+// through MKL, and its own level-0 path never fills the upper-part
+// positions, incomplete_lu.cpp:166 / :267-269).  Row by row (IKJ order): for
+// each stored k < i, ascending, l_ik = a_ik / u_kk, then a_ij -= l_ik * u_kj
+// for every stored j > k that row k also holds.  The result, in A's pattern,
+// is the strictly lower L (unit diagonal implied) and U with its diagonal --
+// what SplitLDU splits and the unit-lower / upper solves apply
+// (incomplete_lu.cpp:36-48).  Returns the first row whose pivot is zero, or
+// -1; -2 when a row has no diagonal entry.
+int ilu0(int n, int base, const int *ai, const int *aj, const double *av, double *lu) {
+  const int nnz = ai[n] - base;
+  std::memcpy(lu, av, sizeof(double) * (size_t)nnz);
+  std::vector<int> diag(n), where(n, -1);
+  for (int i = 0; i < n; i++) {
+    const int *lo = aj + ai[i] - base, *hi = aj + ai[i + 1] - base;
+    const int *at = std::lower_bound(lo, hi, i + base);
+    if (at == hi || *at != i + base)
+      return -2;
+    diag[i] = (int)(at - aj);
+  }
+  for (int i = 0; i < n; i++) {
+    const int r0 = ai[i] - base, r1 = ai[i + 1] - base;
+    for (int k = r0; k < r1; k++)
+      where[aj[k] - base] = k;
+    for (int k = r0; k < diag[i]; k++) {
+      const int c = aj[k] - base; // c < i
+      const double piv = lu[diag[c]];
+      if (piv == 0.0)
+        return c;
+      lu[k] /= piv;
+      const double l = lu[k];
+      for (int m = diag[c] + 1; m < ai[c + 1] - base; m++) {
+        const int w = where[aj[m] - base];
+        if (w >= 0)
+          lu[w] -= l * lu[m];
+      }
+    }
+    if (lu[diag[i]] == 0.0)
+      return i;
+    for (int k = r0; k < r1; k++)
+      where[aj[k] - base] = -1;
+  }
+  return -1;
+}
+
 // matrix_utils.hpp:720-803 SplitLDU: strict lower, diagonal (0 when
 // missing), strict upper; entries keep their column order.
 void split_ldu(int n, int base, const int *ai, const int *aj, const double *av,

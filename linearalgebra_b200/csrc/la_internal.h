@@ -71,6 +71,7 @@ int topological_sort2(int uplo, int n, int base, const int *ai, const int *aj,
                       int *iperm, int *prefix);
 int topological_sort_kahn(int uplo, int n, int base, const int *ai, const int *aj, int *iperm,
                           int *prefix);
+int ilu0(int n, int base, const int *ai, const int *aj, const double *av, double *lu);
 void permute_vec(int n, int base, const double *v, const int *iperm, double *out);
 void inverse_permute(int n, int base, const int *perm, int *iperm);
 bool diagonal(int n, int base, const int *ai, const int *aj, const double *av, int *diagpos,

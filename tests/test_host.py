@@ -317,3 +317,67 @@ def test_permute_vec_inverse_permute_diagonal_bit_exact(lab, orc, golden):
     assert checked >= 5
     with pytest.raises(lab.LAError):
         lab.InversePermute(np.array([0, 0, 2], np.int32))
+
+
+def _ilu0_python(n, ai, aj, av):
+    """ILU(0), IKJ order, in plain Python (the same operations as la_ilu0)."""
+    lu = av.astype(np.float64).copy()
+    diag = [int(np.searchsorted(aj[ai[i]:ai[i + 1]], i)) + ai[i] for i in range(n)]
+    for i in range(n):
+        where = {int(aj[k]): k for k in range(ai[i], ai[i + 1])}
+        for k in range(ai[i], diag[i]):
+            c = int(aj[k])
+            lu[k] = lu[k] / lu[diag[c]]
+            for m in range(diag[c] + 1, ai[c + 1]):
+                w = where.get(int(aj[m]))
+                if w is not None:
+                    lu[w] = lu[w] - lu[k] * lu[m]
+    return lu
+
+
+def test_ilu0_defining_property_and_restatement(lab):
+    """la_ilu0: (L U)_ij = A_ij on A's pattern (L unit lower, U upper, both in
+    A's pattern) to rounding, on stencils and a random diagonally dominant
+    matrix; bit-identical to a plain-Python restatement; exact LU of a
+    tridiagonal matrix; zero pivot and missing diagonal reported."""
+    from linearalgebra_b200 import gen
+    rng = np.random.default_rng(3)
+    mats = [gen.laplacian_2d(12), gen.laplacian_3d(6), gen.stencil27(5)]
+    m = 150
+    dense = np.where(rng.random((m, m)) < 0.05, rng.uniform(-1, 1, (m, m)), 0.0)
+    np.fill_diagonal(dense, np.abs(dense).sum(1) + 1.0)
+    r, c = np.nonzero(dense)
+    ai = np.concatenate([[0], np.cumsum(np.bincount(r, minlength=m))]).astype(np.int32)
+    mats.append((m, ai, c.astype(np.int32), dense[r, c]))
+    for n, ai, aj, av in mats:
+        lu = lab.ILU0(n, 0, ai, aj, av)
+        assert np.array_equal(lu, _ilu0_python(n, ai, aj, av))
+        rows = np.repeat(np.arange(n), np.diff(ai))
+        L = np.eye(n)
+        U = np.zeros((n, n))
+        low = aj < rows
+        L[rows[low], aj[low]] = lu[low]
+        U[rows[~low], aj[~low]] = lu[~low]
+        A = np.zeros((n, n))
+        A[rows, aj] = av
+        prod = (L @ U)[rows, aj]
+        assert np.max(np.abs(prod - av)) <= 1e-12 * np.max(np.abs(av)), n
+    # tridiagonal: no fill, ILU(0) is the LU
+    n = 40
+    A = np.diag(np.full(n, 4.0)) + np.diag(np.full(n - 1, -1.0), 1) + np.diag(np.full(n - 1, -2.0), -1)
+    r, c = np.nonzero(A)
+    ai = np.concatenate([[0], np.cumsum(np.bincount(r, minlength=n))]).astype(np.int32)
+    lu = lab.ILU0(n, 0, ai, c.astype(np.int32), A[r, c])
+    L = np.eye(n)
+    U = np.zeros((n, n))
+    L[r[c < r], c[c < r]] = lu[c < r]
+    U[r[c >= r], c[c >= r]] = lu[c >= r]
+    assert np.allclose(L @ U, A, rtol=0, atol=1e-13)
+    with pytest.raises(lab.LAError) as e:  # zero pivot in row 0
+        lab.ILU0(2, 0, np.array([0, 2, 4], np.int32), np.array([0, 1, 0, 1], np.int32),
+                 np.array([0.0, 1.0, 1.0, 1.0]))
+    assert e.value.name == "LA_ERR_BREAKDOWN"
+    with pytest.raises(lab.LAError) as e:  # row 1 has no diagonal
+        lab.ILU0(2, 0, np.array([0, 1, 2], np.int32), np.array([0, 0], np.int32),
+                 np.array([1.0, 1.0]))
+    assert e.value.name == "LA_ERR_INVALID_ARG"
