@@ -283,6 +283,37 @@ def test_reference_free_solves_bit_exact(lab, orc, golden):
     assert checked >= 5
 
 
+def test_ilu0_apply_bit_exact(lab, orc):
+    """The ILU apply (incomplete_lu.cpp:36-48): la_ilu0's factor split by
+    SplitLDU, a unit-lower then an upper solve on the GPU -- bit for bit the
+    oracle's ForwardSubstitution / BackwardSubstitution of the same factor,
+    on 3D stencils and a nonsymmetric random pattern."""
+    from linearalgebra_b200 import gen
+    P = orc.ptr
+    rng = np.random.default_rng(21)
+    mats = [gen.laplacian_3d(16), gen.aniso7(12, seed=5)]
+    m = 2000  # nonsymmetric, diagonally dominant
+    rows = [np.union1d(rng.choice(m, 6, replace=False), [i]) for i in range(m)]
+    ai = np.concatenate([[0], np.cumsum([len(c) for c in rows])]).astype(np.int32)
+    aj = np.concatenate(rows).astype(np.int32)
+    av = rng.uniform(-1, 1, len(aj))
+    r = np.repeat(np.arange(m), np.diff(ai))
+    av[aj == r] = 8.0
+    mats.append((m, ai, aj, av))
+    for n, ai, aj, av in mats:
+        lu = lab.ILU0(n, 0, ai, aj, av)
+        (l_ai, l_aj, l_av), d, (u_ai, u_aj, u_av) = lab.SplitLDU(n, 0, ai, aj, lu)
+        b = rng.uniform(-1, 1, n)
+        t = lab.ForwardSubstitution(n, 0, l_ai, l_aj, l_av, b, np.zeros(n))
+        x = lab.BackwardSubstitution(n, 0, u_ai, u_aj, u_av, d, t, np.zeros(n))
+        t_ref = np.zeros(n)
+        orc.port().oracle_forward_substitution(n, 0, P(l_ai), P(l_aj), P(l_av), P(b), P(t_ref))
+        x_ref = np.zeros(n)
+        orc.port().oracle_backward_substitution(n, 0, P(u_ai), P(u_aj), P(u_av), P(d), P(t_ref),
+                                                P(x_ref))
+        assert np.array_equal(t, t_ref) and np.array_equal(x, x_ref), n
+
+
 def test_forward_substitution_t(lab, orc, golden):
     """ForwardSubstitutionT (triangle_solve.hpp:87-98): the unit lower solve
     with L = U^T given as the CSR of the strict upper triangle U.  The GPU
