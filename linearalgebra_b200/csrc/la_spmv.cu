@@ -563,7 +563,9 @@ la_status spmv_host_chunked(la_spmv_plan_t P, double alpha, const double *x, dou
   LA_CUDA_TRY(cudaMemcpyAsync(hx, x, sizeof(double) * A->ncols, cudaMemcpyHostToDevice, P->hst));
   if (beta != 0.0)
     LA_CUDA_TRY(cudaMemcpyAsync(hy, y, sizeof(double) * n, cudaMemcpyHostToDevice, P->hst));
-  const int nt = P->ntiles, chunks = std::min(8, nt);
+  // chunks of at least 64 tiles (64K nonzeros): below that the launches and
+  // copies of a chunk cost more than the overlap returns
+  const int nt = P->ntiles, chunks = std::min(8, nt / 64);
   if (chunks <= 1 || A->dtype != LA_F64) {
     LA_TRY(spmv_launch(P, alpha, hx, beta, hy, hy, LA_F64, P->hst));
     LA_CUDA_TRY(cudaMemcpyAsync(y, hy, sizeof(double) * n, cudaMemcpyDeviceToHost, P->hst));
