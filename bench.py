@@ -45,6 +45,14 @@ def spmv_bytes(n, nnz, vbytes=8, xbytes=8, beta=False):
     return nnz * (vbytes + 4) + (n + 1) * 4 + n * xbytes + n * xbytes * (2 if beta else 1)
 
 
+def workload_config(n, nnz, byt):
+    """The workload's description, identical in both arms (arm-specific
+    notes such as the parallelism go outside it)."""
+    return {"workload": WORKLOAD, "rows": n, "nnz": nnz, "bytes_per_step": byt,
+            "row_lengths": "ceil(Pareto(2.1)) clipped to [1, 20000]",
+            "l2": "inputs larger than L2 (matrix %.2f GB); no flush" % (byt / 1e9)}
+
+
 def measured_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -181,8 +189,7 @@ def run_reference(args, rank, world):
         "n_gpus": world, "steps": steps, "warmup": args.warmup,
         "ms_per_step": dt / steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "rows": n, "nnz": nnz, "bytes_per_step": byt,
-                   "l2": "matrix larger than L2; no flush", "parallelism": "host OpenMP"},
+        "config": workload_config(n, nnz, byt), "parallelism": f"host OpenMP x{T}",
         "cpu_baseline": {"value": v, "unit": "GB/s", "cores": T, "kind": "reference",
                          "sample": f"{steps} full SegSumSPMV calls on the same matrix"},
         "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -265,9 +272,9 @@ def extras(la, torch, peak):
     # IC(0)-PCG, FP64 vs mixed: the RCM-ordered 128^3 Laplacian (C3) and the
     # 192^3 anisotropic diffusion (C5, mixed precision at scale)
     out["pcg"], mats = pcg_case(la, torch, "C3_lap3d_128_rcm", gen.laplacian_3d(128))
-    out["pcg_c5"], _ = pcg_case(la, torch, "C5_aniso7_192_rcm", gen.aniso7(192, seed=0))
+    out["pcg_c5"], mats_c5 = pcg_case(la, torch, "C5_aniso7_192_rcm", gen.aniso7(192, seed=0))
     out["adjoint_c4"] = adjoint_case(la, torch, peak)
-    return out, mats
+    return out, {"pcg": mats, "pcg_c5": mats_c5}
 
 
 def adjoint_case(la, torch, peak):
@@ -383,13 +390,13 @@ def pcg_case(la, torch, label, matrix):
                      "GB/s_algorithmic": b32 * r32.iterations / (r32.solve_ms * 1e-3) / 1e9},
            "speedup_mixed_vs_fp64": r64.solve_ms / r32.solve_ms,
            "trsv_schedules": sched}
-    return res, (b_ai, b_aj, b_av, ua, uj, f, bvec, r64)
+    return res, (b_ai, b_aj, b_av, ua, uj, f, bvec, r64, x64.cpu().numpy(), x32.cpu().numpy())
 
 
 def cpu_pcg(mats):
     import oracle
     rf = oracle.ref()
-    b_ai, b_aj, b_av, ua, uj, f, bvec, _ = mats
+    b_ai, b_aj, b_av, ua, uj, f, bvec, r64, x64, x32 = mats
     n = len(b_ai) - 1
     P = oracle.ptr
     T = rf.la_ref_max_threads()
@@ -400,9 +407,13 @@ def cpu_pcg(mats):
     it = rf.la_ref_pcg_solve(h, P(bvec), P(x), 1e-10, 5000, P(rel))
     dt = time.perf_counter() - t0
     rf.la_ref_pcg_destroy(h)
+    xn = float(np.linalg.norm(x))
     return {"kind": "reference kernels (ParallelSPMV + OptimizedTriangularSolve<Barrier>) "
                     "composed into PCG; MKL PCG driver absent",
-            "cores": T, "iterations": it, "s": dt, "rel_residual": float(rel[0])}
+            "cores": T, "iterations": it, "s": dt, "rel_residual": float(rel[0]),
+            "gpu_fp64_iterations": r64.iterations,
+            "rel_diff_gpu_fp64_vs_cpu": float(np.linalg.norm(x64 - x)) / xn,
+            "rel_diff_gpu_mixed_vs_cpu": float(np.linalg.norm(x32 - x)) / xn}
 
 
 def run_case(case):
@@ -550,15 +561,15 @@ def main():
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generator standing in for the reference's "
                 "downloaded matrices)",
-        "config": {"workload": WORKLOAD, "rows": n, "nnz": nnz, "bytes_per_step": byt,
-                   "row_lengths": "ceil(Pareto(2.1)) clipped to [1, 20000]",
-                   "l2": "inputs larger than L2 (matrix %.2f GB); no flush" % (byt / 1e9),
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "config": workload_config(n, nnz, byt),
+        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
         "roofline": {"bound": "hbm", "achieved": byt / launch_s / 1e9, "peak": peak,
                      "unit": "GB/s", "frac": byt / launch_s / 1e9 / peak,
                      "peak_kind": peak_kind,
                      "kernel": "spmv_tile_kernel<SegSum, f64> + spmv_merge_kernel (one step)",
-                     "traffic": profiled_traffic("spmv_tile_kernel_segsum_f64_powerlaw4M")},
+                     "traffic": profiled_traffic("spmv_tile_kernel_segsum_f64_powerlaw4M"),
+                     "traffic_source": "DRAM bytes per launch from a stored ncu capture of "
+                                       "this workload (profiles/traffic.txt), not this run"},
         "e2e": {"value": e2e, "unit": "GB/s", "h2d_bytes_per_step": n * 8,
                 "d2h_bytes_per_step": n * 8, "steps": e2e_steps,
                 "api": "SPMV.__call__ host arrays -> la_spmv_host", "matches_device": bool(ok)},
@@ -578,10 +589,11 @@ def main():
             ex, mats = extras(la, torch, peak)
             result["extras"] = ex
             if not args.no_cpu_pcg:
-                try:
-                    ex["pcg"]["cpu_reference"] = cpu_pcg(mats)
-                except Exception as e:
-                    ex["pcg"]["cpu_reference"] = {"error": str(e)}
+                for key, m in mats.items():
+                    try:
+                        ex[key]["cpu_reference"] = cpu_pcg(m)
+                    except Exception as e:
+                        ex[key]["cpu_reference"] = {"error": str(e)}
     if rank == 0:
         print(json.dumps(result), flush=True)
     if pg:

@@ -120,7 +120,11 @@ la_status la_spmv_plan_destroy(la_spmv_plan_t plan);
  * y = alpha*A*x + beta*y in FP64 with the SegSum or ALBUS form, from DEVICE
  * CSR arrays (d_ai[n+1], d_aj[nnz], d_av[nnz], base 0 or 1), d_x (ncols
  * entries) and d_y (n entries, not aliasing d_x); the result equals
- * la_spmv's.  No cudaMalloc, cudaFree or allocating library call is made:
+ * la_spmv's.  The arrays are used as given, without the host validation
+ * la_csr_create does: d_ai[0] must equal base and d_ai[n] - base must equal
+ * nnz.  If not, the result is undefined, but no write leaves d_y[0, n) and
+ * no read of d_aj / d_av goes beyond the nnz entries declared.  No
+ * cudaMalloc, cudaFree or allocating library call is made:
  * the scratch lives in a fixed device array of 655,616 bytes that every GPU
  * loading the library holds until the process exits, so nnz is limited to
  * LA_SPMV_NOALLOC_MAX_NNZ (larger inputs return LA_ERR_INVALID_ARG).  The
@@ -328,6 +332,14 @@ la_status la_trsv_levels(la_trsv_plan_t plan, int *levels, int *iperm,
  * force level order or a partition; LA_TRSV_RING=<rows> (a power of two, at
  * least 32) forces a ring of that size onto a partition. */
 la_status la_trsv_schedule(la_trsv_plan_t plan, int *schedule, int *parts);
+/* Kernel variant of the plan (no reference counterpart; every variant
+ * computes the same bits): *slots = the number of leading entries of a row
+ * held in registers (3, 4, 8 or 16; 0 for the grouped level-order form whose
+ * rows are read in groups of 8), *second_row = 1 when the partitioned FP32
+ * kernel holds each thread's second row of a level in registers too (chosen
+ * when some level of a part is wider than the CTA; LA_TRSV_W2=0 in the
+ * environment before the analysis keeps it off). */
+la_status la_trsv_variant(la_trsv_plan_t plan, int *slots, int *second_row);
 la_status la_trsv_plan_destroy(la_trsv_plan_t plan);
 
 /* ---------------------------------------------------------- IC(0)-PCG */

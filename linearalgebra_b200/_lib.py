@@ -87,6 +87,7 @@ _SIGS = {
     "la_trsv_host": [P, P, P],
     "la_trsv_levels": [P, IP, P, P],
     "la_trsv_schedule": [P, IP, IP],
+    "la_trsv_variant": [P, IP, IP],
     "la_trsv_plan_destroy": [P],
     "la_pcg_create": [P, P, P, P, I, C.POINTER(P)],
     "la_pcg_solve": [P, P, P, D, I, C.POINTER(PcgInfo), P],

@@ -263,6 +263,13 @@ class OptimizedTriangularSolve:
         call("la_trsv_schedule", self.h, C.byref(s), C.byref(p))
         return {0: "levels", 1: "parts", 2: "parts-ring"}[s.value], p.value
 
+    def variant(self):
+        """(register slots per row, second-row register sets): the kernel
+        variant the analysis picked (la_trsv_variant)."""
+        k, w = C.c_int(), C.c_int()
+        call("la_trsv_variant", self.h, C.byref(k), C.byref(w))
+        return k.value, bool(w.value)
+
     def levels(self):
         lv = C.c_int()
         call("la_trsv_levels", self.h, C.byref(lv), None, None)

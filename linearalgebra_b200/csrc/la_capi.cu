@@ -688,6 +688,13 @@ la_status la_trsv_schedule(la_trsv_plan_t plan, int *schedule, int *parts) {
   return LA_OK;
 }
 
+la_status la_trsv_variant(la_trsv_plan_t plan, int *slots, int *second_row) {
+  LA_CHECK_ARG(plan && slots && second_row, "arguments");
+  *slots = plan->kd;
+  *second_row = plan->sched == 1 && plan->w2 ? 1 : 0;
+  return LA_OK;
+}
+
 la_status la_trsv_plan_destroy(la_trsv_plan_t plan) {
   delete plan;
   return LA_OK;

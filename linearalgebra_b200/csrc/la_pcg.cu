@@ -236,6 +236,10 @@ la_status pcg_run(la_pcg_t S, const X *rhs, X *y, X *r, X *z, X *p, X *q,
     const double rel = std::sqrt(rr) / r0;
     *rel_out = rel;
     if (!std::isfinite(rel)) {
+      // a solve that gave up on a wait leaves sentinel NaNs behind: report
+      // (and clear) the timeout rather than a breakdown it caused
+      LA_TRY(trsv_check(S->L, st));
+      LA_TRY(trsv_check(S->U, st));
       set_error("PCG breakdown: non-finite residual at iteration %d", it);
       return LA_ERR_BREAKDOWN;
     }
@@ -315,6 +319,9 @@ la_status pcg_mixed(la_pcg_t S, const double *b, double *x, double bn, double rt
     rn_prev = rn;
     bool updated = false;
     if (!std::isfinite(rn)) {
+      loc->iterations = it;
+      LA_TRY(trsv_check(S->L, st)); // a timed-out solve, not a breakdown
+      LA_TRY(trsv_check(S->U, st));
       set_error("mixed PCG breakdown: non-finite residual at iteration %d", it);
       loc->iterations = it;
       return LA_ERR_BREAKDOWN;

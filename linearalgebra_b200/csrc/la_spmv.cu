@@ -634,7 +634,13 @@ la_status noalloc_scratch(void **out) {
   return LA_OK;
 }
 
-// tile_row[t] = upper_bound(ai, min(t * kTile, nnz) + base) - 1, t <= ntiles
+// tile_row[t] = upper_bound(ai, min(t * kTile, nnz) + base) - 1, t <= ntiles.
+// The arrays come straight from the caller, so nothing on the host has
+// checked that ai[0] == base and ai[n] - base == nnz.  The rows are clamped
+// so that a violation can never send a write outside y[0, n): a tile's first
+// row to [0, n - 1] (the merge writes y at it), the end row to [0, n].  With
+// nnz > ai[n] - base the surplus tiles then hold empty segments of row n - 1
+// (their aj / av reads stay below the nnz the caller declared).
 __global__ void noalloc_tile_row_kernel(const int n, const int nnz, const int base,
                                         const int *__restrict__ ai, const int ntiles,
                                         int *tile_row) {
@@ -650,7 +656,7 @@ __global__ void noalloc_tile_row_kernel(const int n, const int nnz, const int ba
     else
       lo = mid + 1;
   }
-  tile_row[t] = lo - 1;
+  tile_row[t] = max(0, min(lo - 1, t < ntiles ? n - 1 : n));
 }
 
 template <int FORM>

@@ -848,6 +848,8 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
   bool w2 = false;
   if constexpr (sizeof(X) == 4) {
     w2 = ks == 3 && widest > part_threads<X, 3>();
+    if (const char *e = std::getenv("LA_TRSV_W2")) // testing / tuning override
+      w2 = w2 && std::atoi(e) != 0;
     if (w2) {
       fns[0] = part_fn<X, X, false, 3, true>(), fns[1] = part_fn<X, X, true, 3, true>();
       threads = part_threads<X, 3>();

@@ -19,7 +19,18 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 PORT_SO = HERE / "liboracle.so"
 REF_SO = HERE / "_ref" / "libla_ref.so"
-REFERENCE_TREE = Path("/root/reference")
+
+
+def reference_tree() -> Path:
+    """Where the reference's sources lie: $LA_REFERENCE_TREE if set, else the
+    default of oracle/Makefile's REF (the one place that default is kept)."""
+    import os
+    env = os.environ.get("LA_REFERENCE_TREE")
+    if env:
+        return Path(env)
+    out = subprocess.run(["make", "-s", "-C", str(HERE), "print-ref"], capture_output=True,
+                         text=True)
+    return Path(out.stdout.strip()) if out.returncode == 0 and out.stdout.strip() else Path()
 
 P, I, D = C.c_void_p, C.c_int, C.c_double
 
@@ -36,6 +47,7 @@ _PORT_SIGS = {
     "oracle_backward_substitution": ([I, I, P, P, P, P, P, P], None),
     "oracle_forward_substitution_t": ([I, I, P, P, P, P, P], None),
     "oracle_level_solve": ([I, P, P, I, P, P, P, P, P, P], None),
+    "oracle_level_solve_f32": ([I, P, P, I, P, P, P, P, P, P], None),
     "oracle_topological_sort2": ([I, I, I, P, P, P, P], I),
     "oracle_split_ldu": ([I, I, P, P, P, P, P, P, P, P, P, P, P, P], None),
     "oracle_split_triangle": ([I, I, I, P, P, P, P, P, P], I),
@@ -98,8 +110,9 @@ def _load(path, sigs):
 def build(reference_too: bool = True) -> None:
     """Run oracle/Makefile (the C port always; the reference if present)."""
     subprocess.run(["make", "-s", "-C", str(HERE), "oracle"], check=True)
-    if reference_too and REFERENCE_TREE.exists():
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
+    tree = reference_tree()
+    if reference_too and str(tree) not in ("", ".") and (tree / "sparse_mat_op").is_dir():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={tree}"], check=True)
 
 
 def port():

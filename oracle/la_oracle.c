@@ -340,6 +340,28 @@ void oracle_level_solve(int nlev, const int *iperm, const int *prefix,
     }
 }
 
+/* The same level-scheduled apply with FP32 storage and FP32 arithmetic: the
+ * factor values and the diagonal rounded to float once (as the FP32 plans
+ * store them), every product, sum, difference and quotient a single float
+ * operation (ISO C: no contraction into FMAs, FLT_EVAL_METHOD 0 on x86-64),
+ * so an FP32 solve in the reference's row order is reproduced bit for bit. */
+void oracle_level_solve_f32(int nlev, const int *iperm, const int *prefix,
+                            int base, const int *ai, const int *aj,
+                            const double *av, const double *diag, const float *b,
+                            float *x) {
+  for (int l = 0; l < nlev; l++)
+    for (int p = prefix[l]; p < prefix[l + 1]; p++) {
+      int i = iperm[p] - base;
+      float v = 0.0f;
+      for (int j = ai[i] - base; j < ai[i + 1] - base; j++) {
+        const float prod = (float)av[j] * x[aj[j] - base];
+        v = v + prod;
+      }
+      const float r = b[i] - v;
+      x[i] = diag ? r / (float)diag[i] : r;
+    }
+}
+
 /* ------------------------------------------------------- level scheduling */
 
 /* matrix_utils.hpp:637-675 TopologicalSort2<L|U> (uplo 0 / 1): depth of

@@ -42,7 +42,7 @@ import oracle  # noqa: E402
 from oracle import ptr  # noqa: E402
 from linearalgebra_b200 import gen, mmio  # noqa: E402
 
-REF = Path("/root/reference")
+REF = oracle.reference_tree()
 OUT = Path(__file__).resolve().parent / "golden.npz"
 
 

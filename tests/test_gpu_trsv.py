@@ -230,10 +230,64 @@ def test_trsv_schedules_bit_identical(lab, orc, monkeypatch, schedule):
             assert np.array_equal(x, ref), (n, uplo, schedule, parts)
             ts32, x32 = solve(lab, uplo, n, c_ai, c_aj, c_av, d, b, dtype=np.float32)
             assert rel(x32, ref) <= 1e-4
+            # FP32 storage and arithmetic in the same order: the FP32 oracle bit for bit
+            assert np.array_equal(x32, _oracle_f32(orc, lv, ip, pf, c_ai, c_aj, c_av, d, b))
             monkeypatch.setenv("LA_TRSV_SCHEDULE", "flags" if schedule == "parts" else "parts")
             _, y32 = solve(lab, uplo, n, c_ai, c_aj, c_av, d, b, dtype=np.float32)
             monkeypatch.setenv("LA_TRSV_SCHEDULE", schedule)
             assert np.array_equal(x32, y32), (n, uplo, "fp32 schedules differ")
+
+
+def _oracle_f32(orc, lv, ip, pf, c_ai, c_aj, c_av, d, b):
+    """The oracle's FP32 level solve (float storage, one float operation per
+    step, the reference's row order), as float64 for comparison."""
+    P = orc.ptr
+    n = len(c_ai) - 1
+    b32 = np.ascontiguousarray(b, np.float32)
+    x = np.zeros(n, np.float32)
+    orc.port().oracle_level_solve_f32(lv, P(ip), P(pf), 0, P(c_ai), P(c_aj), P(c_av),
+                                      P(None if d is None else np.ascontiguousarray(d)),
+                                      P(b32), P(x))
+    return x.astype(np.float64)
+
+
+def test_trsv_second_row_variant_bit_identical(lab, orc, monkeypatch):
+    """The partitioned FP32 kernel with second-row register sets (W2), which
+    the analysis picks for 3-slot FP32 factors when some level of a part is
+    wider than the CTA -- the variant the large anisotropic PCG's FP32 solves
+    run.  Two parts on RCM-ordered 40^3 / 48^3 IC(0) factors make the parts'
+    levels wider than 512 rows, so W2 is provably selected; its solve equals
+    the FP32 oracle bit for bit, the partitioned kernel without W2
+    (LA_TRSV_W2=0) bit for bit, and the FP64 oracle within 1e-4."""
+    from linearalgebra_b200 import gen
+    P = orc.ptr
+    monkeypatch.setenv("LA_TRSV_SCHEDULE", "parts")
+    monkeypatch.setenv("LA_TRSV_PARTS", "2")
+    monkeypatch.delenv("LA_TRSV_W2", raising=False)
+    checked = 0
+    for n, ai, aj, av in (gen.laplacian_3d(40), gen.aniso7(48, seed=2)):
+        _, lt, ut, d = _ic_factor_rcm(lab, n, ai, aj, av)
+        for uplo, (c_ai, c_aj, c_av) in (("L", lt), ("U", ut)):
+            b = np.random.default_rng(n + 11).uniform(-1, 1, n)
+            ts32, x32 = solve(lab, uplo, n, c_ai, c_aj, c_av, d, b, dtype=np.float32)
+            assert ts32.schedule() == ("parts", 2), ts32.schedule()
+            assert ts32.variant() == (3, True), ts32.variant()
+            lv, ip, pf = ts32.levels()
+            assert np.array_equal(x32, _oracle_f32(orc, lv, ip, pf, c_ai, c_aj, c_av, d, b)), \
+                (n, uplo)
+            ref = np.zeros(n)
+            orc.port().oracle_level_solve(lv, P(ip), P(pf), 0, P(c_ai), P(c_aj), P(c_av),
+                                          P(d), P(b), P(ref))
+            e = rel(x32, ref)
+            print(f"W2 n={n} {uplo}: fp32 err vs fp64 oracle {e:.2e}")
+            assert e <= 1e-4
+            monkeypatch.setenv("LA_TRSV_W2", "0")
+            ts1, y32 = solve(lab, uplo, n, c_ai, c_aj, c_av, d, b, dtype=np.float32)
+            monkeypatch.delenv("LA_TRSV_W2")
+            assert ts1.variant() == (3, False)
+            assert np.array_equal(x32, y32), (n, uplo, "W2 differs from one register set")
+            checked += 1
+    assert checked == 4
 
 
 def test_reference_free_solves_bit_exact(lab, orc, golden):
