@@ -93,6 +93,7 @@ _SIGS = {
     "la_pcg_solve": [P, P, P, D, I, C.POINTER(PcgInfo), P],
     "la_pcg_solve_host": [P, P, P, D, I, C.POINTER(PcgInfo)],
     "la_pcg_adjoint": [P, P, P, P, P, D, I, C.POINTER(PcgInfo), P],
+    "la_pcg_fused": [P, IP],
     "la_pcg_destroy": [P],
 }
 _RESTYPES = {"la_last_error_string": C.c_char_p, "la_version": C.c_char_p}

@@ -544,6 +544,13 @@ class PCG:
                          info.rel_residual, info.solve_ms,
                          _lib.STATUS_NAMES.get(st, str(st)))
 
+    def fused(self):
+        """True when each iteration's vector work runs in the two fused
+        cooperative kernels (la_pcg_fused)."""
+        f = C.c_int()
+        call("la_pcg_fused", self.h, C.byref(f))
+        return bool(f.value)
+
     def adjoint(self, g, u, dl_db, dl_dvalues=None, rtol=1e-10, maxit=10000):
         """lambda = A^-T g into dl_db; dL/dA_ij = -lambda_i u_j into dl_dvalues
         (device FP64 tensors)."""

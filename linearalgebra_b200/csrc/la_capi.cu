@@ -21,8 +21,8 @@ la_status spmv_noalloc(la_spmv_kind kind, int n, int nnz, int base, const int *a
 la_status spmv_plan_build(la_spmv_plan_t P);
 la_status spmv_host_chunked(la_spmv_plan_t P, double alpha, const double *x, double beta,
                             double *y);
-la_status trsv_launch(la_trsv_plan_t P, const void *b, void *x,
-                      cudaStream_t st);
+la_status trsv_launch(la_trsv_plan_t P, const void *b, void *x, cudaStream_t st,
+                      bool prefilled = false);
 la_status trsv_build(la_trsv_plan_t P, const int *ai, const int *aj,
                      const double *av, const double *diag, const int *iperm = nullptr,
                      const int *prefix = nullptr, int nlevels = 0);
@@ -736,6 +736,12 @@ la_status la_pcg_adjoint(la_pcg_t s, const double *g, const double *u,
                          la_pcg_info *info, la_stream_t stream) {
   LA_CHECK_ARG(s && g && u && dl_db && g != dl_db && rtol > 0 && maxit > 0, "arguments");
   return pcg_adjoint(s, g, u, dl_db, dl_dvalues, rtol, maxit, info, S(stream));
+}
+
+la_status la_pcg_fused(la_pcg_t s, int *fused) {
+  LA_CHECK_ARG(s && fused, "arguments");
+  *fused = s->fused ? 1 : 0;
+  return LA_OK;
 }
 
 la_status la_pcg_destroy(la_pcg_t s) {

@@ -174,8 +174,12 @@ struct la_pcg_s {
   la::DevBuf r, z, p, q, t;        // FP64 work vectors
   la::DevBuf r32, z32, p32, q32, t32, d32, p32b; // FP32 inner vectors (mixed)
   la::DevBuf scal, partials, ticket;
+  la::DevBuf bar; // grid barrier of the fused kernels: arrivals, generation, error
   la::DevBuf hb, hx;
   int dot_blocks = 0;
+  // the iteration's vector work in two cooperative kernels (dot products
+  // finished inside them) instead of separate dot / update launches
+  bool fused = true;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double *h_rr = nullptr;       // pinned host copy of the residual norm
   cudaEvent_t ev_rr = nullptr;  // marks its arrival

@@ -24,6 +24,7 @@
 #include "la_internal.h"
 
 #include <cmath>
+#include <cstdlib>
 #include <utility>
 
 namespace la {
@@ -31,8 +32,8 @@ namespace la {
 la_status spmv_launch(la_spmv_plan_t P, double alpha, const void *x,
                       double beta, void *y, const void *yin, la_dtype vd,
                       cudaStream_t st);
-la_status trsv_launch(la_trsv_plan_t P, const void *b, void *x,
-                      cudaStream_t st);
+la_status trsv_launch(la_trsv_plan_t P, const void *b, void *x, cudaStream_t st,
+                      bool prefilled = false);
 la_status trsv_check(la_trsv_plan_t P, cudaStream_t st);
 la_status trsv_build(la_trsv_plan_t P, const int *ai, const int *aj,
                      const double *av, const double *diag, const int *iperm = nullptr,
@@ -51,6 +52,33 @@ enum { S_RZ = 0, S_PQ, S_RR, S_ALPHA, S_BETA, S_DOT, S_RZ0, S_COUNT };
 // the partials in block order and applies `op`.
 enum DotOp { OP_STORE = 0, OP_ALPHA = 1, OP_BETA = 2 };
 
+// One block's share of a dot product, in the order every dot here uses:
+// each thread's running sum s (its elements i = block * kDotThreads + tid +
+// k * grid * kDotThreads, accumulated by fused multiply-adds in k order),
+// a shuffle tree inside each warp, then the warps' sums in warp order.  The
+// block total lands in thread 0's return value.
+__device__ __forceinline__ double block_sum(double s, double *red) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1)
+    s += __shfl_down_sync(0xffffffffu, s, d);
+  if ((threadIdx.x & 31) == 0)
+    red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < kDotThreads / 32; w++)
+      t += red[w];
+  return t;
+}
+
+// The block totals of `partials` (`count` of them) added in block order.
+__device__ __forceinline__ double sum_partials(const double *partials, int count) {
+  double t = 0.0;
+  for (int k = 0; k < count; k++)
+    t += __ldcg(partials + k);
+  return t;
+}
+
 template <typename XA, typename XB>
 __global__ void __launch_bounds__(kDotThreads)
     dot_kernel(const int n, const XA *__restrict__ a, const XB *__restrict__ b,
@@ -60,18 +88,10 @@ __global__ void __launch_bounds__(kDotThreads)
   double s = 0.0;
   for (int i = blockIdx.x * kDotThreads + threadIdx.x; i < n;
        i += gridDim.x * kDotThreads)
-    s += double(a[i]) * double(b[i]);
-#pragma unroll
-  for (int d = 16; d > 0; d >>= 1)
-    s += __shfl_down_sync(0xffffffffu, s, d);
-  if ((threadIdx.x & 31) == 0)
-    red[threadIdx.x >> 5] = s;
-  __syncthreads();
+    s = __fma_rn(double(a[i]), double(b[i]), s);
+  const double bt = block_sum(s, red);
   if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (int w = 0; w < kDotThreads / 32; w++)
-      t += red[w];
-    partials[blockIdx.x] = t;
+    partials[blockIdx.x] = bt;
     __threadfence();
     last = atomicAdd(ticket, 1u) + 1u == gridDim.x;
   }
@@ -79,9 +99,7 @@ __global__ void __launch_bounds__(kDotThreads)
   if (!last || threadIdx.x != 0)
     return;
   __threadfence();
-  double t = 0.0;
-  for (int k = 0; k < (int)gridDim.x; k++)
-    t += __ldcg(partials + k);
+  const double t = sum_partials(partials, gridDim.x);
   *ticket = 0u;
   scal[S_DOT] = t;
   if (op == OP_ALPHA) { // alpha = (r, z) / (p, A p)
@@ -101,8 +119,8 @@ __global__ void xr_update_kernel(const int n, X *x, X *r, const X *p,
   const double al = scal[S_ALPHA];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += gridDim.x * blockDim.x) {
-    x[i] = X(double(x[i]) + al * double(p[i]));
-    r[i] = X(double(r[i]) - al * double(q[i]));
+    x[i] = X(__fma_rn(al, double(p[i]), double(x[i])));
+    r[i] = X(__fma_rn(-al, double(q[i]), double(r[i])));
   }
 }
 
@@ -113,7 +131,7 @@ __global__ void p_next_kernel(const int n, X *pn, const X *p, const X *z,
   const double be = scal[S_BETA];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += gridDim.x * blockDim.x)
-    pn[i] = X(double(z[i]) + be * double(p[i]));
+    pn[i] = X(__fma_rn(be, double(p[i]), double(z[i])));
 }
 
 // p = z + beta p
@@ -123,7 +141,148 @@ __global__ void p_update_kernel(const int n, X *p, const X *z,
   const double be = scal[S_BETA];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += gridDim.x * blockDim.x)
-    p[i] = X(double(z[i]) + be * double(p[i]));
+    p[i] = X(__fma_rn(be, double(p[i]), double(z[i])));
+}
+
+// ------------------------------------------------------ fused iteration
+// Two cooperative kernels carry all of an iteration's vector work (the role
+// of the RCI loop's dot products and axpys, mkl_solver.cpp:190-238):
+//   pcg_update_kernel:    alpha = (r, z) / (p, q); x += alpha p; r -= alpha q;
+//                         ||r||^2; the next solves' outputs filled with the
+//                         sentinel they wait on;
+//   pcg_direction_kernel: beta = (r, z)_new / (r, z)_old; p' = z + beta p.
+// A dot product ends in a grid-wide barrier, after which every block adds the
+// block totals itself, in block order, so no extra launch is needed to
+// finish it.  Grid, element assignment, per-thread order and reduction tree
+// are those of dot_kernel, and each update is the same single fused
+// multiply-add as in xr_update_kernel / p_update_kernel: the iterates are
+// bit-identical to the unfused sequence's.  Launched cooperatively (all
+// blocks resident); the barrier's wait is bounded by the global timer.
+constexpr unsigned long long kBarrierNs = 1000000000ull; // 1 s
+
+__device__ __forceinline__ unsigned long long pcg_global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+// bar[0]: arrivals, bar[1]: generation, bar[2]: error word (1 = a wait gave up)
+__device__ void grid_barrier(unsigned *bar) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned *gen = bar + 1;
+    const unsigned g = *gen; // read before arriving: the generation to leave
+    __threadfence();
+    if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      const unsigned long long t0 = pcg_global_ns();
+      while (*gen == g) {
+        if (pcg_global_ns() - t0 > kBarrierNs) {
+          atomicExch(bar + 2, 1u);
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+template <typename X> struct AllOnes;
+template <> struct AllOnes<double> {
+  static __device__ __forceinline__ double v() { return __longlong_as_double(-1ll); }
+};
+template <> struct AllOnes<float> {
+  static __device__ __forceinline__ float v() { return __int_as_float(-1); }
+};
+
+// partials: 2 * gridDim.x doubles ((p, q) totals, then ||r||^2 totals).
+template <typename X>
+__global__ void __launch_bounds__(kDotThreads)
+    pcg_update_kernel(const int n, X *x, X *r, const X *__restrict__ p,
+                      const X *__restrict__ q, X *t_fill, X *z_fill, double *partials,
+                      unsigned *ticket, double *scal, unsigned *bar) {
+  __shared__ double red[kDotThreads / 32];
+  __shared__ double alpha_s;
+  __shared__ bool last;
+  const int stride = gridDim.x * kDotThreads, i0 = blockIdx.x * kDotThreads + threadIdx.x;
+  double s = 0.0;
+  for (int i = i0; i < n; i += stride)
+    s = __fma_rn(double(p[i]), double(q[i]), s);
+  const double bt = block_sum(s, red);
+  if (threadIdx.x == 0)
+    partials[blockIdx.x] = bt;
+  grid_barrier(bar);
+  if (threadIdx.x == 0) {
+    const double pq = sum_partials(partials, gridDim.x);
+    const double al = scal[S_RZ] / pq; // alpha = (r, z) / (p, A p)
+    alpha_s = al;
+    if (blockIdx.x == 0) {
+      scal[S_PQ] = pq;
+      scal[S_ALPHA] = al;
+    }
+  }
+  __syncthreads();
+  const double al = alpha_s;
+  const X sentinel = AllOnes<X>::v();
+  s = 0.0;
+  for (int i = i0; i < n; i += stride) {
+    x[i] = X(__fma_rn(al, double(p[i]), double(x[i])));
+    const X ri = X(__fma_rn(-al, double(q[i]), double(r[i])));
+    r[i] = ri;
+    s = __fma_rn(double(ri), double(ri), s);
+    t_fill[i] = sentinel;
+    z_fill[i] = sentinel;
+  }
+  const double bt2 = block_sum(s, red);
+  if (threadIdx.x == 0) {
+    partials[gridDim.x + blockIdx.x] = bt2;
+    __threadfence();
+    last = atomicAdd(ticket, 1u) + 1u == gridDim.x;
+  }
+  __syncthreads();
+  if (!last || threadIdx.x != 0)
+    return;
+  __threadfence();
+  scal[S_DOT] = sum_partials(partials + gridDim.x, gridDim.x);
+  *ticket = 0u;
+}
+
+// pn = z + beta p (pn may equal p); beta and the new (r, z) into scal.
+template <typename X>
+__global__ void __launch_bounds__(kDotThreads)
+    pcg_direction_kernel(const int n, X *pn, const X *p, const X *__restrict__ r,
+                         const X *__restrict__ z, double *partials, double *scal,
+                         unsigned *bar) {
+  __shared__ double red[kDotThreads / 32];
+  __shared__ double beta_s;
+  const int stride = gridDim.x * kDotThreads, i0 = blockIdx.x * kDotThreads + threadIdx.x;
+  const double rz_old = scal[S_RZ]; // read before block 0 replaces it
+  double s = 0.0;
+  for (int i = i0; i < n; i += stride)
+    s = __fma_rn(double(r[i]), double(z[i]), s);
+  const double bt = block_sum(s, red);
+  if (threadIdx.x == 0)
+    partials[blockIdx.x] = bt;
+  grid_barrier(bar);
+  if (threadIdx.x == 0) {
+    const double rz = sum_partials(partials, gridDim.x);
+    const double be = rz / rz_old;
+    beta_s = be;
+    if (blockIdx.x == 0) {
+      scal[S_BETA] = be;
+      scal[S_RZ0] = rz_old;
+      scal[S_RZ] = rz;
+    }
+  }
+  __syncthreads();
+  const double be = beta_s;
+  for (int i = i0; i < n; i += stride)
+    pn[i] = X(__fma_rn(be, double(p[i]), double(z[i])));
 }
 
 // out = X(scale * in)
@@ -165,6 +324,46 @@ la_status dot(la_pcg_t S, const XA *a, const XB *b, int op, cudaStream_t st) {
       S->n, a, b, S->partials.as<double>(), S->ticket.as<unsigned>(),
       S->scal.as<double>(), op);
   LA_CUDA_TRY(cudaGetLastError());
+  return LA_OK;
+}
+
+template <typename X>
+la_status fused_update(la_pcg_t S, X *x, X *r, const X *p, const X *q, X *t, X *z,
+                       cudaStream_t st) {
+  int n = S->n;
+  double *partials = S->partials.as<double>(), *scal = S->scal.as<double>();
+  unsigned *ticket = S->ticket.as<unsigned>(), *bar = S->bar.as<unsigned>();
+  void *args[] = {&n, &x, &r, &p, &q, &t, &z, &partials, &ticket, &scal, &bar};
+  LA_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)pcg_update_kernel<X>,
+                                          dim3(S->dot_blocks), dim3(kDotThreads), args, 0, st));
+  return LA_OK;
+}
+
+template <typename X>
+la_status fused_direction(la_pcg_t S, X *pn, const X *p, const X *r, const X *z,
+                          cudaStream_t st) {
+  int n = S->n;
+  double *partials = S->partials.as<double>(), *scal = S->scal.as<double>();
+  unsigned *bar = S->bar.as<unsigned>();
+  void *args[] = {&n, &pn, &p, &r, &z, &partials, &scal, &bar};
+  LA_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)pcg_direction_kernel<X>,
+                                          dim3(S->dot_blocks), dim3(kDotThreads), args, 0, st));
+  return LA_OK;
+}
+
+// Reads (and clears) the fused kernels' barrier error word; synchronises st.
+la_status barrier_check(la_pcg_t S, cudaStream_t st) {
+  if (!S->fused)
+    return LA_OK;
+  unsigned h = 0;
+  LA_CUDA_TRY(cudaMemcpyAsync(&h, S->bar.as<unsigned>() + 2, sizeof(unsigned),
+                              cudaMemcpyDeviceToHost, st));
+  LA_CUDA_TRY(cudaStreamSynchronize(st));
+  if (h) {
+    LA_CUDA_TRY(cudaMemsetAsync(S->bar.p, 0, S->bar.bytes, st));
+    set_error("PCG: a grid-wide barrier wait exceeded its 1 s bound");
+    return LA_ERR_TIMEOUT;
+  }
   return LA_OK;
 }
 
@@ -216,9 +415,13 @@ la_status pcg_run(la_pcg_t S, const X *rhs, X *y, X *r, X *z, X *p, X *q,
                               cudaMemcpyDeviceToDevice, st));
   for (int it = 1; it <= maxit; it++) {
     LA_TRY(spmv_launch(S->Ap, 1.0, p, 0.0, q, q, vd, st));
-    LA_TRY(dot(S, p, q, OP_ALPHA, st));
-    xr_update_kernel<X><<<g, 256, 0, st>>>(n, y, r, p, q, S->scal.as<double>());
-    LA_TRY(dot(S, r, r, OP_STORE, st));
+    if (S->fused) {
+      LA_TRY(fused_update<X>(S, y, r, p, q, t, z, st));
+    } else {
+      LA_TRY(dot(S, p, q, OP_ALPHA, st));
+      xr_update_kernel<X><<<g, 256, 0, st>>>(n, y, r, p, q, S->scal.as<double>());
+      LA_TRY(dot(S, r, r, OP_STORE, st));
+    }
     // ||r||^2 travels to the host while the next iteration's preconditioner
     // and direction update are already queued behind it, so the GPU does
     // not idle through the host's check.  They write only t, z, p and the
@@ -226,10 +429,14 @@ la_status pcg_run(la_pcg_t S, const X *rhs, X *y, X *r, X *z, X *p, X *q,
     LA_CUDA_TRY(cudaMemcpyAsync(S->h_rr, S->scal.as<double>() + S_DOT, sizeof(double),
                                 cudaMemcpyDeviceToHost, st));
     LA_CUDA_TRY(cudaEventRecord(S->ev_rr, st));
-    LA_TRY(trsv_launch(S->L, r, t, st));
-    LA_TRY(trsv_launch(S->U, t, z, st));
-    LA_TRY(dot(S, r, z, OP_BETA, st));
-    p_update_kernel<X><<<g, 256, 0, st>>>(n, p, z, S->scal.as<double>());
+    LA_TRY(trsv_launch(S->L, r, t, st, S->fused));
+    LA_TRY(trsv_launch(S->U, t, z, st, S->fused));
+    if (S->fused) {
+      LA_TRY(fused_direction<X>(S, p, p, r, z, st));
+    } else {
+      LA_TRY(dot(S, r, z, OP_BETA, st));
+      p_update_kernel<X><<<g, 256, 0, st>>>(n, p, z, S->scal.as<double>());
+    }
     LA_CUDA_TRY(cudaEventSynchronize(S->ev_rr));
     const double rr = *S->h_rr;
     *iters = it;
@@ -290,9 +497,14 @@ la_status pcg_mixed(la_pcg_t S, const double *b, double *x, double bn, double rt
   int updates = 0, it;
   for (it = 1; it <= maxit; it++) {
     LA_TRY(spmv_launch(S->Ap, 1.0, p32, 0.0, q32, q32, LA_F32, st));
-    LA_TRY(dot(S, p32, q32, OP_ALPHA, st));
-    xr_update_kernel<float><<<g, 256, 0, st>>>(n, d32, r32, p32, q32, S->scal.as<double>());
-    LA_TRY(dot(S, r32, r32, OP_STORE, st));
+    if (S->fused) {
+      LA_TRY(fused_update<float>(S, d32, r32, p32, q32, t32, z32, st));
+    } else {
+      LA_TRY(dot(S, p32, q32, OP_ALPHA, st));
+      xr_update_kernel<float><<<g, 256, 0, st>>>(n, d32, r32, p32, q32, S->scal.as<double>());
+      LA_TRY(dot(S, r32, r32, OP_STORE, st));
+    }
+    bool filled = S->fused; // t32 / z32 hold the solves' sentinel
     // As in pcg_run: ||r||^2 travels to the host while the next step's
     // preconditioner and direction are queued -- when the last residual was
     // well above the reliable-update threshold, so that no update is likely
@@ -305,10 +517,15 @@ la_status pcg_mixed(la_pcg_t S, const double *b, double *x, double bn, double rt
     LA_CUDA_TRY(cudaEventRecord(S->ev_rr, st));
     const bool ahead = rn_prev > 0.13 * rmax && rn_prev > 2.0 * rtol * bn;
     auto precondition = [&]() -> la_status {
-      LA_TRY(trsv_launch(S->L, r32, t32, st));
-      LA_TRY(trsv_launch(S->U, t32, z32, st));
-      LA_TRY(dot(S, r32, z32, OP_BETA, st));
-      p_next_kernel<float><<<g, 256, 0, st>>>(n, pn32, p32, z32, S->scal.as<double>());
+      LA_TRY(trsv_launch(S->L, r32, t32, st, filled));
+      LA_TRY(trsv_launch(S->U, t32, z32, st, filled));
+      filled = false;
+      if (S->fused) {
+        LA_TRY(fused_direction<float>(S, pn32, p32, r32, z32, st));
+      } else {
+        LA_TRY(dot(S, r32, z32, OP_BETA, st));
+        p_next_kernel<float><<<g, 256, 0, st>>>(n, pn32, p32, z32, S->scal.as<double>());
+      }
       return LA_OK;
     };
     if (ahead)
@@ -323,7 +540,6 @@ la_status pcg_mixed(la_pcg_t S, const double *b, double *x, double bn, double rt
       LA_TRY(trsv_check(S->L, st)); // a timed-out solve, not a breakdown
       LA_TRY(trsv_check(S->U, st));
       set_error("mixed PCG breakdown: non-finite residual at iteration %d", it);
-      loc->iterations = it;
       return LA_ERR_BREAKDOWN;
     }
     if (rn < kReliableDelta * rmax || rn / bn < rtol) {
@@ -433,10 +649,33 @@ la_status pcg_create(la_csr_t A, const int *u_ai, const int *u_aj,
         return fail(s);
   S->dot_blocks = std::max(1, std::min(2 * sm_count(), (n + kDotThreads - 1) / kDotThreads));
   if ((s = S->scal.alloc(sizeof(double) * S_COUNT)) != LA_OK ||
-      (s = S->partials.alloc(sizeof(double) * S->dot_blocks)) != LA_OK ||
-      (s = S->ticket.alloc(sizeof(unsigned))) != LA_OK)
+      (s = S->partials.alloc(sizeof(double) * 2 * S->dot_blocks)) != LA_OK ||
+      (s = S->ticket.alloc(sizeof(unsigned))) != LA_OK ||
+      (s = S->bar.alloc(sizeof(unsigned) * 4)) != LA_OK)
     return fail(s);
-  if (cudaMemset(S->ticket.p, 0, sizeof(unsigned)) != cudaSuccess ||
+  // The fused kernels need every block resident at once (cooperative
+  // launch); LA_PCG_FUSED=0 keeps the separate dot / update launches (same
+  // iterates, bit for bit).
+  S->fused = true;
+  if (const char *e = std::getenv("LA_PCG_FUSED"))
+    S->fused = std::atoi(e) != 0;
+  if (S->fused) {
+    const void *fns[] = {(const void *)pcg_update_kernel<double>,
+                         (const void *)pcg_update_kernel<float>,
+                         (const void *)pcg_direction_kernel<double>,
+                         (const void *)pcg_direction_kernel<float>};
+    for (const void *f : fns) {
+      int per_sm = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, kDotThreads, 0) !=
+              cudaSuccess ||
+          (long long)per_sm * sm_count() < S->dot_blocks) {
+        cudaGetLastError();
+        S->fused = false;
+      }
+    }
+  }
+  if (cudaMemset(S->bar.p, 0, S->bar.bytes) != cudaSuccess ||
+      cudaMemset(S->ticket.p, 0, sizeof(unsigned)) != cudaSuccess ||
       cudaEventCreate(&S->ev0) != cudaSuccess || cudaEventCreate(&S->ev1) != cudaSuccess ||
       cudaEventCreateWithFlags(&S->ev_rr, cudaEventDisableTiming) != cudaSuccess ||
       cudaMallocHost((void **)&S->h_rr, sizeof(double)) != cudaSuccess) {
@@ -479,6 +718,7 @@ la_status pcg_solve(la_pcg_t S, const double *b, double *x, double rtol,
     LA_TRY(trsv_check(S->L, st));
     LA_TRY(trsv_check(S->U, st));
   }
+  LA_TRY(barrier_check(S, st));
   if (info)
     *info = loc;
   if (res == LA_ERR_NOT_CONVERGED)

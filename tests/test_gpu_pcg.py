@@ -81,3 +81,32 @@ def test_pcg_host_path_and_not_converged(lab):
     assert r2.status == "LA_ERR_NOT_CONVERGED" and r2.iterations == 3
     with pytest.raises(lab.LAError):
         s.solve(b, x, rtol=1e-10, maxit=3)
+
+
+@pytest.mark.parametrize("case", ["lap3d_32", "aniso_24"])
+def test_pcg_fused_iteration_bit_identical(lab, monkeypatch, case):
+    """The fused iteration (dot products finished inside two cooperative
+    vector kernels, the solves' sentinel written by the update) gives the
+    same iterates as the separate dot / update launches, bit for bit, in FP64
+    and mixed precision: same iteration counts, same x."""
+    from linearalgebra_b200 import gen
+    n, ai, aj, av = {"lap3d_32": lambda: gen.laplacian_3d(32),
+                     "aniso_24": lambda: gen.aniso7(24, seed=4)}[case]()
+    (b_ai, b_aj, b_av), (ua, uj, f) = setup(lab, n, ai, aj, av)
+    A = lab.CSR(n, n, 0, b_ai, b_aj, b_av, keep_f32=True)
+    b = dev(np.random.default_rng(7).uniform(-1, 1, n))
+    for mixed in (False, True):
+        monkeypatch.setenv("LA_PCG_FUSED", "0")
+        s0 = lab.PCG(A, ua, uj, f, mixed=mixed)
+        monkeypatch.delenv("LA_PCG_FUSED")
+        s1 = lab.PCG(A, ua, uj, f, mixed=mixed)
+        assert not s0.fused() and s1.fused()
+        x0 = torch.empty(n, dtype=torch.float64, device="cuda")
+        x1 = torch.empty_like(x0)
+        r0 = s0.solve(b, x0, rtol=1e-10, maxit=20000)
+        r1 = s1.solve(b, x1, rtol=1e-10, maxit=20000)
+        assert (r0.iterations, r0.outer_iterations) == (r1.iterations, r1.outer_iterations)
+        assert torch.equal(x0, x1), (case, mixed)
+        assert r1.rel_residual == r0.rel_residual
+        print(f"{case} mixed={mixed}: {r1.iterations} it, fused {r1.solve_ms:.2f} ms, "
+              f"unfused {r0.solve_ms:.2f} ms")

@@ -118,7 +118,11 @@ def test_noalloc_spmv_vs_oracle(lab, orc):
                     ref = y0.copy()
                     getattr(orc.port(), f"oracle_{kname}_spmv_tiled")(
                         1024, n, 0, P(ai), P(aj), P(av), P(x), P(ref), alpha, beta)
-                    assert np.array_equal(y, ref), (name, kname, alpha, beta)
+                    # ALBUSSPMV leaves the rows before its first block's start
+                    # row unwritten (spmv.hpp:239-293); the GPU writes beta*y
+                    # there as SerialSPMV does, checked above
+                    lead = int(np.argmax(seg > 0)) if kname == "albus" else 0
+                    assert np.array_equal(y[lead:], ref[lead:]), (name, kname, alpha, beta)
 
 
 def test_noalloc_inconsistent_row_pointers_stay_inside_y(lab):
