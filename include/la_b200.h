@@ -89,6 +89,42 @@ la_status la_csr_update_values(la_csr_t A, const void *av, int on_device);
 la_status la_csr_info(la_csr_t A, int *n, int *ncols, int *nnz, int *base,
                       la_dtype *dtype);
 la_status la_csr_destroy(la_csr_t A);
+/* Host copies of a handle's arrays (ai[n+1], aj[nnz], av[nnz] in its dtype);
+ * any pointer may be NULL to skip that array. */
+la_status la_csr_download(la_csr_t A, int *ai, int *aj, void *av);
+
+/* ---------------------------------------------------------------- ingest */
+/* The on-disk formats either side of the path (utils/utils.h:23-132).
+ *
+ * la_csr_from_coo: a device CSR from HOST coordinate entries (indices carry
+ * `base`: rows[k] - base in [0, nrows), cols[k] - base in [0, ncols)),
+ * ordered by (row, col) on the device -- the construction ReadFromBinaryCSR
+ * (utils.h:46-91) and read_matrix_market_csr (utils.h:93-132) perform on the
+ * host.  Entries with equal (row, col) are kept, in input order. */
+la_status la_csr_from_coo(int nrows, int ncols, long long nnz, int base, const int *rows,
+                          const int *cols, const void *vals, la_dtype dtype, int flags,
+                          la_csr_t *out);
+/* ReadFromBinaryCOO (utils.h:23-44), host only: the file is an int64 entry
+ * count followed by std::tuple<int32 row, int32 col, double value> records
+ * (16 bytes each as libstdc++ lays the tuple out: value, col, row); *m /
+ * *n = largest row / column index + 1 - base, as the reference returns them.
+ * Call with rows == cols == vals == NULL to learn *nnz, then again with
+ * arrays of *nnz entries (entries in file order). */
+la_status la_read_binary_coo(const char *path, int base, long long *nnz, int *rows, int *cols,
+                             double *vals, int *m, int *n);
+/* A Matrix Market coordinate file (real, integer or pattern; general,
+ * symmetric or skew-symmetric), host only, as 0-based entries: symmetric
+ * storage expanded by mirroring every off-diagonal entry (the reference reads
+ * through fast_matrix_market with its symmetry generalisation), pattern
+ * entries valued 1.  Two-call pattern as above. */
+la_status la_read_matrix_market(const char *path, long long *nnz, int *rows, int *cols,
+                                double *vals, int *m, int *n);
+/* ReadFromBinaryCSR (utils.h:46-91) into a device CSR with the file's base,
+ * and read_matrix_market_csr (utils.h:93-132) into a 0-based device CSR
+ * (from a file, or from the text already in memory). */
+la_status la_csr_read_binary_coo(const char *path, int base, int flags, la_csr_t *out);
+la_status la_csr_read_matrix_market(const char *path, int flags, la_csr_t *out);
+la_status la_csr_parse_matrix_market(const char *text, size_t len, int flags, la_csr_t *out);
 
 /* ---------------------------------------------------------------- SpMV */
 /* Plan = the reference's preprocess() (SegSumSPMV::preprocess,

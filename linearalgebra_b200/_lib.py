@@ -53,6 +53,13 @@ _SIGS = {
     "la_csr_create": [I, I, I, P, P, P, I, I, C.POINTER(P)],
     "la_csr_create_device": [I, I, I, I, P, P, P, I, I, C.POINTER(P)],
     "la_csr_update_values": [P, P, I],
+    "la_csr_download": [P, P, P, P],
+    "la_csr_from_coo": [I, I, C.c_longlong, I, P, P, P, I, I, C.POINTER(P)],
+    "la_read_binary_coo": [C.c_char_p, I, C.POINTER(C.c_longlong), P, P, P, IP, IP],
+    "la_read_matrix_market": [C.c_char_p, C.POINTER(C.c_longlong), P, P, P, IP, IP],
+    "la_csr_read_binary_coo": [C.c_char_p, I, I, C.POINTER(P)],
+    "la_csr_read_matrix_market": [C.c_char_p, I, C.POINTER(P)],
+    "la_csr_parse_matrix_market": [C.c_char_p, C.c_size_t, I, C.POINTER(P)],
     "la_csr_info": [P, IP, IP, IP, IP, IP],
     "la_csr_destroy": [P],
     "la_spmv_plan_create": [P, I, C.POINTER(P)],

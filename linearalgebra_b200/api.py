@@ -41,7 +41,8 @@ __all__ = [
     "spmv_transpose", "sddmm_pattern", "ForwardSubstitutionT", "ForwardSubstitution",
     "BackwardSubstitution", "LevelScheduleForwardSubstitution",
     "LevelScheduleBackwardSubstitution", "trsv_partition", "TopologicalSort",
-    "PermuteVec", "InversePermute", "Diagonal", "ILU0",
+    "PermuteVec", "InversePermute", "Diagonal", "ILU0", "csr_from_coo", "ReadFromBinaryCOO",
+    "read_matrix_market_coo", "ReadFromBinaryCSR", "read_matrix_market_csr",
 ]
 
 
@@ -98,6 +99,27 @@ class CSR:
              LA_CSR_KEEP_F32 if keep_f32 else 0, C.byref(h))
         self.h = h
         self.host = (ai, aj, av)
+
+    @classmethod
+    def _adopt(cls, h, keep_host=True):
+        """Wrap a handle the library created (ingest); host arrays downloaded."""
+        self = cls.__new__(cls)
+        self.h = h
+        n, nc, nnz, base, dt = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        call("la_csr_info", h, C.byref(n), C.byref(nc), C.byref(nnz), C.byref(base),
+             C.byref(dt))
+        self.n, self.ncols, self.nnz, self.base = n.value, nc.value, nnz.value, base.value
+        self.dtype = np.dtype(np.float64 if dt.value == LA_F64 else np.float32)
+        self.host = self.download() if keep_host else None
+        return self
+
+    def download(self):
+        """(ai, aj, av) host copies of the device arrays (la_csr_download)."""
+        ai = np.empty(self.n + 1, np.int32)
+        aj = np.empty(self.nnz, np.int32)
+        av = np.empty(self.nnz, self.dtype)
+        call("la_csr_download", self.h, _ptr(ai), _ptr(aj), _ptr(av))
+        return ai, aj, av
 
     def update_values(self, av):
         if _is_device(av):
@@ -203,6 +225,59 @@ class ALBUSSPMV(SegSumSPMV):
     """``ALBUSSPMV`` (spmv.hpp:186-300) on the GPU."""
 
     KIND = LA_SPMV_ALBUS
+
+
+# --------------------------------------------------------------- ingest
+def csr_from_coo(nrows, ncols, base, rows, cols, vals, dtype=np.float64, keep_f32=False):
+    """Device CSR from host COO entries (indices carry `base`), ordered by
+    (row, col) on the device; equal (row, col) entries kept in input order."""
+    rows, cols = _i32(rows), _i32(cols)
+    vals = np.ascontiguousarray(vals, dtype=dtype)
+    h = C.c_void_p()
+    call("la_csr_from_coo", int(nrows), int(ncols), len(rows), int(base), _ptr(rows),
+         _ptr(cols), _ptr(vals), LA_F64 if np.dtype(dtype) == np.float64 else LA_F32,
+         LA_CSR_KEEP_F32 if keep_f32 else 0, C.byref(h))
+    return CSR._adopt(h)
+
+
+def _two_call(fn, *lead):
+    nnz, m, n = C.c_longlong(), C.c_int(), C.c_int()
+    call(fn, *lead, C.byref(nnz), None, None, None, C.byref(m), C.byref(n))
+    rows, cols = np.empty(nnz.value, np.int32), np.empty(nnz.value, np.int32)
+    vals = np.empty(nnz.value, np.float64)
+    call(fn, *lead, C.byref(nnz), _ptr(rows), _ptr(cols), _ptr(vals), C.byref(m), C.byref(n))
+    return m.value, n.value, rows, cols, vals
+
+
+def ReadFromBinaryCOO(filename, base=0):
+    """``utils::ReadFromBinaryCOO`` (utils/utils.h:23-44), host:
+    (rows, cols, vals, (m, n)) in file order."""
+    m, n, r, c, v = _two_call("la_read_binary_coo", str(filename).encode(), int(base))
+    return r, c, v, (m, n)
+
+
+def read_matrix_market_coo(filename):
+    """0-based COO entries of a Matrix Market coordinate file, symmetric
+    storage expanded: (m, n, rows, cols, vals)."""
+    return _two_call("la_read_matrix_market", str(filename).encode())
+
+
+def ReadFromBinaryCSR(filename, base=0, keep_f32=False):
+    """``utils::ReadFromBinaryCSR`` (utils/utils.h:46-91) into a device CSR
+    (the file's base); ``.host`` holds (ai, aj, av)."""
+    h = C.c_void_p()
+    call("la_csr_read_binary_coo", str(filename).encode(), int(base),
+         LA_CSR_KEEP_F32 if keep_f32 else 0, C.byref(h))
+    return CSR._adopt(h)
+
+
+def read_matrix_market_csr(filename, keep_f32=False):
+    """``utils::read_matrix_market_csr`` (utils/utils.h:93-132) into a
+    0-based device CSR; ``.host`` holds (ai, aj, av)."""
+    h = C.c_void_p()
+    call("la_csr_read_matrix_market", str(filename).encode(),
+         LA_CSR_KEEP_F32 if keep_f32 else 0, C.byref(h))
+    return CSR._adopt(h)
 
 
 # ----------------------------------------------------------- triangular

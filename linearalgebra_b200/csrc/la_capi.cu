@@ -120,6 +120,20 @@ using namespace la;
 
 static cudaStream_t S(la_stream_t s) { return static_cast<cudaStream_t>(s); }
 
+namespace la {
+// The optional FP32 copy of an FP64 matrix's values (LA_CSR_KEEP_F32).
+la_status csr_finish(la_csr_t A, int flags) {
+  if ((flags & LA_CSR_KEEP_F32) && A->dtype == LA_F64 && A->nnz > 0) {
+    LA_TRY(A->av32.alloc(sizeof(float) * A->nnz));
+    f64_to_f32_kernel<<<std::min((A->nnz + 255) / 256, 8192), 256>>>(
+        A->nnz, A->av.as<double>(), A->av32.as<float>());
+    LA_CUDA_TRY(cudaGetLastError());
+    LA_CUDA_TRY(cudaDeviceSynchronize());
+  }
+  return LA_OK;
+}
+} // namespace la
+
 extern "C" {
 
 const char *la_last_error_string(void) { return la::get_error(); }
@@ -133,16 +147,6 @@ la_status la_device_sm_count(int *sms) {
 }
 
 // ------------------------------------------------------------------ CSR
-static la_status csr_finish(la_csr_t A, int flags) {
-  if ((flags & LA_CSR_KEEP_F32) && A->dtype == LA_F64 && A->nnz > 0) {
-    LA_TRY(A->av32.alloc(sizeof(float) * A->nnz));
-    f64_to_f32_kernel<<<std::min((A->nnz + 255) / 256, 8192), 256>>>(
-        A->nnz, A->av.as<double>(), A->av32.as<float>());
-    LA_CUDA_TRY(cudaGetLastError());
-    LA_CUDA_TRY(cudaDeviceSynchronize());
-  }
-  return LA_OK;
-}
 
 la_status la_csr_create(int n, int ncols, int base, const int *ai,
                         const int *aj, const void *av, la_dtype dtype,
@@ -233,6 +237,93 @@ la_status la_csr_info(la_csr_t A, int *n, int *ncols, int *nnz, int *base,
 la_status la_csr_destroy(la_csr_t A) {
   delete A;
   return LA_OK;
+}
+
+la_status la_csr_download(la_csr_t A, int *ai, int *aj, void *av) {
+  LA_CHECK_ARG(A, "A is NULL");
+  if (ai)
+    LA_CUDA_TRY(cudaMemcpy(ai, A->ai.p, sizeof(int) * (A->n + 1), cudaMemcpyDeviceToHost));
+  if (aj && A->nnz)
+    LA_CUDA_TRY(cudaMemcpy(aj, A->aj.p, sizeof(int) * A->nnz, cudaMemcpyDeviceToHost));
+  if (av && A->nnz)
+    LA_CUDA_TRY(cudaMemcpy(av, A->av.p, (A->dtype == LA_F64 ? 8 : 4) * (size_t)A->nnz,
+                           cudaMemcpyDeviceToHost));
+  return LA_OK;
+}
+
+// ------------------------------------------------------------------ ingest
+la_status la_csr_from_coo(int nrows, int ncols, long long nnz, int base, const int *rows,
+                          const int *cols, const void *vals, la_dtype dtype, int flags,
+                          la_csr_t *out) {
+  LA_CHECK_ARG(out && nrows >= 0 && ncols >= 0, "arguments");
+  LA_CHECK_ARG(base == 0 || base == 1, "base must be 0 or 1");
+  LA_CHECK_ARG(dtype == LA_F64 || dtype == LA_F32, "dtype");
+  LA_CHECK_ARG(nnz >= 0 && nnz < (1LL << 31), "nnz out of int32 range");
+  LA_CHECK_ARG(nnz == 0 || (rows && cols && vals), "rows/cols/vals NULL with nnz > 0");
+  return csr_from_coo(nrows, ncols, nnz, base, rows, cols, vals, dtype, flags, out);
+}
+
+// Two-call pattern of the host readers: with rows == NULL only the sizes
+// are returned; then arrays of *nnz entries are filled.
+static la_status copy_coo(const std::vector<int> &r, const std::vector<int> &c,
+                          const std::vector<double> &v, long long *nnz, int *rows, int *cols,
+                          double *vals) {
+  if (rows || cols || vals) {
+    LA_CHECK_ARG(rows && cols && vals, "rows/cols/vals: all or none");
+    LA_CHECK_ARG(*nnz >= (long long)r.size(), "arrays shorter than the entry count");
+    std::memcpy(rows, r.data(), sizeof(int) * r.size());
+    std::memcpy(cols, c.data(), sizeof(int) * c.size());
+    std::memcpy(vals, v.data(), sizeof(double) * v.size());
+  }
+  *nnz = (long long)r.size();
+  return LA_OK;
+}
+
+la_status la_read_binary_coo(const char *path, int base, long long *nnz, int *rows, int *cols,
+                             double *vals, int *m, int *n) {
+  LA_CHECK_ARG(path && nnz && m && n && (base == 0 || base == 1), "arguments");
+  std::vector<int> r, c;
+  std::vector<double> v;
+  LA_TRY(read_binary_coo(path, base, r, c, v, m, n));
+  return copy_coo(r, c, v, nnz, rows, cols, vals);
+}
+
+la_status la_read_matrix_market(const char *path, long long *nnz, int *rows, int *cols,
+                                double *vals, int *m, int *n) {
+  LA_CHECK_ARG(path && nnz && m && n, "arguments");
+  std::string text;
+  LA_TRY(read_file(path, text));
+  std::vector<int> r, c;
+  std::vector<double> v;
+  LA_TRY(parse_matrix_market(text.data(), text.size(), r, c, v, m, n));
+  return copy_coo(r, c, v, nnz, rows, cols, vals);
+}
+
+la_status la_csr_read_binary_coo(const char *path, int base, int flags, la_csr_t *out) {
+  LA_CHECK_ARG(path && out && (base == 0 || base == 1), "arguments");
+  std::vector<int> r, c;
+  std::vector<double> v;
+  int m = 0, n = 0;
+  LA_TRY(read_binary_coo(path, base, r, c, v, &m, &n));
+  return csr_from_coo(m, n, (long long)r.size(), base, r.data(), c.data(), v.data(), LA_F64,
+                      flags, out);
+}
+
+la_status la_csr_parse_matrix_market(const char *text, size_t len, int flags, la_csr_t *out) {
+  LA_CHECK_ARG(text && out, "arguments");
+  std::vector<int> r, c;
+  std::vector<double> v;
+  int m = 0, n = 0;
+  LA_TRY(parse_matrix_market(text, len, r, c, v, &m, &n));
+  return csr_from_coo(m, n, (long long)r.size(), 0, r.data(), c.data(), v.data(), LA_F64, flags,
+                      out);
+}
+
+la_status la_csr_read_matrix_market(const char *path, int flags, la_csr_t *out) {
+  LA_CHECK_ARG(path && out, "arguments");
+  std::string text;
+  LA_TRY(read_file(path, text));
+  return la_csr_parse_matrix_market(text.data(), text.size(), flags, out);
 }
 
 // ----------------------------------------------------------------- SpMV

@@ -45,6 +45,20 @@ const char *get_error();
     }                                                                          \
   } while (0)
 
+// Ingest (la_ingest.cu): host readers of the reference's binary COO and of
+// Matrix Market text, and the device build of a CSR from COO entries.
+la_status read_file(const char *path, std::string &buf);
+la_status read_binary_coo(const char *path, int base, std::vector<int> &rows,
+                          std::vector<int> &cols, std::vector<double> &vals, int *m, int *n);
+la_status parse_matrix_market(const char *text, size_t len, std::vector<int> &rows,
+                              std::vector<int> &cols, std::vector<double> &vals, int *m,
+                              int *n);
+la_status csr_from_coo(int nrows, int ncols, long long nnz, int base, const int *rows,
+                       const int *cols, const void *vals, la_dtype dtype, int flags,
+                       la_csr_t *out);
+// The optional FP32 copy of an FP64 matrix's values (LA_CSR_KEEP_F32).
+la_status csr_finish(la_csr_t A, int flags);
+
 // Returns LA_OK if a CUDA device of compute capability 10.x is current.
 la_status require_device();
 int sm_count();
@@ -120,6 +134,7 @@ struct la_spmv_plan_s {
   la::DevBuf part;     // double[2 * ntiles]: head / tail partial sums
   la::DevBuf group_end; // int[ntiles]: end of the merge group a tile starts, else -1
   bool long_rows = true; // some row is longer than the per-thread row sum limit
+  bool vec_tiles = false; // every row is short enough for the 16-byte load layout
   // lazily built transpose for the adjoint
   la_csr_t At = nullptr;
   la_spmv_plan_t Atplan = nullptr;

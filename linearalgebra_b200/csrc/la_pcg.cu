@@ -71,6 +71,31 @@ __device__ __forceinline__ double block_sum(double s, double *red) {
   return t;
 }
 
+// A thread's running sum over its elements i = block * kDotThreads + tid +
+// k * stride, in k order; four elements are loaded before their four
+// multiply-adds, so more loads are in flight and the order is unchanged.
+template <typename XA, typename XB>
+__device__ __forceinline__ double thread_dot(const int n, const XA *__restrict__ a,
+                                             const XB *__restrict__ b) {
+  const int stride = gridDim.x * kDotThreads;
+  int i = blockIdx.x * kDotThreads + threadIdx.x;
+  double s = 0.0;
+  for (; i + 3 * stride < n; i += 4 * stride) {
+    double u[4], v[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      u[k] = double(a[i + k * stride]);
+      v[k] = double(b[i + k * stride]);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      s = __fma_rn(u[k], v[k], s);
+  }
+  for (; i < n; i += stride)
+    s = __fma_rn(double(a[i]), double(b[i]), s);
+  return s;
+}
+
 // The block totals of `partials` (`count` of them) added in block order.
 __device__ __forceinline__ double sum_partials(const double *partials, int count) {
   double t = 0.0;
@@ -85,10 +110,7 @@ __global__ void __launch_bounds__(kDotThreads)
                double *partials, unsigned *ticket, double *scal, const int op) {
   __shared__ double red[kDotThreads / 32];
   __shared__ bool last;
-  double s = 0.0;
-  for (int i = blockIdx.x * kDotThreads + threadIdx.x; i < n;
-       i += gridDim.x * kDotThreads)
-    s = __fma_rn(double(a[i]), double(b[i]), s);
+  const double s = thread_dot(n, a, b);
   const double bt = block_sum(s, red);
   if (threadIdx.x == 0) {
     partials[blockIdx.x] = bt;
@@ -210,9 +232,7 @@ __global__ void __launch_bounds__(kDotThreads)
   __shared__ double alpha_s;
   __shared__ bool last;
   const int stride = gridDim.x * kDotThreads, i0 = blockIdx.x * kDotThreads + threadIdx.x;
-  double s = 0.0;
-  for (int i = i0; i < n; i += stride)
-    s = __fma_rn(double(p[i]), double(q[i]), s);
+  double s = thread_dot(n, p, q);
   const double bt = block_sum(s, red);
   if (threadIdx.x == 0)
     partials[blockIdx.x] = bt;
@@ -230,14 +250,31 @@ __global__ void __launch_bounds__(kDotThreads)
   const double al = alpha_s;
   const X sentinel = AllOnes<X>::v();
   s = 0.0;
-  for (int i = i0; i < n; i += stride) {
-    x[i] = X(__fma_rn(al, double(p[i]), double(x[i])));
-    const X ri = X(__fma_rn(-al, double(q[i]), double(r[i])));
-    r[i] = ri;
-    s = __fma_rn(double(ri), double(ri), s);
+  auto step = [&](int i, X pi, X qi, X xi, X ri) {
+    x[i] = X(__fma_rn(al, double(pi), double(xi)));
+    const X rn = X(__fma_rn(-al, double(qi), double(ri)));
+    r[i] = rn;
+    s = __fma_rn(double(rn), double(rn), s);
     t_fill[i] = sentinel;
     z_fill[i] = sentinel;
+  };
+  int i = i0;
+  for (; i + 3 * stride < n; i += 4 * stride) { // loads first, then the k-order steps
+    X pv[4], qv[4], xv[4], rv[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int j = i + k * stride;
+      pv[k] = p[j];
+      qv[k] = q[j];
+      xv[k] = x[j];
+      rv[k] = r[j];
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      step(i + k * stride, pv[k], qv[k], xv[k], rv[k]);
   }
+  for (; i < n; i += stride)
+    step(i, p[i], q[i], x[i], r[i]);
   const double bt2 = block_sum(s, red);
   if (threadIdx.x == 0) {
     partials[gridDim.x + blockIdx.x] = bt2;
@@ -262,9 +299,7 @@ __global__ void __launch_bounds__(kDotThreads)
   __shared__ double beta_s;
   const int stride = gridDim.x * kDotThreads, i0 = blockIdx.x * kDotThreads + threadIdx.x;
   const double rz_old = scal[S_RZ]; // read before block 0 replaces it
-  double s = 0.0;
-  for (int i = i0; i < n; i += stride)
-    s = __fma_rn(double(r[i]), double(z[i]), s);
+  const double s = thread_dot(n, r, z);
   const double bt = block_sum(s, red);
   if (threadIdx.x == 0)
     partials[blockIdx.x] = bt;
@@ -281,7 +316,19 @@ __global__ void __launch_bounds__(kDotThreads)
   }
   __syncthreads();
   const double be = beta_s;
-  for (int i = i0; i < n; i += stride)
+  int i = i0;
+  for (; i + 3 * stride < n; i += 4 * stride) {
+    X pv[4], zv[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      pv[k] = p[i + k * stride];
+      zv[k] = z[i + k * stride];
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      pn[i + k * stride] = X(__fma_rn(be, double(pv[k]), double(zv[k])));
+  }
+  for (; i < n; i += stride)
     pn[i] = X(__fma_rn(be, double(p[i]), double(z[i])));
 }
 

@@ -55,6 +55,7 @@ constexpr int kRowCap = kTile + 1;       // staged row pointers per tile
 constexpr int kLongRow = 64;             // in-tile segments longer than this
                                          // are summed by a warp
 constexpr int kLongCap = kTile / (kLongRow + 1) + 2;
+constexpr int kVecRow = 8;               // 16-byte loads when no row is longer
 
 enum Form { kSegSum = 0, kAlbus = 1 };
 
@@ -177,11 +178,12 @@ __device__ __forceinline__ void st_vec4(float *p, const float (&v)[kNpt]) {
 // VEC: a full tile's columns and values are read with 16-byte loads, thread
 // tid owning its 4 consecutive nonzeros, instead of one element per 256-wide
 // stride.  Same products, same row sums: the results are bit-identical.  The
-// plan selects it with LONG = false (measured on the 128^3 Laplacian: 44.1
-// against 45.1 us back to back, 52.2 against 56.3 us with L2 flushed); on the
-// power-law matrix, whose rows reach 20000 entries, it measured slower (186.6
-// against 178.1 us), and it needs 16-byte aligned aj / av, which the plan's
-// own copies are.
+// plan selects it when no row has more than kVecRow entries (measured on the
+// 128^3 Laplacian: 44.1 against 45.1 us back to back, 52.2 against 56.3 us
+// with L2 flushed); with the 27-entry rows of the 96^3 stencil's transpose
+// it measured slower (78.8 against 71.3 us), as on the power-law matrix,
+// whose rows reach 20000 entries (186.6 against 178.1 us).  It needs 16-byte
+// aligned aj / av, which the plan's own copies are.
 template <int FORM, typename V, typename X, typename ACC, bool XP = false, bool LONG = true,
           bool CHUNK = false, bool VEC = false>
 __global__ void __launch_bounds__(kThreads, kTileBlocksPerSm)
@@ -436,9 +438,11 @@ la_status launch_form(la_spmv_plan_t P, const V *av, ACC alpha, const X *x,
   // short rows only: 16-byte loads (not with x slices, whose gathers keep
   // the element layout)
   auto tile = chunk ? (P->long_rows ? spmv_tile_kernel<FORM, V, X, ACC, XP, true, true>
-                                    : spmv_tile_kernel<FORM, V, X, ACC, XP, false, true, !XP>)
+                      : P->vec_tiles ? spmv_tile_kernel<FORM, V, X, ACC, XP, false, true, !XP>
+                                     : spmv_tile_kernel<FORM, V, X, ACC, XP, false, true>)
                     : (P->long_rows ? spmv_tile_kernel<FORM, V, X, ACC, XP, true>
-                                    : spmv_tile_kernel<FORM, V, X, ACC, XP, false, false, !XP>);
+                      : P->vec_tiles ? spmv_tile_kernel<FORM, V, X, ACC, XP, false, false, !XP>
+                                     : spmv_tile_kernel<FORM, V, X, ACC, XP, false>);
   if (tile1 < 0)
     tile1 = P->ntiles;
   int f0 = 0;
@@ -592,6 +596,7 @@ la_status spmv_plan_build(la_spmv_plan_t P) {
   for (int r = 0; r < n; r++)
     longest = std::max(longest, ai[r + 1] - ai[r]);
   P->long_rows = longest > kLongRow;
+  P->vec_tiles = longest <= kVecRow;
   LA_TRY(P->part.alloc(sizeof(double) * 2 * ntiles));
   LA_CUDA_TRY(cudaMemset(P->part.p, 0, P->part.bytes));
   return LA_OK;

@@ -90,6 +90,8 @@ _REF_SIGS = {
     "la_ref_icc0": ([I, I, P, P, P, D, P], I),
     "la_ref_serial_cm": ([I, I, P, P, P, P], None),
     "la_ref_pcg_create": ([I, I, I, P, P, P, P, P, P], P),
+    "la_ref_read_binary_coo": ([C.c_char_p, I, P, P, P, P, P], C.c_longlong),
+    "la_ref_read_binary_csr": ([C.c_char_p, I, P, P, P, P, P], C.c_longlong),
     "la_ref_pcg_solve": ([P, P, P, D, I, P], I),
     "la_ref_pcg_destroy": ([P], None),
 }

@@ -19,6 +19,7 @@
 #include "triangle_solve.hpp"
 #include "Reordering.h"
 #include "mkl_sparse_mat.h"
+#include "utils.h"
 
 #include <cmath>
 #include <cstring>
@@ -138,6 +139,44 @@ struct RefTrsv {
   int kind, uplo;
   void *obj;
 };
+
+// ------------------------------------------------------------ file readers
+// utils::ReadFromBinaryCOO (utils/utils.h:23-44).  Returns the entry count;
+// with rows != NULL the entries (file order) and *m / *n are written too.
+long long la_ref_read_binary_coo(const char *path, int base, int *rows, int *cols,
+                                 double *vals, int *m, int *n) {
+  std::vector<int> r, c;
+  std::vector<double> v;
+  auto mn = utils::ReadFromBinaryCOO(path, r, c, v, base);
+  if (rows) {
+    std::memcpy(rows, r.data(), sizeof(int) * r.size());
+    std::memcpy(cols, c.data(), sizeof(int) * c.size());
+    std::memcpy(vals, v.data(), sizeof(double) * v.size());
+  }
+  if (m)
+    *m = mn.first;
+  if (n)
+    *n = mn.second;
+  return (long long)r.size();
+}
+
+// utils::ReadFromBinaryCSR (utils/utils.h:46-91): ai[m + 1], aj / av[nnz].
+long long la_ref_read_binary_csr(const char *path, int base, int *ai, int *aj, double *av,
+                                 int *m, int *n) {
+  std::vector<int> a, j;
+  std::vector<double> v;
+  auto mn = utils::ReadFromBinaryCSR(path, a, j, v, base);
+  if (ai) {
+    std::memcpy(ai, a.data(), sizeof(int) * a.size());
+    std::memcpy(aj, j.data(), sizeof(int) * j.size());
+    std::memcpy(av, v.data(), sizeof(double) * v.size());
+  }
+  if (m)
+    *m = mn.first;
+  if (n)
+    *n = mn.second;
+  return (long long)j.size();
+}
 
 } // extern "C"
 

@@ -145,6 +145,24 @@ def main():
             assert ok
             out[f"{nm}/u_ai"], out[f"{nm}/u_aj"], out[f"{nm}/u_av"] = ua, uj, uv
             out[f"{nm}/icc0"] = f
+    # binary COO ingest: the reference's own data/shared/*.bin files (raw
+    # bytes) and what its ReadFromBinaryCSR (utils/utils.h:46-91) builds from
+    # them, with the files' base 1 and read as base 0
+    for nm in ("K", "M", "G", "G2"):
+        path = REF / "data" / "shared" / f"{nm}.bin"
+        out[f"bin_{nm}/bytes"] = np.frombuffer(path.read_bytes(), np.uint8).copy()
+        for base in (1, 0):
+            m, n = np.zeros(1, np.int32), np.zeros(1, np.int32)
+            cnt = rf.la_ref_read_binary_csr(str(path).encode(), base, None, None, None,
+                                            ptr(m), ptr(n))
+            ai = np.zeros(int(m[0]) + 1, np.int32)
+            aj = np.zeros(cnt, np.int32)
+            av = np.zeros(cnt)
+            rf.la_ref_read_binary_csr(str(path).encode(), base, ptr(ai), ptr(aj), ptr(av),
+                                      ptr(m), ptr(n))
+            key = f"bin_{nm}/base{base}"
+            out[f"{key}_ai"], out[f"{key}_aj"], out[f"{key}_av"] = ai, aj, av
+            out[f"{key}_shape"] = np.array([int(m[0]), int(n[0])])
     np.savez_compressed(OUT, **out)
     print(f"wrote {OUT} ({OUT.stat().st_size} bytes, {len(out)} arrays)")
 
