@@ -59,6 +59,7 @@ typedef struct la_csr_s *la_csr_t;
 typedef struct la_spmv_plan_s *la_spmv_plan_t;
 typedef struct la_trsv_plan_s *la_trsv_plan_t;
 typedef struct la_pcg_s *la_pcg_t;
+typedef struct la_factor_plan_s *la_factor_plan_t;
 typedef void *la_stream_t; /* a cudaStream_t; NULL is the legacy stream */
 
 /* ---------------------------------------------------------------- misc */
@@ -222,6 +223,14 @@ la_status la_topological_sort(la_uplo uplo, int n, int base, const int *ai, cons
 la_status la_topological_sort2(la_uplo uplo, int n, int base, const int *ai,
                                const int *aj, int *iperm, int *prefix,
                                int *levels);
+/* The same level sets computed on the GPU (no reference counterpart beyond
+ * TopologicalSort2 itself): the depths as a (max, +) triangular solve in one
+ * persistent launch, the rows ordered by a stable radix sort on their depth.
+ * Host arrays in and out, outputs identical to la_topological_sort2.  The
+ * triangle must be strict (LA_ERR_INVALID_ARG otherwise).  The triangular
+ * solve analysis uses it for triangles of at least 65,536 rows. */
+la_status la_topological_sort2_device(la_uplo uplo, int n, int base, const int *ai,
+                                      const int *aj, int *iperm, int *prefix, int *levels);
 /* SerialCM reverse Cuthill-McKee (reordering/Reordering.cpp:37-136),
  * bit-identical iperm/perm (values carry the base). */
 la_status la_rcm(int n, int base, const int *ai, const int *aj, int *iperm,
@@ -286,6 +295,36 @@ la_status la_icc0(int n, int base, const int *u_ai, const int *u_aj,
 la_status la_icc0_shifted(int n, int base, const int *u_ai, const int *u_aj,
                           const double *u_av, double *icc_av,
                           double *shift_used);
+
+/* The same factorisations on the GPU: a symbolic plan built once per
+ * pattern on the host (the sequential algorithm replayed on the pattern,
+ * recording every row's updates in their order), then numeric passes on the
+ * device, one persistent launch each, level-scheduled by the rows'
+ * dependencies -- bit-identical to la_icc0 / la_ilu0 (same operations, same
+ * order).  For a pattern factored more than once (new values, shift
+ * retries) the numeric pass replaces the host's.
+ * la_icc0_plan_create: u_ai/u_aj as la_icc0 takes them (ICCLevelNumeric,
+ * precond.hpp:615-693).  la_ilu0_plan_create: a full pattern, every row
+ * holding its diagonal, as la_ilu0 takes it.  HOST arrays. */
+la_status la_icc0_plan_create(int n, int base, const int *u_ai, const int *u_aj,
+                              la_factor_plan_t *out);
+la_status la_ilu0_plan_create(int n, int base, const int *ai, const int *aj,
+                              la_factor_plan_t *out);
+/* Numeric pass: values av in (the plan's pattern order), the factor out (same
+ * pattern); both host arrays when on_device == 0, device arrays otherwise
+ * (synchronises `stream`).  omega shifts IC(0)'s diagonal by (1 + omega)
+ * (ignored for ILU(0)).  LA_ERR_BREAKDOWN on a negative IC(0) pivot or a zero
+ * ILU(0) pivot, with *bad_row (if non-NULL) the smallest such row -- where
+ * the sequential algorithm stops; -1 otherwise. */
+la_status la_factor_numeric(la_factor_plan_t plan, const double *av, double omega,
+                            double *out, int on_device, int *bad_row, la_stream_t stream);
+/* la_icc0_shifted's retry loop (incomplete_cholesky.cpp:315-342) over device
+ * numeric passes. */
+la_status la_factor_icc0_shifted(la_factor_plan_t plan, const double *av, double *out,
+                                 int on_device, double *shift_used, la_stream_t stream);
+/* Number of dependency levels of the plan's rows. */
+la_status la_factor_levels(la_factor_plan_t plan, int *levels);
+la_status la_factor_plan_destroy(la_factor_plan_t plan);
 
 /* ------------------------------------------------- triangular solves */
 /* OptimizedTriangularSolve<Barrier, L|U>::analysis (triangle_solve.hpp:

@@ -101,6 +101,13 @@ _SIGS = {
     "la_pcg_solve_host": [P, P, P, D, I, C.POINTER(PcgInfo)],
     "la_pcg_adjoint": [P, P, P, P, P, D, I, C.POINTER(PcgInfo), P],
     "la_pcg_fused": [P, IP],
+    "la_topological_sort2_device": [I, I, I, P, P, P, P, IP],
+    "la_icc0_plan_create": [I, I, P, P, C.POINTER(P)],
+    "la_ilu0_plan_create": [I, I, P, P, C.POINTER(P)],
+    "la_factor_numeric": [P, P, D, P, I, IP, P],
+    "la_factor_icc0_shifted": [P, P, P, I, C.POINTER(D), P],
+    "la_factor_levels": [P, IP],
+    "la_factor_plan_destroy": [P],
     "la_pcg_destroy": [P],
 }
 _RESTYPES = {"la_last_error_string": C.c_char_p, "la_version": C.c_char_p}

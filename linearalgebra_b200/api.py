@@ -42,7 +42,7 @@ __all__ = [
     "BackwardSubstitution", "LevelScheduleForwardSubstitution",
     "LevelScheduleBackwardSubstitution", "trsv_partition", "TopologicalSort",
     "PermuteVec", "InversePermute", "Diagonal", "ILU0", "csr_from_coo", "ReadFromBinaryCOO",
-    "read_matrix_market_coo", "ReadFromBinaryCSR", "read_matrix_market_csr",
+    "read_matrix_market_coo", "ReadFromBinaryCSR", "read_matrix_market_csr", "FactorPlan",
 ]
 
 
@@ -225,6 +225,59 @@ class ALBUSSPMV(SegSumSPMV):
     """``ALBUSSPMV`` (spmv.hpp:186-300) on the GPU."""
 
     KIND = LA_SPMV_ALBUS
+
+
+# ------------------------------------------------- device factorisation
+class FactorPlan:
+    """IC(0) or ILU(0) on the GPU, bit-identical to ``ICCLevelNumeric0`` /
+    ``ILU0``: the pattern is analysed once (``kind`` "ic0": u_ai/u_aj the
+    upper triangle with diagonals first; "ilu0": a full pattern), then
+    ``factor`` runs numeric passes on the device."""
+
+    def __init__(self, kind, n, base, ai, aj):
+        ai, aj = _i32(ai), _i32(aj)
+        self.kind, self.n, self.nnz = kind, int(n), int(ai[n] - base)
+        h = C.c_void_p()
+        fn = {"ic0": "la_icc0_plan_create", "ilu0": "la_ilu0_plan_create"}[kind]
+        call(fn, int(n), int(base), _ptr(ai), _ptr(aj), C.byref(h))
+        self.h = h
+
+    def factor(self, av, omega=0.0, out=None):
+        """The factor of values av (host array -> numpy result; CUDA tensor
+        -> written into `out`, a CUDA tensor).  LAError LA_ERR_BREAKDOWN on
+        a negative IC / zero ILU pivot; its ``bad_row`` is the first such
+        row."""
+        bad = C.c_int(-1)
+        if _is_device(av):
+            st = call("la_factor_numeric", self.h, _ptr(av), float(omega), _ptr(out), 1,
+                      C.byref(bad), _stream(av), ok=(0, 5))
+            res = out
+        else:
+            av = _f64(av)
+            res = np.empty(self.nnz)
+            st = call("la_factor_numeric", self.h, _ptr(av), float(omega), _ptr(res), 0,
+                      C.byref(bad), None, ok=(0, 5))
+        if st == 5:
+            e = LAError(st, "la_factor_numeric", _lib.last_error())
+            e.bad_row = bad.value
+            raise e
+        return res
+
+    def shifted(self, av):
+        """IC(0) with the reference's shift retries: (factor, shift used)."""
+        av = _f64(av)
+        res = np.empty(self.nnz)
+        sh = C.c_double()
+        call("la_factor_icc0_shifted", self.h, _ptr(av), _ptr(res), 0, C.byref(sh), None)
+        return res, sh.value
+
+    def levels(self):
+        lv = C.c_int()
+        call("la_factor_levels", self.h, C.byref(lv))
+        return lv.value
+
+    def __del__(self):
+        _release("la_factor_plan_destroy", self)
 
 
 # --------------------------------------------------------------- ingest
@@ -439,13 +492,16 @@ def TopologicalSort(uplo, nodes, base, ai, aj):
     return r.value, iperm[:nodes], prefix[: r.value + 2].copy()
 
 
-def TopologicalSort2(uplo, nodes, base, ai, aj):
-    """Level sets (matrix_utils.hpp:637-675): returns (levels, iperm, prefix)."""
+def TopologicalSort2(uplo, nodes, base, ai, aj, device=False):
+    """Level sets (matrix_utils.hpp:637-675): returns (levels, iperm, prefix);
+    ``device=True`` computes them on the GPU (la_topological_sort2_device,
+    same outputs; strict triangles only)."""
     ai, aj = _i32(ai), _i32(aj)
     iperm = np.empty(nodes, np.int32)
     prefix = np.empty(nodes + 1, np.int32)
     lv = C.c_int()
-    call("la_topological_sort2", LA_LOWER if uplo in ("L", 0) else LA_UPPER,
+    call("la_topological_sort2_device" if device else "la_topological_sort2",
+         LA_LOWER if uplo in ("L", 0) else LA_UPPER,
          int(nodes), int(base), _ptr(ai), _ptr(aj), _ptr(iperm), _ptr(prefix),
          C.byref(lv))
     return lv.value, iperm, prefix[: lv.value + 1].copy()

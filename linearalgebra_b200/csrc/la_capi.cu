@@ -448,6 +448,20 @@ la_status la_topological_sort2(la_uplo uplo, int n, int base, const int *ai,
   return LA_OK;
 }
 
+la_status la_topological_sort2_device(la_uplo uplo, int n, int base, const int *ai,
+                                      const int *aj, int *iperm, int *prefix, int *levels) {
+  LA_CHECK_ARG(ai && iperm && prefix && levels && n >= 0, "arguments");
+  LA_CHECK_ARG(base == 0 || base == 1, "base must be 0 or 1");
+  LA_CHECK_ARG(n == 0 || ai[n] - base == 0 || aj, "aj");
+  if (n == 0) {
+    *levels = 0;
+    prefix[0] = 0;
+    return LA_OK;
+  }
+  LA_TRY(require_device());
+  return topological_sort2_device(uplo, n, base, ai, aj, iperm, prefix, levels);
+}
+
 la_status la_topological_sort(la_uplo uplo, int n, int base, const int *ai, const int *aj,
                               int *iperm, int *prefix, int *result) {
   LA_CHECK_ARG(ai && iperm && prefix && result && n >= 0, "arguments");
@@ -611,6 +625,71 @@ la_status la_icc0_shifted(int n, int base, const int *u_ai, const int *u_aj,
       return s;
     shift = std::max(2 * shift, 1e-3); // _initial_shift (incomplete_cholesky.h:27)
   }
+}
+
+// ------------------------------------------------ device factorisation
+la_status la_icc0_plan_create(int n, int base, const int *u_ai, const int *u_aj,
+                              la_factor_plan_t *out) {
+  LA_CHECK_ARG(u_ai && out && n >= 0 && (base == 0 || base == 1), "arguments");
+  LA_CHECK_ARG(u_ai[n] - base == 0 || u_aj, "u_aj");
+  for (int i = 0; i < n; i++)
+    if (u_ai[i + 1] == u_ai[i] || u_aj[u_ai[i] - base] - base != i) {
+      set_error("IC(0): row %d of the upper triangle does not start with its diagonal", i);
+      return LA_ERR_INVALID_ARG;
+    }
+  LA_TRY(require_device());
+  return factor_plan_create(0, n, base, u_ai, u_aj, out);
+}
+
+la_status la_ilu0_plan_create(int n, int base, const int *ai, const int *aj,
+                              la_factor_plan_t *out) {
+  LA_CHECK_ARG(ai && out && n >= 0 && (base == 0 || base == 1), "arguments");
+  std::string why;
+  if (!valid_csr(n, n, base, ai, aj, &why)) {
+    set_error("invalid CSR: %s", why.c_str());
+    return LA_ERR_BAD_CSR;
+  }
+  LA_TRY(require_device());
+  return factor_plan_create(1, n, base, ai, aj, out);
+}
+
+la_status la_factor_numeric(la_factor_plan_t plan, const double *av, double omega,
+                            double *out, int on_device, int *bad_row, la_stream_t stream) {
+  LA_CHECK_ARG(plan && (plan->nnz == 0 || (av && out)), "arguments");
+  int bad = -1;
+  const la_status s = factor_numeric(plan, av, omega, out, on_device != 0, &bad, S(stream));
+  if (bad_row)
+    *bad_row = bad;
+  return s;
+}
+
+la_status la_factor_icc0_shifted(la_factor_plan_t plan, const double *av, double *out,
+                                 int on_device, double *shift_used, la_stream_t stream) {
+  LA_CHECK_ARG(plan && plan->kind == 0, "an IC(0) plan");
+  double shift = 0.0;
+  for (int restart = 0;; restart++) {
+    int bad = -1;
+    const la_status s = factor_numeric(plan, av, shift, out, on_device != 0, &bad, S(stream));
+    if (s != LA_ERR_BREAKDOWN) {
+      if (shift_used)
+        *shift_used = shift;
+      return s;
+    }
+    if (restart + 1 > 20) // _nrestart (incomplete_cholesky.h:28)
+      return s;
+    shift = std::max(2 * shift, 1e-3); // _initial_shift (incomplete_cholesky.h:27)
+  }
+}
+
+la_status la_factor_levels(la_factor_plan_t plan, int *levels) {
+  LA_CHECK_ARG(plan && levels, "arguments");
+  *levels = plan->levels;
+  return LA_OK;
+}
+
+la_status la_factor_plan_destroy(la_factor_plan_t plan) {
+  delete plan;
+  return LA_OK;
 }
 
 // ------------------------------------------------------------------ trsv

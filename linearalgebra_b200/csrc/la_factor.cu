@@ -1,0 +1,387 @@
+// la_factor.cu -- IC(0) and ILU(0) numeric factorisation on the GPU.
+//
+// Reference: ICCLevel0SymSymbolic + ICCLevelNumeric (sparse_mat_op/
+// precond.hpp:13-37, 615-693), the up-looking IC(0) whose factor U (the
+// upper triangle of A, diagonal first in each row) gives A ~= U^T U, with
+// the shift-retry loop of incomplete_cholesky_k_2 (mkl_wrapper/
+// incomplete_cholesky.cpp:286-342); and ILU(0) on A's own pattern in IKJ
+// order (the reference factors ILU through MKL, incomplete_lu.cpp:277-325;
+// the host restatement here is la_host.cpp's ilu0).
+//
+// B200 design.  The factorisation is split into a symbolic plan, built once
+// per pattern on the host, and a numeric pass on the GPU that can run many
+// times (new values, or the shift retries after a breakdown):
+//  * symbolic: the host replays the sequential algorithm on the pattern
+//    alone and records, for every row j, the ordered list of updates it
+//    receives -- for IC(0) the rows k with U_kj != 0 in the order the
+//    up-looking algorithm's linked lists deliver them, for ILU(0) the stored
+//    k < j in ascending order -- and, for each update, the (target entry of
+//    row j, source entry of row k) pairs it subtracts.  Row j depends exactly
+//    on the rows of its updates, so their level sets (by longest path, as
+//    TopologicalSort2 computes them) order the rows for the device;
+//  * numeric: one persistent launch; warps claim 32-row chunks in level
+//    order from an atomic ticket, one lane per row.  A lane copies its row's
+//    values, waits (bounded by the global timer) for each update's source row
+//    to be published, applies the update's products with exact, never fused
+//    multiplies and subtractions in the recorded order, finishes its row
+//    (IC: pivot check, square root, row division; ILU: zero-pivot check) and
+//    publishes it.  Every value is produced by the same operations in the
+//    same order as the host algorithm: the factor is bit-identical to it.
+//    Because a chunk is claimed only after every earlier chunk, the lowest
+//    unfinished row always has its inputs, and the pass cannot deadlock.
+// A breakdown (IC: negative pivot; ILU: zero pivot) is reported as the
+// smallest such row -- the row where the sequential algorithm stops, since
+// no earlier row depends on a later one.
+//
+// Roofline: latency-bound (levels x one dependency round trip through L2);
+// bytes per factorisation: nnz * 8 (values in) + nnz * 8 (factor out) +
+// the update and pair lists (4 bytes per index).
+
+#include "la_device.cuh"
+#include "la_internal.h"
+
+#include <algorithm>
+#include <cmath>
+#include <memory>
+#include <vector>
+
+namespace la {
+namespace {
+
+constexpr int kFactorThreads = 256;
+constexpr int kFactorChunk = 32;
+constexpr unsigned long long kFactorWaitNs = 1000000000ull; // 1 s
+
+enum FactorKind { kIC0 = 0, kILU0 = 1 };
+
+} // namespace
+} // namespace la
+
+
+namespace la {
+namespace {
+
+// The pattern's update lists.  IC(0): la_host.cpp's icc0 (the reference's
+// ICCLevelNumeric order) replayed without arithmetic.  ILU(0): ilu0's IKJ
+// loop replayed likewise.
+struct Symbolic {
+  std::vector<int> uptr, uk, us, upiv, pptr, ptgt, psrc, diag;
+};
+
+void symbolic_ic0(int n, int base, const int *ai, const int *aj, Symbolic &S) {
+  constexpr int kEnd = 0x7fffffff;
+  std::vector<int> next(n, kEnd), cursor(n, 0);
+  S.uptr.assign(n + 1, 0);
+  S.pptr.assign(1, 0);
+  S.diag.resize(n);
+  for (int j = 0; j < n; j++) {
+    const int rs = ai[j] - base, re = ai[j + 1] - base;
+    S.diag[j] = rs;
+    for (int k = next[j]; k < j;) {
+      const int ck0 = cursor[k]++;
+      const int ke = ai[k + 1] - base;
+      const int after = next[k];
+      if (ck0 + 1 < ke) {
+        const int c = aj[ck0 + 1] - base;
+        next[k] = next[c];
+        next[c] = k;
+      }
+      S.uk.push_back(k);
+      S.us.push_back(ck0);
+      S.upiv.push_back(0);
+      for (int p = rs, ck = ck0; ck < ke && p < re;) {
+        if (aj[ck] == aj[p]) {
+          S.ptgt.push_back(p++);
+          S.psrc.push_back(ck++);
+        } else if (aj[ck] < aj[p]) {
+          ck++;
+        } else {
+          p++;
+        }
+      }
+      S.pptr.push_back((int)S.ptgt.size());
+      k = after;
+    }
+    if (re - rs > 1) {
+      const int c = aj[rs + 1] - base;
+      next[j] = next[c];
+      next[c] = j;
+      cursor[j] = rs + 1;
+    }
+    S.uptr[j + 1] = (int)S.uk.size();
+  }
+}
+
+void symbolic_ilu0(int n, int base, const int *ai, const int *aj, const std::vector<int> &diag,
+                   Symbolic &S) {
+  std::vector<int> where(n, -1);
+  S.uptr.assign(n + 1, 0);
+  S.pptr.assign(1, 0);
+  S.diag = diag;
+  for (int i = 0; i < n; i++) {
+    const int r0 = ai[i] - base, r1 = ai[i + 1] - base;
+    for (int k = r0; k < r1; k++)
+      where[aj[k] - base] = k;
+    for (int k = r0; k < diag[i]; k++) {
+      const int c = aj[k] - base;
+      S.uk.push_back(c);
+      S.us.push_back(k);
+      S.upiv.push_back(diag[c]);
+      for (int m = diag[c] + 1; m < ai[c + 1] - base; m++) {
+        const int w = where[aj[m] - base];
+        if (w >= 0) {
+          S.ptgt.push_back(w);
+          S.psrc.push_back(m);
+        }
+      }
+      S.pptr.push_back((int)S.ptgt.size());
+    }
+    for (int k = r0; k < r1; k++)
+      where[aj[k] - base] = -1;
+    S.uptr[i + 1] = (int)S.uk.size();
+  }
+}
+
+} // namespace
+} // namespace la
+
+namespace la {
+namespace {
+
+__device__ __forceinline__ unsigned long long factor_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ int ld_acquire(const int *p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_release(int *p, int v) {
+  asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// state[0]: chunk ticket, state[1]: a wait gave up, state[2]: smallest row
+// whose pivot broke down (INT_MAX if none).
+template <int KIND>
+__global__ void __launch_bounds__(kFactorThreads)
+    factor_kernel(const int nchunks, const int *__restrict__ chunk_start,
+                  const int *__restrict__ exec_row, const int *__restrict__ rs_of,
+                  const int *__restrict__ diag_of, const int *__restrict__ uptr,
+                  const int *__restrict__ uk, const int *__restrict__ us,
+                  const int *__restrict__ upiv, const int *__restrict__ pptr,
+                  const int *__restrict__ ptgt, const int *__restrict__ psrc,
+                  const double *__restrict__ vin, double *v, const double diag_scale, int *done,
+                  int *state) {
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    // lane 0 alone decides (a wait gave up somewhere: stop) and broadcasts,
+    // so the whole warp leaves together; no lane ever returns on its own
+    int c = 0;
+    if (lane == 0)
+      c = ld_acquire(state + 1) != 0 ? nchunks : atomicAdd(state, 1);
+    c = __shfl_sync(0xffffffffu, c, 0);
+    if (c >= nchunks)
+      return;
+    const int p = __ldg(chunk_start + c) + lane;
+    if (p >= __ldg(chunk_start + c + 1))
+      continue;
+    const int j = __ldg(exec_row + p);
+    const int rs = __ldg(rs_of + j), re = __ldg(rs_of + j + 1);
+    for (int q = rs; q < re; q++)
+      v[q] = __ldg(vin + q);
+    if (KIND == kIC0)
+      v[rs] = __dmul_rn(__ldg(vin + rs), diag_scale); // the (1 + omega) shift
+    bool gave_up = false;
+    for (int u = __ldg(uptr + j); u < __ldg(uptr + j + 1) && !gave_up; u++) {
+      const int k = __ldg(uk + u);
+      const unsigned long long t0 = factor_ns();
+      for (unsigned pass = 1; ld_acquire(done + k) == 0; pass++)
+        if ((pass & 63u) == 0u &&
+            (ld_acquire(state + 1) != 0 || factor_ns() - t0 > kFactorWaitNs)) {
+          atomicExch(state + 1, 1);
+          gave_up = true;
+          break;
+        }
+      if (gave_up)
+        break;
+      double s;
+      if (KIND == kIC0) {
+        s = __ldcg(v + __ldg(us + u)); // U_kj, final
+      } else {
+        const int own = __ldg(us + u); // L_jk = a_jk / u_kk
+        s = __ddiv_rn(v[own], __ldcg(v + __ldg(upiv + u)));
+        v[own] = s;
+      }
+      for (int e = __ldg(pptr + u); e < __ldg(pptr + u + 1); e++) {
+        const int t = __ldg(ptgt + e);
+        v[t] = __dsub_rn(v[t], __dmul_rn(s, __ldcg(v + __ldg(psrc + e))));
+      }
+    }
+    if (gave_up) // the row stays unpublished; the warp stops at its next claim
+      continue;
+    if (KIND == kIC0) {
+      if (v[rs] < 0.0)
+        atomicMin(state + 2, j);
+      const double piv = __dsqrt_rn(v[rs]);
+      v[rs] = piv;
+      for (int q = rs + 1; q < re; q++)
+        v[q] = __ddiv_rn(v[q], piv);
+    } else if (v[__ldg(diag_of + j)] == 0.0) {
+      atomicMin(state + 2, j);
+    }
+    __threadfence();
+    st_release(done + j, 1);
+  }
+}
+
+// level of every row (longest path over its updates' source rows, which all
+// precede it), rows sorted by (level, row), 32-row chunks inside levels
+void schedule(int n, const Symbolic &S, std::vector<int> &erow, std::vector<int> &cstart,
+              int *levels) {
+  std::vector<int> lvl(n, 0);
+  int top = 0;
+  for (int j = 0; j < n; j++) {
+    int l = 0;
+    for (int u = S.uptr[j]; u < S.uptr[j + 1]; u++)
+      l = std::max(l, lvl[S.uk[u]] + 1);
+    lvl[j] = l;
+    top = std::max(top, l + 1);
+  }
+  *levels = n ? top : 0;
+  std::vector<int> start(top + 1, 0);
+  for (int j = 0; j < n; j++)
+    start[lvl[j] + 1]++;
+  for (int l = 0; l < top; l++)
+    start[l + 1] += start[l];
+  erow.resize(n);
+  std::vector<int> fill(start.begin(), start.end() - 1);
+  for (int j = 0; j < n; j++)
+    erow[fill[lvl[j]]++] = j;
+  cstart.clear();
+  for (int l = 0; l < top; l++)
+    for (int p = start[l]; p < start[l + 1]; p += kFactorChunk)
+      cstart.push_back(p);
+  cstart.push_back(n);
+}
+
+la_status plan_build(la_factor_plan_s *P, const int *ai, const int *aj, Symbolic &S) {
+  const int n = P->n;
+  std::vector<int> erow, cstart;
+  schedule(n, S, erow, cstart, &P->levels);
+  P->nchunks = (int)cstart.size() - 1;
+  std::vector<int> rs(n + 1);
+  for (int j = 0; j <= n; j++)
+    rs[j] = ai[j] - P->base;
+  auto up = [](DevBuf &b, const std::vector<int> &v) {
+    return b.upload(v.empty() ? nullptr : v.data(), sizeof(int) * std::max<size_t>(v.size(), 1));
+  };
+  // empty lists still get a (1-entry) buffer so every pointer is valid
+  for (std::vector<int> *v : {&S.uk, &S.us, &S.upiv, &S.ptgt, &S.psrc})
+    if (v->empty())
+      v->push_back(0);
+  LA_TRY(up(P->rs, rs));
+  LA_TRY(up(P->diag, S.diag.empty() ? std::vector<int>{0} : S.diag));
+  LA_TRY(up(P->exec_row, erow.empty() ? std::vector<int>{0} : erow));
+  LA_TRY(up(P->chunk_start, cstart));
+  LA_TRY(up(P->uptr, S.uptr));
+  LA_TRY(up(P->uk, S.uk));
+  LA_TRY(up(P->us, S.us));
+  LA_TRY(up(P->upiv, S.upiv));
+  LA_TRY(up(P->pptr, S.pptr));
+  LA_TRY(up(P->ptgt, S.ptgt));
+  LA_TRY(up(P->psrc, S.psrc));
+  LA_TRY(P->vin.alloc(sizeof(double) * std::max(P->nnz, 1)));
+  LA_TRY(P->done.alloc(sizeof(int) * std::max(n, 1)));
+  LA_TRY(P->state.alloc(sizeof(int) * 4));
+  int per_sm = 0;
+  LA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm, (const void *)factor_kernel<kIC0>, kFactorThreads, 0));
+  const int need = (P->nchunks + kFactorThreads / 32 - 1) / (kFactorThreads / 32);
+  P->grid = std::max(1, std::min(std::max(per_sm, 1) * sm_count(), need));
+  return LA_OK;
+}
+
+} // namespace
+
+// Values in (host or device), factor out (host or device), on `st`;
+// synchronises st.  *bad_row: the smallest row that broke down, or -1.
+la_status factor_numeric(la_factor_plan_s *P, const double *av, double omega, double *out,
+                         bool on_device, int *bad_row, cudaStream_t st) {
+  *bad_row = -1;
+  if (P->n == 0)
+    return LA_OK;
+  const size_t bytes = sizeof(double) * P->nnz;
+  DevBuf tmp;
+  double *v = out;
+  if (!on_device) {
+    LA_TRY(tmp.alloc(std::max<size_t>(bytes, 8)));
+    v = tmp.as<double>();
+  }
+  if (bytes)
+    LA_CUDA_TRY(cudaMemcpyAsync(P->vin.p, av, bytes,
+                                on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                st));
+  const int init[4] = {0, 0, 0x7fffffff, 0};
+  LA_CUDA_TRY(cudaMemcpyAsync(P->state.p, init, sizeof(init), cudaMemcpyHostToDevice, st));
+  LA_CUDA_TRY(cudaMemsetAsync(P->done.p, 0, sizeof(int) * P->n, st));
+  auto launch = P->kind == kIC0 ? factor_kernel<kIC0> : factor_kernel<kILU0>;
+  launch<<<P->grid, kFactorThreads, 0, st>>>(
+      P->nchunks, P->chunk_start.as<int>(), P->exec_row.as<int>(), P->rs.as<int>(),
+      P->diag.as<int>(), P->uptr.as<int>(), P->uk.as<int>(), P->us.as<int>(), P->upiv.as<int>(),
+      P->pptr.as<int>(), P->ptgt.as<int>(), P->psrc.as<int>(), P->vin.as<double>(), v,
+      1.0 + omega, P->done.as<int>(), P->state.as<int>());
+  LA_CUDA_TRY(cudaGetLastError());
+  int state[4];
+  LA_CUDA_TRY(cudaMemcpyAsync(state, P->state.p, sizeof(state), cudaMemcpyDeviceToHost, st));
+  if (!on_device && bytes)
+    LA_CUDA_TRY(cudaMemcpyAsync(out, v, bytes, cudaMemcpyDeviceToHost, st));
+  LA_CUDA_TRY(cudaStreamSynchronize(st));
+  if (state[1]) {
+    set_error("numeric factorisation: a dependency wait exceeded its 1 s bound");
+    return LA_ERR_TIMEOUT;
+  }
+  if (state[2] != 0x7fffffff) {
+    *bad_row = state[2];
+    set_error(P->kind == kIC0 ? "IC(0) breakdown: negative pivot in row %d (omega = %g)"
+                              : "ILU(0): zero pivot in row %d",
+              state[2], omega);
+    return LA_ERR_BREAKDOWN;
+  }
+  return LA_OK;
+}
+
+la_status factor_plan_create(int kind, int n, int base, const int *ai, const int *aj,
+                             la_factor_plan_t *out) {
+  std::unique_ptr<la_factor_plan_s> P(new la_factor_plan_s());
+  P->kind = kind;
+  P->n = n;
+  P->base = base;
+  P->nnz = ai[n] - base;
+  P->h_ai.assign(ai, ai + n + 1);
+  Symbolic S;
+  if (kind == kIC0) {
+    symbolic_ic0(n, base, ai, aj, S);
+  } else {
+    std::vector<int> diag(n);
+    for (int i = 0; i < n; i++) {
+      const int *lo = aj + ai[i] - base, *hi = aj + ai[i + 1] - base;
+      const int *at = std::lower_bound(lo, hi, i + base);
+      if (at == hi || *at != i + base) {
+        set_error("ILU(0): row %d has no diagonal entry", i);
+        return LA_ERR_INVALID_ARG;
+      }
+      diag[i] = (int)(at - aj);
+    }
+    symbolic_ilu0(n, base, ai, aj, diag, S);
+  }
+  if (n)
+    LA_TRY(plan_build(P.get(), ai, aj, S));
+  *out = P.release();
+  return LA_OK;
+}
+
+} // namespace la

@@ -231,6 +231,45 @@ int bits_for(unsigned range) { // bits to hold 0 .. range - 1
 
 } // namespace
 
+// Stable LSD radix sort of n entries by (hi, lo), hi major: lo digits first,
+// then hi digits, 8 bits per pass, as many passes as [0, hi_range) and
+// [0, lo_range) need; pos travels with the keys.  Buffers [cur] hold the
+// input; on return *cur names the buffers holding the result.
+la_status radix_sort_pairs(int n, unsigned hi_range, unsigned lo_range, DevBuf (&kh)[2],
+                           DevBuf (&kl)[2], DevBuf (&kp)[2], int *cur, cudaStream_t st) {
+  if (n <= 1)
+    return LA_OK;
+  const int nb = (n + kSortTile - 1) / kSortTile;
+  DevBuf table;
+  LA_TRY(table.alloc(sizeof(int) * (size_t)kRadix * nb));
+  const int lpass = (bits_for(lo_range) + 7) / 8, hpass = (bits_for(hi_range) + 7) / 8;
+  int c = *cur;
+  for (int pass = 0; pass < lpass + hpass; pass++) {
+    const bool on_lo = pass < lpass;
+    const int shift = 8 * (on_lo ? pass : pass - lpass);
+    const unsigned *key = on_lo ? kl[c].as<unsigned>() : kh[c].as<unsigned>();
+    radix_hist_kernel<<<nb, kSortThreads, 0, st>>>(n, key, shift, table.as<int>());
+    LA_CUDA_TRY(cudaGetLastError());
+    LA_TRY(scan_exclusive(table.as<int>(), kRadix * nb, st));
+    radix_scatter_kernel<<<nb, kSortThreads, 0, st>>>(
+        n, key, shift, table.as<int>(), kh[c].as<unsigned>(), kl[c].as<unsigned>(),
+        kp[c].as<int>(), kh[1 - c].as<unsigned>(), kl[1 - c].as<unsigned>(), kp[1 - c].as<int>());
+    LA_CUDA_TRY(cudaGetLastError());
+    c = 1 - c;
+  }
+  LA_CUDA_TRY(cudaStreamSynchronize(st)); // table is released on return
+  *cur = c;
+  return LA_OK;
+}
+
+// out[q] = base + (number of sorted keys below q), q in [0, nq]: the start of
+// every key's run in a sorted array (row pointers, level boundaries).
+la_status run_starts(int n, const unsigned *sorted, int nq, int base, int *out, cudaStream_t st) {
+  row_pointer_kernel<<<(nq + 1 + 255) / 256, 256, 0, st>>>(nq, n, sorted, base, out);
+  LA_CUDA_TRY(cudaGetLastError());
+  return LA_OK;
+}
+
 // Device CSR from host COO entries (indices carry `base`; rows[k] - base in
 // [0, nrows), cols[k] - base in [0, ncols)).
 la_status csr_from_coo(int nrows, int ncols, long long nnz_l, int base, const int *rows,
@@ -286,26 +325,8 @@ la_status csr_from_coo(int nrows, int ncols, long long nnz_l, int base, const in
   int unordered = 0;
   LA_CUDA_TRY(cudaMemcpy(&unordered, flag.p, sizeof(int), cudaMemcpyDeviceToHost));
   int cur = 0;
-  if (unordered) {
-    const int nb = (nnz + kSortTile - 1) / kSortTile;
-    DevBuf table;
-    LA_TRY(table.alloc(sizeof(int) * (size_t)kRadix * nb));
-    const int cpass = (bits_for((unsigned)ncols) + 7) / 8, rpass = (bits_for((unsigned)nrows) + 7) / 8;
-    for (int pass = 0; pass < cpass + rpass; pass++) {
-      const bool on_col = pass < cpass;
-      const int shift = 8 * (on_col ? pass : pass - cpass);
-      const unsigned *key = on_col ? kc[cur].as<unsigned>() : kr[cur].as<unsigned>();
-      radix_hist_kernel<<<nb, kSortThreads, 0, st>>>(nnz, key, shift, table.as<int>());
-      LA_CUDA_TRY(cudaGetLastError());
-      LA_TRY(scan_exclusive(table.as<int>(), kRadix * nb, st));
-      radix_scatter_kernel<<<nb, kSortThreads, 0, st>>>(
-          nnz, key, shift, table.as<int>(), kr[cur].as<unsigned>(), kc[cur].as<unsigned>(),
-          kp[cur].as<int>(), kr[1 - cur].as<unsigned>(), kc[1 - cur].as<unsigned>(),
-          kp[1 - cur].as<int>());
-      LA_CUDA_TRY(cudaGetLastError());
-      cur = 1 - cur;
-    }
-  }
+  if (unordered)
+    LA_TRY(radix_sort_pairs(nnz, (unsigned)nrows, (unsigned)ncols, kr, kc, kp, &cur, st));
   row_pointer_kernel<<<(nrows + 1 + 255) / 256, 256, 0, st>>>(nrows, nnz, kr[cur].as<unsigned>(),
                                                               base, A->ai.as<int>());
   if (dtype == LA_F64)

@@ -45,19 +45,6 @@ const char *get_error();
     }                                                                          \
   } while (0)
 
-// Ingest (la_ingest.cu): host readers of the reference's binary COO and of
-// Matrix Market text, and the device build of a CSR from COO entries.
-la_status read_file(const char *path, std::string &buf);
-la_status read_binary_coo(const char *path, int base, std::vector<int> &rows,
-                          std::vector<int> &cols, std::vector<double> &vals, int *m, int *n);
-la_status parse_matrix_market(const char *text, size_t len, std::vector<int> &rows,
-                              std::vector<int> &cols, std::vector<double> &vals, int *m,
-                              int *n);
-la_status csr_from_coo(int nrows, int ncols, long long nnz, int base, const int *rows,
-                       const int *cols, const void *vals, la_dtype dtype, int flags,
-                       la_csr_t *out);
-// The optional FP32 copy of an FP64 matrix's values (LA_CSR_KEEP_F32).
-la_status csr_finish(la_csr_t A, int flags);
 
 // Returns LA_OK if a CUDA device of compute capability 10.x is current.
 la_status require_device();
@@ -76,6 +63,36 @@ struct DevBuf {
   void release();
   template <typename T> T *as() const { return static_cast<T *>(p); }
 };
+
+// Ingest (la_ingest.cu): host readers of the reference's binary COO and of
+// Matrix Market text, and the device build of a CSR from COO entries.
+la_status read_file(const char *path, std::string &buf);
+la_status read_binary_coo(const char *path, int base, std::vector<int> &rows,
+                          std::vector<int> &cols, std::vector<double> &vals, int *m, int *n);
+la_status parse_matrix_market(const char *text, size_t len, std::vector<int> &rows,
+                              std::vector<int> &cols, std::vector<double> &vals, int *m,
+                              int *n);
+la_status csr_from_coo(int nrows, int ncols, long long nnz, int base, const int *rows,
+                       const int *cols, const void *vals, la_dtype dtype, int flags,
+                       la_csr_t *out);
+// Device IC(0) / ILU(0) (la_factor.cu): kind 0 = IC(0) on the upper
+// triangle with diagonals first, 1 = ILU(0) on a full pattern.
+la_status factor_plan_create(int kind, int n, int base, const int *ai, const int *aj,
+                             la_factor_plan_t *out);
+la_status factor_numeric(la_factor_plan_t P, const double *av, double omega, double *out,
+                         bool on_device, int *bad_row, cudaStream_t st);
+// Stable LSD radix sort by (hi, lo) keys on the device (la_ingest.cu); the
+// buffers [*cur] hold the input, *cur names the result's on return.
+la_status radix_sort_pairs(int n, unsigned hi_range, unsigned lo_range, DevBuf (&kh)[2],
+                           DevBuf (&kl)[2], DevBuf (&kp)[2], int *cur, cudaStream_t st);
+// out[q] = base + (sorted keys below q) for q in [0, nq].
+la_status run_starts(int n, const unsigned *sorted, int nq, int base, int *out, cudaStream_t st);
+// TopologicalSort2 on the device (la_levels.cu), same outputs as
+// topological_sort2; the triangle must be strict.
+la_status topological_sort2_device(int uplo, int n, int base, const int *ai, const int *aj,
+                                   int *iperm, int *prefix, int *levels);
+// The optional FP32 copy of an FP64 matrix's values (LA_CSR_KEEP_F32).
+la_status csr_finish(la_csr_t A, int flags);
 
 // ------------------------------------------------------------ host algos
 // (la_host.cpp) -- restatements of the reference's host-side steps.
@@ -198,4 +215,20 @@ struct la_pcg_s {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double *h_rr = nullptr;       // pinned host copy of the residual norm
   cudaEvent_t ev_rr = nullptr;  // marks its arrival
+};
+
+// Device IC(0) / ILU(0) plan (la_factor.cu).
+struct la_factor_plan_s {
+  int kind = 0; // 0: IC(0), 1: ILU(0)
+  int n = 0, nnz = 0, base = 0, levels = 0, nchunks = 0, grid = 0;
+  // per row (original numbering): its value range [rs, re) and its diagonal
+  la::DevBuf rs, diag;
+  // rows in execution order, 32-row chunks that never cross a level
+  la::DevBuf exec_row, chunk_start;
+  // per row: its updates [uptr[j], uptr[j+1]); per update: source row k,
+  // scalar index (IC: U_kj in row k; ILU: the row's own L_jk entry), pivot
+  // index (ILU: row k's diagonal), and its pairs [pptr[u], pptr[u+1])
+  la::DevBuf uptr, uk, us, upiv, pptr, ptgt, psrc;
+  la::DevBuf vin, done, state; // state: ticket, timeout flag, smallest bad row
+  std::vector<int> h_ai;
 };

@@ -62,6 +62,7 @@ constexpr int kThreads = 256;
 constexpr int kChunk = 32;
 constexpr int kDeps = 8; // dependency loads issued together per row
 constexpr unsigned long long kWaitNs = 1000000000ull; // 1 s per wait
+constexpr int kDeviceLevelsRows = 65536; // level sets on the GPU from this size
 
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
@@ -1029,9 +1030,15 @@ la_status trsv_build(la_trsv_plan_t P, const int *ai, const int *aj,
   } else {
     P->h_iperm.resize(n);
     P->h_prefix.resize(n + 1);
-    P->levels = n == 0 ? 0
-                       : topological_sort2(P->uplo, n, base, ai, aj,
-                                           P->h_iperm.data(), P->h_prefix.data());
+    // large triangles: the same level sets computed on the GPU
+    if (n >= kDeviceLevelsRows) {
+      LA_TRY(topological_sort2_device(P->uplo, n, base, ai, aj, P->h_iperm.data(),
+                                      P->h_prefix.data(), &P->levels));
+    } else {
+      P->levels = n == 0 ? 0
+                         : topological_sort2(P->uplo, n, base, ai, aj, P->h_iperm.data(),
+                                             P->h_prefix.data());
+    }
     P->h_prefix.resize(P->levels + 1);
   }
   if (n == 0)

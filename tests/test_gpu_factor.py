@@ -1,0 +1,128 @@
+"""IC(0) and ILU(0) numeric factorisation on the GPU (la_factor_*).
+
+The device factor equals the host factorisation bit for bit -- la_icc0,
+whose values are bit-identical to the reference's ICCLevelNumeric
+(precond.hpp:615-693), and la_ilu0 -- on stencils in natural and RCM order,
+a nonsymmetric pattern and base 1; a breakdown is reported at the row where
+the sequential algorithm stops; the shift-retry loop (incomplete_cholesky.cpp
+:315-342) ends at the same shift with the same factor.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import gpu_available
+
+
+def _ic_inputs(lab, mat, rcm):
+    from linearalgebra_b200 import gen
+    n, ai, aj, av = mat
+    if rcm:
+        iperm, perm = lab.SerialCM(n, 0, ai, aj)
+        ai, aj, av = lab.Permute(n, 0, ai, aj, av, iperm, perm)
+    ua, uj, uv = gen.upper_with_diag(n, ai, aj, av)
+    return n, np.asarray(ua, np.int32), np.asarray(uj, np.int32), np.asarray(uv)
+
+
+def _nonsym(m, seed):
+    rng = np.random.default_rng(seed)
+    rows = [np.union1d(rng.choice(m, 6, replace=False), [i]) for i in range(m)]
+    ai = np.concatenate([[0], np.cumsum([len(c) for c in rows])]).astype(np.int32)
+    aj = np.concatenate(rows).astype(np.int32)
+    av = rng.uniform(-1, 1, len(aj))
+    r = np.repeat(np.arange(m), np.diff(ai))
+    av[aj == r] = 8.0
+    return m, ai, aj, av
+
+
+@pytest.mark.skipif(gpu_available(), reason="checks the no-GPU behaviour")
+def test_factor_plan_needs_a_device(lab):
+    from linearalgebra_b200 import gen
+    n, ua, uj, uv = _ic_inputs(lab, gen.laplacian_2d(8), False)
+    with pytest.raises(lab.LAError) as e:
+        lab.FactorPlan("ic0", n, 0, ua, uj)
+    assert e.value.name == "LA_ERR_NO_DEVICE"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rcm", [False, True])
+def test_ic0_device_bit_identical(lab, rcm):
+    from linearalgebra_b200 import gen
+    for mat in (gen.laplacian_3d(32), gen.stencil27(16, seed=2), gen.aniso7(24, seed=1),
+                gen.laplacian_2d(64)):
+        n, ua, uj, uv = _ic_inputs(lab, mat, rcm)
+        want = lab.ICCLevelNumeric0(n, 0, ua, uj, uv)
+        plan = lab.FactorPlan("ic0", n, 0, ua, uj)
+        got = plan.factor(uv)
+        assert np.array_equal(got, want), (n, rcm, np.abs(got - want).max())
+        # the same plan again, with a shift, and with device arrays
+        import torch
+        want2 = lab.ICCLevelNumeric0(n, 0, ua, uj, uv, omega=0.25)
+        assert np.array_equal(plan.factor(uv, omega=0.25), want2)
+        out = torch.empty(len(uv), dtype=torch.float64, device="cuda")
+        plan.factor(torch.as_tensor(uv).cuda(), out=out)
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy(), want)
+
+
+@pytest.mark.gpu
+def test_ic0_device_base1_and_breakdown(lab):
+    from linearalgebra_b200 import gen
+    n, ua, uj, uv = _ic_inputs(lab, gen.laplacian_3d(16), True)
+    want = lab.ICCLevelNumeric0(n, 0, ua, uj, uv)
+    got = lab.FactorPlan("ic0", n, 1, ua + 1, uj + 1).factor(uv)
+    assert np.array_equal(got, want)
+    # a negative pivot at row j0 (its diagonal made negative): reported there
+    j0 = n // 3
+    bad = uv.copy()
+    bad[ua[j0]] = -1.0
+    with pytest.raises(lab.LAError):
+        lab.ICCLevelNumeric0(n, 0, ua, uj, bad)
+    plan = lab.FactorPlan("ic0", n, 0, ua, uj)
+    with pytest.raises(lab.LAError) as e:
+        plan.factor(bad)
+    assert e.value.name == "LA_ERR_BREAKDOWN" and e.value.bad_row == j0
+    # shift retries: same shift, same factor as the host loop
+    hv, hs = lab.ICCShifted(n, 0, ua, uj, bad)
+    dv, ds = plan.shifted(bad)
+    assert ds == hs and np.array_equal(dv, hv)
+
+
+@pytest.mark.gpu
+def test_ilu0_device_bit_identical(lab):
+    from linearalgebra_b200 import gen
+    for n, ai, aj, av in (gen.laplacian_3d(20), gen.aniso7(16, seed=3), _nonsym(3000, 5)):
+        want = lab.ILU0(n, 0, ai, aj, av)
+        plan = lab.FactorPlan("ilu0", n, 0, ai, aj)
+        assert np.array_equal(plan.factor(av), want), n
+        got1 = lab.FactorPlan("ilu0", n, 1, np.asarray(ai) + 1, np.asarray(aj) + 1).factor(av)
+        assert np.array_equal(got1, want), n
+    # a zero pivot: row 1 of [[1, 1], [1, 1]]
+    ai, aj = np.array([0, 2, 4], np.int32), np.array([0, 1, 0, 1], np.int32)
+    with pytest.raises(lab.LAError) as e:
+        lab.FactorPlan("ilu0", 2, 0, ai, aj).factor(np.ones(4))
+    assert e.value.bad_row == 1
+
+
+@pytest.mark.gpu
+def test_ic0_device_c3_size(lab):
+    """The RCM-ordered 128^3 Laplacian's IC(0): bit-identical at full size;
+    prints the host and device numeric times."""
+    import time
+    from linearalgebra_b200 import gen
+    n, ua, uj, uv = _ic_inputs(lab, gen.laplacian_3d(128), True)
+    t0 = time.perf_counter()
+    want = lab.ICCLevelNumeric0(n, 0, ua, uj, uv)
+    t_host = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    plan = lab.FactorPlan("ic0", n, 0, ua, uj)
+    t_sym = time.perf_counter() - t0
+    plan.factor(uv)
+    t0 = time.perf_counter()
+    got = plan.factor(uv)
+    t_num = time.perf_counter() - t0
+    assert np.array_equal(got, want)
+    print(f"IC(0) 128^3: host {t_host * 1e3:.1f} ms, device plan {t_sym * 1e3:.1f} ms, "
+          f"device numeric (host arrays in and out) {t_num * 1e3:.1f} ms, "
+          f"{plan.levels()} levels")
