@@ -350,15 +350,40 @@ def pcg_case(la, torch, label, matrix):
     """FP64 vs mixed IC(0)-PCG to 1e-10 on an RCM-ordered SPD matrix."""
     from linearalgebra_b200 import gen
     n, ai, aj, av = matrix
+    br = {}
     t0 = time.perf_counter()
+
+    def lap(key, t=[t0]):
+        now = time.perf_counter()
+        br[key] = now - t[0]
+        t[0] = now
+
     iperm, perm = la.SerialCM(n, 0, ai, aj)
+    lap("rcm_host")
     b_ai, b_aj, b_av = la.Permute(n, 0, ai, aj, av, iperm, perm)
     ua, uj, uv = gen.upper_with_diag(n, b_ai, b_aj, b_av)
+    lap("permute_and_upper_host")
     f = la.ICCLevelNumeric0(n, 0, ua, uj, uv)
+    lap("icc0_host")
     A = la.CSR(n, n, 0, b_ai, b_aj, b_av, keep_f32=True)
+    lap("csr_upload")
     s64 = la.PCG(A, ua, uj, f)
+    lap("pcg_create_fp64")
     s32 = la.PCG(A, ua, uj, f, mixed=True)
+    lap("pcg_create_mixed")
     setup_s = time.perf_counter() - t0
+    # the same IC(0) on the GPU (plan once per pattern, numeric pass), and
+    # the L factor's level sets on the host and on the GPU -- outside setup_s
+    t1 = time.perf_counter()
+    fp = la.FactorPlan("ic0", n, 0, ua, uj)
+    br["icc0_device_plan"] = time.perf_counter() - t1
+    fp.factor(uv)
+    t1 = time.perf_counter()
+    fd = fp.factor(uv)
+    br["icc0_device_numeric"] = time.perf_counter() - t1
+    br["icc0_device_bit_identical"] = bool(np.array_equal(fd, f))
+    br["icc0_levels"] = fp.levels()
+    del fp
     bvec = gen.uniform_vector(n, 0)
     bd = torch.as_tensor(bvec).to("cuda")
     x64 = torch.empty(n, dtype=torch.float64, device="cuda")
@@ -372,6 +397,14 @@ def pcg_case(la, torch, label, matrix):
     nnz_tri = (nnz - n) // 2
     _, d, (s_ai, s_aj, s_av) = la.SplitLDU(n, 0, ua, uj, f)
     t_ai, t_aj, t_av = la.Transpose(n, n, 0, s_ai, s_aj, s_av)
+    t1 = time.perf_counter()
+    lh = la.TopologicalSort2("L", n, 0, t_ai, t_aj)
+    br["levels_host"] = time.perf_counter() - t1
+    t1 = time.perf_counter()
+    ld = la.TopologicalSort2("L", n, 0, t_ai, t_aj, device=True)
+    br["levels_device"] = time.perf_counter() - t1
+    br["levels_identical"] = bool(lh[0] == ld[0] and np.array_equal(lh[1], ld[1])
+                                  and np.array_equal(lh[2], ld[2]))
     sched = {}
     for name, dt in (("fp64", np.float64), ("fp32", np.float32)):
         ts = la.OptimizedTriangularSolve("L", dtype=dt).analysis(n, 0, t_ai, t_aj, t_av, d)
@@ -380,7 +413,7 @@ def pcg_case(la, torch, label, matrix):
     b64 = pcg_iteration_bytes(n, nnz, nnz_tri, 8)
     b32 = pcg_iteration_bytes(n, nnz, nnz_tri, 4)
     res = {"config": label, "n": n, "nnz": nnz, "rtol": 1e-10, "levels": levels,
-           "setup_s_host": setup_s,
+           "setup_s_host": setup_s, "setup_breakdown_s": br,
            "fp64": {"iterations": r64.iterations, "ms": r64.solve_ms,
                     "rel_residual": r64.rel_residual,
                     "GB/s_algorithmic": b64 * r64.iterations / (r64.solve_ms * 1e-3) / 1e9},
@@ -431,6 +464,56 @@ def run_case(case):
         y = torch.empty_like(x)
         for _ in range(3):
             P(x, y)
+    elif case == "adjoint-c4":
+        # the SpMV adjoints on the 96^3 27-point stencil: transpose SpMV and
+        # the sampled outer product over the pattern
+        n, ai, aj, av = gen.stencil27(96, seed=0)
+        P = la.SPMV(la.CSR(n, n, 0, ai, aj, av))
+        g = torch.as_tensor(gen.uniform_vector(n, 1)).cuda()
+        x = torch.as_tensor(gen.uniform_vector(n, 2)).cuda()
+        out = torch.empty_like(x)
+        dv = torch.empty(int(ai[-1]), dtype=torch.float64, device="cuda")
+        for _ in range(3):
+            P.transpose(g, out)
+            P.sddmm(g, x, dv)
+    elif case in ("factor-c3", "levels-c3"):
+        # IC(0) of the RCM-ordered 128^3 Laplacian on the GPU, or the level
+        # sets of its L factor on the GPU
+        n, ai, aj, av = gen.laplacian_3d(128)
+        iperm, perm = la.SerialCM(n, 0, ai, aj)
+        b_ai, b_aj, b_av = la.Permute(n, 0, ai, aj, av, iperm, perm)
+        ua, uj, uv = gen.upper_with_diag(n, b_ai, b_aj, b_av)
+        if case == "factor-c3":
+            fp = la.FactorPlan("ic0", n, 0, ua, uj)
+            for _ in range(3):
+                fp.factor(uv)
+        else:
+            f = la.ICCLevelNumeric0(n, 0, ua, uj, uv)
+            _, d, (s_ai, s_aj, s_av) = la.SplitLDU(n, 0, ua, uj, f)
+            t_ai, t_aj, _ = la.Transpose(n, n, 0, s_ai, s_aj, s_av)
+            for _ in range(3):
+                la.TopologicalSort2("L", n, 0, t_ai, t_aj, device=True)
+    elif case == "ingest":
+        # 16M shuffled COO entries (4M x 4M) sorted into a device CSR
+        rng = np.random.default_rng(0)
+        k, m = 16_000_000, 4_000_000
+        rows, cols = rng.integers(0, m, k), rng.integers(0, m, k)
+        vals = rng.standard_normal(k)
+        for _ in range(2):
+            la.csr_from_coo(m, m, 0, rows, cols, vals)
+    elif case == "noalloc-c3":
+        # the allocation-free SpMV on the 128^3 Laplacian
+        n, ai, aj, av = gen.laplacian_3d(128)
+        dev_ = lambda a, t: torch.as_tensor(np.ascontiguousarray(a)).to("cuda", t)
+        ai_d, aj_d, av_d = dev_(ai, torch.int32), dev_(aj, torch.int32), dev_(av, torch.float64)
+        x = dev_(gen.uniform_vector(n, 0), torch.float64)
+        y = torch.empty_like(x)
+        st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        for _ in range(3):
+            la.lib().la_spmv_noalloc(la.api.LA_SPMV_SEGSUM, n, int(ai[-1]), 0,
+                                     C.c_void_p(ai_d.data_ptr()), C.c_void_p(aj_d.data_ptr()),
+                                     C.c_void_p(av_d.data_ptr()), 1.0, C.c_void_p(x.data_ptr()),
+                                     0.0, C.c_void_p(y.data_ptr()), st)
     elif case == "trsv-c5-f32":
         # FP32 lower solve of the RCM-ordered 192^3 anisotropic IC(0) factor:
         # the partitioned kernel with second-row register sets
@@ -480,7 +563,8 @@ def main():
     ap.add_argument("--no-cpu-pcg", action="store_true")
     ap.add_argument("--case", default=None,
                     choices=["spmv-powerlaw", "spmv-lap3d", "trsv-lap3d", "trsv-c5-f32",
-                             "pcg-lap3d"],
+                             "pcg-lap3d", "adjoint-c4", "factor-c3", "levels-c3", "ingest",
+                             "noalloc-c3"],
                     help="run one kernel workload a few times and exit (for ncu)")
     args = ap.parse_args()
     args.steps_given = args.steps is not None
@@ -538,6 +622,24 @@ def main():
     value = replica_value(world, args.steps, byt, t)
     launch_s = t / args.steps
 
+    # the matrix's own bound for the tile pass (la_spmv_ceiling): its columns
+    # and values streamed, with and without the random x gather, back to back
+    ceiling = {}
+    for key, gather in (("stream_us", False), ("stream_and_gather_us", True)):
+        sink = torch.zeros(1, dtype=torch.float64, device="cuda")
+        for _ in range(3):
+            plan.ceiling(xd, gather, sink)
+        torch.cuda.synchronize()
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0.record()
+        for _ in range(100):
+            plan.ceiling(xd, gather, sink)
+        c1.record()
+        torch.cuda.synchronize()
+        ceiling[key] = c0.elapsed_time(c1) / 100 * 1e3
+    ceiling["matrix_bytes_streamed"] = (nnz // 1024) * 1024 * 12
+    ceiling["headline_over_gather_ceiling"] = ceiling["stream_and_gather_us"] / (launch_s * 1e6)
+
     # end to end through the reference-facing host-pointer call: pinned host
     # x in, y out, every step
     hx = torch.as_tensor(x).pin_memory()
@@ -573,6 +675,7 @@ def main():
         "e2e": {"value": e2e, "unit": "GB/s", "h2d_bytes_per_step": n * 8,
                 "d2h_bytes_per_step": n * 8, "steps": e2e_steps,
                 "api": "SPMV.__call__ host arrays -> la_spmv_host", "matches_device": bool(ok)},
+        "gather_ceiling": ceiling,
         "gpu_launches": 2 * args.steps,
         "clocks": sampler.summary(),
     }

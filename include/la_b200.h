@@ -147,6 +147,15 @@ la_status la_spmv(la_spmv_plan_t plan, double alpha, const void *x,
 la_status la_spmv_host(la_spmv_plan_t plan, double alpha, const double *x,
                        double beta, double *y);
 la_status la_spmv_plan_destroy(la_spmv_plan_t plan);
+/* Measurement aid (no reference counterpart; not an SpMV): the bound a
+ * matrix sets for the SpMV tile pass.  One launch streams the plan's FP64
+ * matrix (columns and values, 16-byte loads, whole 1024-nonzero tiles) and,
+ * when gather != 0, also gathers the device vector x through the columns --
+ * the tile pass without its row structure.  sink: one device double that is
+ * never written in practice.  Time it like la_spmv; its algorithmic bytes
+ * are nnz * 12 (whole tiles). */
+la_status la_spmv_ceiling(la_spmv_plan_t plan, const double *x, int gather, double *sink,
+                          la_stream_t stream);
 
 /* Allocation-free SpMV.  No counterpart in the reference (which has no
  * device code); it exists for callers that must not allocate device memory:
@@ -235,6 +244,15 @@ la_status la_topological_sort2_device(la_uplo uplo, int n, int base, const int *
  * bit-identical iperm/perm (values carry the base). */
 la_status la_rcm(int n, int base, const int *ai, const int *aj, int *iperm,
                  int *perm);
+/* The same ordering with its large components ordered on the GPU (no
+ * reference counterpart beyond SerialCM itself): components of at least
+ * 65,536 nodes, when no row holds more than 64 entries, get their
+ * pseudo-peripheral search as level-synchronous device BFS and their
+ * Cuthill-McKee sweep as per-level device steps (parents, child counts, a
+ * scan, per-parent sorts by (degree, index)); the rest as la_rcm.  The
+ * outputs are identical to la_rcm's. */
+la_status la_rcm_device(int n, int base, const int *ai, const int *aj, int *iperm,
+                        int *perm);
 /* ILU(0) on A's own pattern, from scratch (no reference counterpart: the
  * reference factors ILU through MKL, and its level-0 path never fills the
  * upper-part positions, incomplete_lu.cpp:166 / :267-269).  lu_av (A's

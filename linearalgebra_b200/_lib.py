@@ -101,6 +101,8 @@ _SIGS = {
     "la_pcg_solve_host": [P, P, P, D, I, C.POINTER(PcgInfo)],
     "la_pcg_adjoint": [P, P, P, P, P, D, I, C.POINTER(PcgInfo), P],
     "la_pcg_fused": [P, IP],
+    "la_rcm_device": [I, I, P, P, P, P],
+    "la_spmv_ceiling": [P, P, I, P, P],
     "la_topological_sort2_device": [I, I, I, P, P, P, P, IP],
     "la_icc0_plan_create": [I, I, P, P, C.POINTER(P)],
     "la_ilu0_plan_create": [I, I, P, P, C.POINTER(P)],

@@ -170,6 +170,16 @@ class SPMV:
              len(slices), float(beta), _ptr(y), vd, _stream(y))
         return y
 
+    def ceiling(self, x, gather=True, sink=None):
+        """The matrix's streaming bound for the tile pass (la_spmv_ceiling):
+        its columns and values streamed, x gathered when ``gather``; a
+        measurement aid, not an SpMV."""
+        import torch
+        if sink is None:
+            sink = torch.zeros(1, dtype=torch.float64, device=x.device)
+        call("la_spmv_ceiling", self.h, _ptr(x), int(bool(gather)), _ptr(sink), _stream(x))
+        return sink
+
     def transpose(self, g, out, alpha=1.0, beta=0.0):
         """out = alpha*A^T g + beta*out (device FP64 tensors)."""
         call("la_spmv_transpose", self.h, float(alpha), _ptr(g), float(beta),
@@ -507,12 +517,15 @@ def TopologicalSort2(uplo, nodes, base, ai, aj, device=False):
     return lv.value, iperm, prefix[: lv.value + 1].copy()
 
 
-def SerialCM(n, base, ai, aj):
-    """Reverse Cuthill-McKee (reordering/Reordering.cpp:37-136): (iperm, perm)."""
+def SerialCM(n, base, ai, aj, device=False):
+    """Reverse Cuthill-McKee (reordering/Reordering.cpp:37-136): (iperm, perm);
+    ``device=True`` orders large components on the GPU (la_rcm_device, the
+    same ordering)."""
     ai, aj = _i32(ai), _i32(aj)
     iperm = np.empty(n, np.int32)
     perm = np.empty(n, np.int32)
-    call("la_rcm", int(n), int(base), _ptr(ai), _ptr(aj), _ptr(iperm), _ptr(perm))
+    call("la_rcm_device" if device else "la_rcm", int(n), int(base), _ptr(ai), _ptr(aj),
+         _ptr(iperm), _ptr(perm))
     return iperm, perm
 
 

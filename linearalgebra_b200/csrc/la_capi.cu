@@ -15,6 +15,8 @@ la_status spmv_xparts_launch(la_spmv_plan_t P, double alpha, const void *const *
                              la_dtype vd, cudaStream_t st);
 la_status sddmm_launch(la_spmv_plan_t P, double alpha, const double *g,
                        const double *x, double *dv, cudaStream_t st);
+la_status spmv_ceiling_launch(la_spmv_plan_t P, const double *x, int gather, double *sink,
+                              cudaStream_t st);
 la_status spmv_noalloc(la_spmv_kind kind, int n, int nnz, int base, const int *ai,
                        const int *aj, const double *av, double alpha, const double *x,
                        double beta, double *y, cudaStream_t st);
@@ -431,6 +433,12 @@ la_status la_spmv_noalloc(la_spmv_kind kind, int n, int nnz, int base,
                       S(stream));
 }
 
+la_status la_spmv_ceiling(la_spmv_plan_t plan, const double *x, int gather, double *sink,
+                          la_stream_t stream) {
+  LA_CHECK_ARG(plan && sink && (!gather || x), "arguments");
+  return spmv_ceiling_launch(plan, x, gather, sink, S(stream));
+}
+
 la_status la_sddmm_pattern(la_spmv_plan_t plan, double alpha, const double *g,
                            const double *x, double *dv, la_stream_t stream) {
   LA_CHECK_ARG(plan && g && x && (dv || plan->A->nnz == 0), "arguments");
@@ -494,8 +502,22 @@ la_status la_rcm(int n, int base, const int *ai, const int *aj, int *iperm,
     set_error("la_rcm needs a structurally symmetric pattern");
     return LA_ERR_INVALID_ARG;
   }
-  rcm(n, base, ai, aj, iperm, perm);
-  return LA_OK;
+  return rcm(n, base, ai, aj, iperm, perm);
+}
+
+la_status la_rcm_device(int n, int base, const int *ai, const int *aj, int *iperm,
+                        int *perm) {
+  LA_CHECK_ARG(ai && iperm && perm && n >= 0, "arguments");
+  const int nnz = ai[n] - base;
+  std::vector<int> tai(n + 1), taj(std::max(nnz, 1));
+  transpose(n, n, base, ai, aj, nullptr, tai.data(), taj.data(), nullptr);
+  if (std::memcmp(tai.data(), ai, sizeof(int) * (n + 1)) != 0 ||
+      std::memcmp(taj.data(), aj, sizeof(int) * nnz) != 0) {
+    set_error("la_rcm_device needs a structurally symmetric pattern");
+    return LA_ERR_INVALID_ARG;
+  }
+  LA_TRY(require_device());
+  return rcm(n, base, ai, aj, iperm, perm, true);
 }
 
 la_status la_permute(int n, int base, const int *ai, const int *aj,

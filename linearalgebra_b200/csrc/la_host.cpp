@@ -460,10 +460,22 @@ struct Bfs {
 };
 } // namespace
 
-void rcm(int n, int base, const int *ai, const int *aj, int *iperm, int *perm) {
+// With `device`, components of at least kRcmDeviceMin nodes are ordered on
+// the GPU (la_rcm.cu; same ordering) when no row holds more than
+// kRcmMaxDegree entries.
+la_status rcm(int n, int base, const int *ai, const int *aj, int *iperm, int *perm,
+              bool device) {
   std::vector<int> deg(n);
-  for (int i = 0; i < n; i++)
+  int maxdeg = 0;
+  for (int i = 0; i < n; i++) {
     deg[i] = ai[i + 1] - ai[i];
+    maxdeg = std::max(maxdeg, deg[i]);
+  }
+  device = device && maxdeg <= kRcmMaxDegree;
+  struct DeviceOwner {
+    RcmDevice *d = nullptr;
+    ~DeviceOwner() { rcm_device_destroy(d); }
+  } dev;
   Bfs bfs{ai, aj, base, {}, {}, {}};
 
   // components, ordered by their largest node; members ascending
@@ -501,6 +513,16 @@ void rcm(int n, int base, const int *ai, const int *aj, int *iperm, int *perm) {
     if (size <= 2) {
       for (int q = 0; q < size; q++)
         iperm[off + q] = members[off + q] + base;
+      continue;
+    }
+    if (device && size >= kRcmDeviceMin) {
+      if (!dev.d) {
+        la_status st = LA_OK;
+        dev.d = rcm_device_create(n, base, ai, aj, deg.data(), &st);
+        if (!dev.d)
+          return st;
+      }
+      LA_TRY(rcm_device_component(dev.d, members.data() + off, size, iperm + off));
       continue;
     }
     int src = members[off];
@@ -562,6 +584,7 @@ void rcm(int n, int base, const int *ai, const int *aj, int *iperm, int *perm) {
   std::reverse(iperm, iperm + n);
   for (int i = 0; i < n; i++)
     perm[iperm[i] - base] = i + base;
+  return LA_OK;
 }
 
 } // namespace la

@@ -119,7 +119,16 @@ int split_triangle(int uplo, int n, int base, const int *ai, const int *aj,
                    const double *av, int *t_ai, int *t_aj, double *t_av);
 bool icc0(int n, int base, const int *u_ai, const int *u_aj, const double *u_av,
           double omega, double *icc_av);
-void rcm(int n, int base, const int *ai, const int *aj, int *iperm, int *perm);
+// RCM (SerialCM); with `device` large components are ordered on the GPU.
+constexpr int kRcmDeviceMin = 65536;
+constexpr int kRcmMaxDegree = 64;
+struct RcmDevice;
+RcmDevice *rcm_device_create(int n, int base, const int *ai, const int *aj, const int *deg,
+                             la_status *st);
+void rcm_device_destroy(RcmDevice *D);
+la_status rcm_device_component(RcmDevice *D, const int *members, int size, int *out);
+la_status rcm(int n, int base, const int *ai, const int *aj, int *iperm, int *perm,
+              bool device = false);
 // Row partition for the partitioned triangular solve (la_partition.cpp):
 // k-d cuts on coordinates monotone along the dependency edges (row i reads
 // row j for every stored (i, j) of dep_ptr/dep_col, which carry `base`), so

@@ -389,8 +389,14 @@ __global__ void spmv_empty_kernel(int n, X *y, const X *yin, ACC beta) {
     y[r] = X(beta == ACC(0) ? ACC(0) : beta * ACC(yin[r]));
 }
 
-// dv[k] = alpha * g[row(k)] * x[col(k)] over the stored pattern; the row of
-// each nonzero is found by binary search in the staged row starts.
+// dv[k] = alpha * g[row(k)] * x[col(k)] over the stored pattern.  The column
+// loads and x gathers are issued first; meanwhile every nonempty row of the
+// tile marks the slot of its first nonzero with its tile-local index, and an
+// inclusive max-scan over the tile's 1024 slots (4 consecutive slots per
+// thread, a warp shuffle scan, the warps' totals in shared memory) gives
+// every nonzero its row -- the last row starting at or before it -- with no
+// search.  A tile whose row span does not fit in shared memory (runs of
+// empty rows) finds its rows by binary search in the row pointers.
 __global__ void __launch_bounds__(kThreads)
     sddmm_kernel(const int n, const int nnz, const int base,
                  const int *__restrict__ ai, const int *__restrict__ aj,
@@ -398,25 +404,107 @@ __global__ void __launch_bounds__(kThreads)
                  double *__restrict__ dv, const double alpha,
                  const int *__restrict__ tile_row) {
   __shared__ int rp[kRowCap];
+  __shared__ int row_of[kTile];
+  __shared__ int wmax[kThreads / 32];
   const TileRows T = tile_rows(blockIdx.x, n, nnz, tile_row);
-  stage_rows(T, base, ai, rp);
-  __syncthreads();
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  int jj[kNpt];
+  double xv[kNpt];
 #pragma unroll
   for (int q = 0; q < kNpt; q++) {
-    const int kk = q * kThreads + threadIdx.x;
-    if (kk >= T.cnt)
-      continue;
-    int lo = 0, hi = T.nrows - 1; // last row i with start(i) <= kk
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (row_start(T, base, ai, rp, mid) <= kk)
-        lo = mid;
-      else
-        hi = mid - 1;
-    }
-    const int k = T.s + kk;
-    dv[k] = alpha * __ldg(g + T.R0 + lo) * __ldg(x + ld_once(aj + k) - base);
+    const int kk = q * kThreads + tid;
+    if (kk < T.cnt)
+      jj[q] = ld_once(aj + T.s + kk);
   }
+#pragma unroll
+  for (int q = 0; q < kNpt; q++)
+    if (q * kThreads + tid < T.cnt)
+      xv[q] = __ldg(x + jj[q] - base);
+  stage_rows(T, base, ai, rp);
+#pragma unroll
+  for (int q = 0; q < kNpt; q++)
+    row_of[q * kThreads + tid] = -1;
+  __syncthreads();
+  if (T.staged) {
+    for (int i = tid; i < T.nrows; i += kThreads) // distinct starts: nonempty rows
+      if (rp[i] < rp[i + 1])
+        row_of[rp[i]] = i;
+    __syncthreads();
+    const int k0 = kNpt * tid;
+    int r[kNpt], m = -1;
+#pragma unroll
+    for (int q = 0; q < kNpt; q++) {
+      m = max(m, row_of[k0 + q]);
+      r[q] = m;
+    }
+    int incl = m;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, d);
+      if (lane >= d)
+        incl = max(incl, v);
+    }
+    if (lane == 31)
+      wmax[warp] = incl;
+    int before = __shfl_up_sync(0xffffffffu, incl, 1);
+    if (lane == 0)
+      before = -1;
+    __syncthreads();
+    for (int w = 0; w < warp; w++)
+      before = max(before, wmax[w]);
+#pragma unroll
+    for (int q = 0; q < kNpt; q++)
+      row_of[k0 + q] = max(before, r[q]);
+    __syncthreads();
+  } else {
+#pragma unroll
+    for (int q = 0; q < kNpt; q++) {
+      const int kk = q * kThreads + tid;
+      if (kk >= T.cnt)
+        continue;
+      int lo = 0, hi = T.nrows - 1; // last row i with start(i) <= kk
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (row_start(T, base, ai, rp, mid) <= kk)
+          lo = mid;
+        else
+          hi = mid - 1;
+      }
+      row_of[kk] = lo;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < kNpt; q++) {
+    const int kk = q * kThreads + tid;
+    if (kk < T.cnt)
+      dv[T.s + kk] = alpha * __ldg(g + T.R0 + row_of[kk]) * xv[q];
+  }
+}
+
+// The achievable bound of a matrix (measurement aid, not an SpMV): every
+// CTA streams one tile's columns and values with 16-byte loads and, when
+// GATHER, gathers x through the columns -- the SpMV tile pass without its row
+// structure (no row pointers, no products in shared memory, no row sums, no
+// partials, no merge).  Each thread's sum is kept live by a store that never
+// happens unless it equals the unlikely `guard`.
+template <bool GATHER>
+__global__ void __launch_bounds__(kThreads, kTileBlocksPerSm)
+    spmv_ceiling_kernel(const int nnz, const int base, const int *__restrict__ aj,
+                        const double *__restrict__ av, const double *__restrict__ x,
+                        double *sink, const double guard) {
+  const int k0 = blockIdx.x * kTile + kNpt * threadIdx.x;
+  if (k0 + kNpt > nnz)
+    return;
+  int jj[kNpt];
+  double vv[kNpt];
+  ld_vec4(aj + k0, jj);
+  ld_vec4(av + k0, vv);
+  double s = 0.0;
+#pragma unroll
+  for (int q = 0; q < kNpt; q++)
+    s += GATHER ? vv[q] * __ldg(x + jj[q] - base) : vv[q] + double(jj[q]);
+  if (s == guard)
+    sink[0] = s;
 }
 
 // Tiles [tile0, tile1) only when tile1 >= 0 (a chunk of a host-pointer call:
@@ -550,6 +638,24 @@ la_status spmv_xparts_launch(la_spmv_plan_t P, double alpha, const void *const *
                                                           (float)beta, yy, yy, st, xp);
   return launch_form<kSegSum, float, float, float, true>(P, av, (float)alpha, nullptr,
                                                          (float)beta, yy, yy, st, xp);
+}
+
+la_status spmv_ceiling_launch(la_spmv_plan_t P, const double *x, int gather, double *sink,
+                              cudaStream_t st) {
+  const la_csr_t A = P->A;
+  if (A->nnz < kTile || A->dtype != LA_F64) {
+    set_error("la_spmv_ceiling: an FP64 matrix of at least %d nonzeros", kTile);
+    return LA_ERR_INVALID_ARG;
+  }
+  const int grid = A->nnz / kTile; // whole tiles only
+  if (gather)
+    spmv_ceiling_kernel<true><<<grid, kThreads, 0, st>>>(A->nnz, A->base, A->aj.as<int>(),
+                                                          A->av.as<double>(), x, sink, 1e300);
+  else
+    spmv_ceiling_kernel<false><<<grid, kThreads, 0, st>>>(A->nnz, A->base, A->aj.as<int>(),
+                                                           A->av.as<double>(), x, sink, 1e300);
+  LA_CUDA_TRY(cudaGetLastError());
+  return LA_OK;
 }
 
 la_status sddmm_launch(la_spmv_plan_t P, double alpha, const double *g,

@@ -1,0 +1,72 @@
+"""RCM with large components ordered on the GPU (la_rcm_device): the same
+(iperm, perm) as the host's la_rcm -- which equals the reference's SerialCM
+(reordering/Reordering.cpp:37-136) on the golden fixtures -- on 2D / 3D
+stencils above the device size threshold, with the nodes in natural and
+shuffled numbering, and on a pattern of several components (a large one
+between small ones and isolated nodes, ordered by their largest node)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _relabel(n, ai, aj, av, seed):
+    """The same graph with its nodes renumbered at random."""
+    p = np.random.default_rng(seed).permutation(n).astype(np.int32)  # new -> old
+    inv = np.argsort(p).astype(np.int32)
+    import linearalgebra_b200 as la
+    return la.Permute(n, 0, ai, aj, av, p, inv)
+
+
+def _blocks(parts):
+    """Block-diagonal union of (n, ai, aj, av) patterns."""
+    ai_l, aj_l, off, nnz = [np.zeros(1, np.int64)], [], 0, 0
+    for n, ai, aj, av in parts:
+        ai_l.append(np.asarray(ai[1:], np.int64) + nnz)
+        aj_l.append(np.asarray(aj, np.int64) + off)
+        off += n
+        nnz += int(ai[-1])
+    return (off, np.concatenate(ai_l).astype(np.int32), np.concatenate(aj_l).astype(np.int32),
+            np.ones(nnz))
+
+
+def test_rcm_device_equals_host(lab):
+    from linearalgebra_b200 import gen
+    iso = (5, np.arange(6, dtype=np.int32), np.arange(5, dtype=np.int32), np.ones(5))
+    cases = {
+        "lap3d_48": gen.laplacian_3d(48),
+        "st27_44": gen.stencil27(44, seed=1),
+        "aniso_48": gen.aniso7(48, seed=4),
+        "lap2d_400": gen.laplacian_2d(400),
+        "multi": _blocks([gen.laplacian_2d(12), gen.laplacian_3d(44), iso, gen.laplacian_2d(3),
+                          gen.laplacian_2d(300)]),
+    }
+    cases["lap3d_48_shuffled"] = (cases["lap3d_48"][0],
+                                  *_relabel(*cases["lap3d_48"], seed=2))
+    for name, (n, ai, aj, av) in cases.items():
+        want = lab.SerialCM(n, 0, ai, aj)
+        got = lab.SerialCM(n, 0, ai, aj, device=True)
+        assert np.array_equal(got[0], want[0]), name
+        assert np.array_equal(got[1], want[1]), name
+        got1 = lab.SerialCM(n, 1, np.asarray(ai) + 1, np.asarray(aj) + 1, device=True)
+        want1 = lab.SerialCM(n, 1, np.asarray(ai) + 1, np.asarray(aj) + 1)
+        assert np.array_equal(got1[0], want1[0]), (name, "base 1")
+
+
+def test_rcm_device_timing_c5_size(lab):
+    """The 192^3 anisotropic diffusion pattern (C5): host and device
+    orderings equal; prints both times."""
+    import time
+    from linearalgebra_b200 import gen
+    n, ai, aj, av = gen.aniso7(192, seed=0)
+    t0 = time.perf_counter()
+    want = lab.SerialCM(n, 0, ai, aj)
+    t_host = time.perf_counter() - t0
+    lab.SerialCM(n, 0, ai, aj, device=True)
+    t0 = time.perf_counter()
+    got = lab.SerialCM(n, 0, ai, aj, device=True)
+    t_dev = time.perf_counter() - t0
+    assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+    print(f"RCM 192^3: host {t_host:.3f} s, with the device ordering {t_dev:.3f} s")

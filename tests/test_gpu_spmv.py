@@ -260,6 +260,29 @@ def test_spmv_adjoints(lab, orc, golden):
         assert np.array_equal(dv.cpu().numpy(), ref), name
 
 
+def test_sddmm_rows_found_in_every_tile_shape(lab, orc):
+    """The sampled outer product finds each nonzero's row by a scan of the
+    tile's row starts, or -- for tiles spanning more rows than shared memory
+    holds (long runs of empty rows) -- by binary search: bit for bit the
+    oracle on edge shapes (empty rows, rows on tile edges, rows spanning many
+    tiles), a power-law matrix and a 27-point stencil."""
+    from linearalgebra_b200 import gen
+    P = orc.ptr
+    mats = [(name, m, n, ai, aj, av) for name, m, n, ai, aj, av in _edge_matrices()]
+    for name, t in (("powerlaw", gen.powerlaw(50_000, seed=6)), ("st27", gen.stencil27(20))):
+        n, ai, aj, av = t
+        mats.append((name, n, n, ai, aj, av))
+    rng = np.random.default_rng(9)
+    for name, m, n, ai, aj, av in mats:
+        g, x = rng.standard_normal(m), rng.standard_normal(n)
+        plan = lab.SPMV(lab.CSR(m, n, 0, ai, aj, av))
+        dv = torch.empty(len(aj), dtype=torch.float64, device="cuda")
+        plan.sddmm(dev(g), dev(x), dv, 0.5)
+        ref = np.empty(len(aj))
+        orc.port().oracle_sddmm_pattern(m, 0, P(ai), P(aj), P(g), P(x), P(ref), 0.5)
+        assert np.array_equal(dv.cpu().numpy(), ref), name
+
+
 def test_spmv_xparts_emulated_ranks(lab):
     """The row-block SpMV of a sharded matrix reading x from its owners'
     slices (la_spmv_xparts), with the ranks emulated as separate device
