@@ -328,3 +328,85 @@ COLTYPE TopologicalSort2(const COLTYPE nodes, const int base, ROWTYPE const *ai,
 
 } // namespace b200
 } // namespace matrix_utils
+
+// The file readers of utils/utils.h, in utils::b200 with the reference's
+// signatures (a caller switches utils::ReadFromBinaryCSR to
+// utils::b200::ReadFromBinaryCSR).  ReadFromBinaryCOO reads on the host;
+// ReadFromBinaryCSR and read_matrix_market_csr sort the entries into a CSR on
+// the GPU (la_csr_read_binary_coo / la_csr_parse_matrix_market) and return
+// host vectors, as the reference's do.
+#include <istream>
+#include <iterator>
+#include <string>
+#include <utility>
+
+namespace utils {
+namespace b200 {
+
+// ReadFromBinaryCOO (utils.h:23-44): entries in file order; returns
+// {largest row + 1 - base, largest column + 1 - base}.
+template <typename IVEC, typename VVEC, typename IB>
+auto ReadFromBinaryCOO(const std::string &filename, IVEC &rows, IVEC &cols, VVEC &vals,
+                       const IB base) {
+  long long nnz = 0;
+  int m = 0, n = 0;
+  matrix_utils::b200::check(la_read_binary_coo(filename.c_str(), (int)base, &nnz, nullptr,
+                                               nullptr, nullptr, &m, &n),
+                            "la_read_binary_coo");
+  std::vector<int> r(nnz), c(nnz);
+  std::vector<double> v(nnz);
+  matrix_utils::b200::check(la_read_binary_coo(filename.c_str(), (int)base, &nnz, r.data(),
+                                               c.data(), v.data(), &m, &n),
+                            "la_read_binary_coo");
+  rows.assign(r.begin(), r.end());
+  cols.assign(c.begin(), c.end());
+  vals.assign(v.begin(), v.end());
+  using I = typename IVEC::value_type;
+  return std::make_pair((I)m, (I)n);
+}
+
+namespace detail {
+template <typename IVEC, typename VVEC>
+void download(la_csr_t A, IVEC &ai, IVEC &aj, VVEC &av) {
+  int n = 0, nnz = 0;
+  la_csr_info(A, &n, nullptr, &nnz, nullptr, nullptr);
+  std::vector<int> a(n + 1), j(nnz);
+  std::vector<double> v(nnz);
+  const la_status s = la_csr_download(A, a.data(), j.data(), v.data());
+  la_csr_destroy(A);
+  matrix_utils::b200::check(s, "la_csr_download");
+  ai.assign(a.begin(), a.end());
+  aj.assign(j.begin(), j.end());
+  av.assign(v.begin(), v.end());
+}
+} // namespace detail
+
+// ReadFromBinaryCSR (utils.h:46-91): rows sorted by (row, col), row pointers
+// with the file's base; returns {rows, cols} as ReadFromBinaryCOO does.
+template <typename IVEC, typename VVEC, typename IB>
+auto ReadFromBinaryCSR(const std::string &filename, IVEC &ai, IVEC &aj, VVEC &av,
+                       const IB base) {
+  la_csr_t A = nullptr;
+  matrix_utils::b200::check(la_csr_read_binary_coo(filename.c_str(), (int)base, 0, &A),
+                            "la_csr_read_binary_coo");
+  int m = 0, n = 0;
+  la_csr_info(A, &m, &n, nullptr, nullptr, nullptr);
+  detail::download(A, ai, aj, av);
+  using I = typename IVEC::value_type;
+  return std::make_pair((I)m, (I)n);
+}
+
+// read_matrix_market_csr (utils.h:93-132): a 0-based CSR (rows[nrows+1],
+// cols, values) from a Matrix Market coordinate stream.
+template <typename IVEC, typename VVEC>
+void read_matrix_market_csr(std::istream &instream, IVEC &rows, IVEC &cols, VVEC &values) {
+  const std::string text((std::istreambuf_iterator<char>(instream)),
+                         std::istreambuf_iterator<char>());
+  la_csr_t A = nullptr;
+  matrix_utils::b200::check(la_csr_parse_matrix_market(text.data(), text.size(), 0, &A),
+                            "la_csr_parse_matrix_market");
+  detail::download(A, rows, cols, values);
+}
+
+} // namespace b200
+} // namespace utils

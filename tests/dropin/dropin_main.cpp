@@ -4,16 +4,18 @@
 // tests/test_dropin.py compiles it with g++ against the header, links it to
 // liblab200.so and compares what it writes with the committed fixtures.
 //
-//   dropin_main <in.bin> <out.bin>
+//   dropin_main <in.bin> <out.bin> <coo.bin>
 // in.bin: int32 n, int32 nnz, ai[n+1], aj[nnz] (int32), av[nnz], x[n],
 //         y0[n] (double); a square FP64 CSR with base 0.
 // out.bin: records of (int32 kind: 0 int32 / 1 double, int64 count, data),
 // in the order written below.  Device results are written only when a GPU
 // is present; otherwise the status the device classes throw is recorded.
+// coo.bin: a file in ReadFromBinaryCOO's layout, base 1.
 #include "la_b200.hpp"
 
 #include <cstdint>
 #include <cstdio>
+#include <sstream>
 #include <vector>
 
 namespace m = matrix_utils::b200;
@@ -67,7 +69,7 @@ static void triangle(const Csr &A, bool lower, std::vector<int> &ai, std::vector
 }
 
 int main(int argc, char **argv) {
-  if (argc != 3)
+  if (argc != 4)
     return 2;
   FILE *in = std::fopen(argv[1], "rb");
   if (!in)
@@ -124,6 +126,17 @@ int main(int argc, char **argv) {
   put(p_aj);
   put(p_av);
 
+  // the binary COO reader, host only (utils.h:23-44)
+  auto coo_records = [&]() {
+    std::vector<int> cr, cc;
+    std::vector<double> cv;
+    auto mn = utils::b200::ReadFromBinaryCOO(std::string(argv[3]), cr, cc, cv, 1);
+    put(cr);
+    put(cc);
+    put(cv);
+    put(std::vector<int>{mn.first, mn.second});
+  };
+
   int sms = 0;
   if (la_device_sm_count(&sms) != LA_OK || sms == 0) {
     // no device: every device class must fail loudly, with no CPU fallback
@@ -135,10 +148,12 @@ int main(int argc, char **argv) {
       status = (int)e.status;
     }
     put(std::vector<int>{status});
+    coo_records();
     std::fclose(g_out);
     return 0;
   }
   put(std::vector<int>{-1});
+  coo_records();
 
   // SpMV: both forms and the SPMV<> adapter, y = 1.5 A x + 0.5 y0
   std::vector<double> y = y0;
@@ -184,6 +199,29 @@ int main(int argc, char **argv) {
   put(t);
   m::ForwardSubstitutionT(n, 0, u_ai.data(), u_aj.data(), u_av.data(), ones.data(), t.data());
   put(t);
+
+  // ReadFromBinaryCSR (utils.h:46-91) and read_matrix_market_csr
+  // (utils.h:93-132), built on the device
+  std::vector<int> bai, baj;
+  std::vector<double> bav;
+  auto bmn = utils::b200::ReadFromBinaryCSR(std::string(argv[3]), bai, baj, bav, 1);
+  put(bai);
+  put(baj);
+  put(bav);
+  put(std::vector<int>{bmn.first, bmn.second});
+  std::ostringstream mm;
+  mm.precision(17);
+  mm << "%%MatrixMarket matrix coordinate real general\n" << n << " " << n << " " << nnz << "\n";
+  for (int i = n - 1; i >= 0; i--) // rows in reverse: the reader sorts them
+    for (int k = A.ai[i]; k < A.ai[i + 1]; k++)
+      mm << i + 1 << " " << A.aj[k] + 1 << " " << A.av[k] << "\n";
+  std::istringstream in_mm(mm.str());
+  std::vector<int> mai, maj;
+  std::vector<double> mav;
+  utils::b200::read_matrix_market_csr(in_mm, mai, maj, mav);
+  put(mai);
+  put(maj);
+  put(mav);
   std::fclose(g_out);
   return 0;
 }

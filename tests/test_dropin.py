@@ -36,14 +36,14 @@ def dropin(lab, tmp_path_factory):
     return out
 
 
-def run(exe, tmp_path, n, ai, aj, av, x, y0):
+def run(exe, tmp_path, n, ai, aj, av, x, y0, coo):
     fin, fout = tmp_path / "in.bin", tmp_path / "out.bin"
     with open(fin, "wb") as f:
         f.write(struct.pack("<ii", n, int(ai[-1])))
         for a, dt in ((ai, np.int32), (aj, np.int32), (av, np.float64), (x, np.float64),
                       (y0, np.float64)):
             f.write(np.ascontiguousarray(a, dt).tobytes())
-    subprocess.run([str(exe), str(fin), str(fout)], check=True, timeout=300)
+    subprocess.run([str(exe), str(fin), str(fout), str(coo)], check=True, timeout=300)
     recs, buf, off = [], fout.read_bytes(), 0
     while off < len(buf):
         kind, count = struct.unpack_from("<iq", buf, off)
@@ -52,6 +52,13 @@ def run(exe, tmp_path, n, ai, aj, av, x, y0):
         recs.append(np.frombuffer(buf, dt, count, off).copy())
         off += sz * count
     return recs
+
+
+def coo_file(golden, tmp_path, nm="K"):
+    """One of the reference's own binary COO files (frozen bytes), base 1."""
+    p = tmp_path / f"{nm}.bin"
+    p.write_bytes(golden[f"bin_{nm}/bytes"].tobytes())
+    return p
 
 
 def cases(golden):
@@ -64,9 +71,16 @@ def test_dropin_host_steps(lab, dropin, golden, tmp_path):
     """Host functions through the C++ layer equal the reference's outputs;
     without a GPU the device classes throw LA_ERR_NO_DEVICE."""
     checked = 0
+    coo = coo_file(golden, tmp_path)
+    raw = np.frombuffer(coo.read_bytes(), np.dtype([("v", "<f8"), ("c", "<i4"), ("r", "<i4")]),
+                        offset=8)
     for name, n, ai, aj, av, x, y0 in cases(golden):
-        r = run(dropin, tmp_path, n, ai, aj, av, x, y0)
+        r = run(dropin, tmp_path, n, ai, aj, av, x, y0, coo)
         lv, ip, pf, last, kip, alld, diag, p_ai, p_aj, p_av, status = r[:11]
+        cr, cc, cv, cmn = r[11:15]  # utils::b200::ReadFromBinaryCOO, host
+        assert np.array_equal(cr, raw["r"]) and np.array_equal(cc, raw["c"])
+        assert np.array_equal(cv, raw["v"])
+        assert tuple(cmn) == tuple(golden["bin_K/base1_shape"])
         assert lv[0] == int(golden[f"{name}/topoL_levels"][0]), name
         assert np.array_equal(ip, golden[f"{name}/topoL_iperm"]), name
         assert np.array_equal(pf, golden[f"{name}/topoL_prefix"]), name
@@ -92,10 +106,19 @@ def test_dropin_device_classes(lab, orc, dropin, golden, tmp_path):
     substitutions; the free functions bit for bit."""
     P = orc.ptr
     checked = 0
+    coo = coo_file(golden, tmp_path)
     for name, n, ai, aj, av, x, y0 in cases(golden):
-        r = run(dropin, tmp_path, n, ai, aj, av, x, y0)
+        r = run(dropin, tmp_path, n, ai, aj, av, x, y0, coo)
         assert r[10][0] == -1
-        seg, alb, ad, lsol, usol, fwd, bwd, lfwd, lbwd, fwdt = r[11:21]
+        seg, alb, ad, lsol, usol, fwd, bwd, lfwd, lbwd, fwdt = r[15:25]
+        bai, baj, bav, bmn = r[25:29]  # utils::b200::ReadFromBinaryCSR
+        assert np.array_equal(bai, golden["bin_K/base1_ai"])
+        assert np.array_equal(baj, golden["bin_K/base1_aj"])
+        assert np.array_equal(bav, golden["bin_K/base1_av"])
+        assert tuple(bmn) == tuple(golden["bin_K/base1_shape"])
+        mai, maj, mav = r[29:32]  # utils::b200::read_matrix_market_csr
+        assert np.array_equal(mai, ai) and np.array_equal(maj, aj), name
+        assert np.array_equal(mav, av), name
         want = golden[f"{name}/spmv_serial"]
         for y in (seg, alb, ad):
             assert np.linalg.norm(y - want) <= 1e-13 * np.linalg.norm(want), name
