@@ -985,6 +985,17 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
     LA_TRY(P->ai.upload(eai.data(), sizeof(int) * eai.size()));
     LA_TRY(P->aj.upload(eaj.data(), sizeof(int) * eaj.size()));
   }
+  // Testing override (the partitioned kernel's bounded wait): the first row
+  // with a stored entry reads its own value through global memory instead,
+  // a value it publishes only after that read -- so the wait runs out after
+  // its 1 s bound and the solve reports LA_ERR_TIMEOUT.
+  if (const char *e = std::getenv("LA_TRSV_STALL_TEST"))
+    if (std::atoi(e) != 0)
+      for (int r = 0; r < n; r++)
+        if (ej[r] != kEmptySlot) {
+          ej[r] = erow[r];
+          break;
+        }
   LA_TRY(P->ej.upload(ej.data(), sizeof(int) * cells));
   LA_TRY(P->exec_row.upload(erow.data(), sizeof(int) * erow.size()));
   LA_TRY(P->pstart.upload(pstart.data(), sizeof(int) * pstart.size()));

@@ -73,10 +73,11 @@ def test_ic0_device_base1_and_breakdown(lab):
     want = lab.ICCLevelNumeric0(n, 0, ua, uj, uv)
     got = lab.FactorPlan("ic0", n, 1, ua + 1, uj + 1).factor(uv)
     assert np.array_equal(got, want)
-    # a negative pivot at row j0 (its diagonal made negative): reported there
+    # a negative pivot at row j0 (its diagonal shrunk below what its updates
+    # subtract): reported there; a shift large enough repairs it
     j0 = n // 3
     bad = uv.copy()
-    bad[ua[j0]] = -1.0
+    bad[ua[j0]] = 0.1
     with pytest.raises(lab.LAError):
         lab.ICCLevelNumeric0(n, 0, ua, uj, bad)
     plan = lab.FactorPlan("ic0", n, 0, ua, uj)

@@ -176,6 +176,42 @@ def test_trsv_bounded_wait_reports_timeout(lab, orc):
     assert np.array_equal(x.cpu().numpy(), ref)
 
 
+def test_trsv_partitioned_bounded_wait_reports_timeout(lab, orc, monkeypatch):
+    """The partitioned schedule's abort path: with LA_TRSV_STALL_TEST one row
+    waits for its own, never published value, so its wait runs out after the
+    1 s bound; every thread of every part leaves (the CTA-wide abort vote),
+    the solve returns LA_ERR_TIMEOUT without a fault or hang, and the next
+    plan on the same context solves correctly."""
+    import time
+    from linearalgebra_b200 import gen
+    n, ai, aj, av = gen.laplacian_3d(24)
+    _, (t_ai, t_aj, t_av), _, d = _ic_factor_rcm(lab, n, ai, aj, av)
+    b = torch.as_tensor(np.random.default_rng(4).uniform(-1, 1, n)).cuda()
+    x = torch.empty_like(b)
+    monkeypatch.setenv("LA_TRSV_SCHEDULE", "parts")
+    for dt in (np.float64, np.float32):
+        monkeypatch.setenv("LA_TRSV_STALL_TEST", "1")
+        bad = lab.OptimizedTriangularSolve("L", dtype=dt).analysis(n, 0, t_ai, t_aj, t_av, d)
+        assert bad.schedule()[0] == "parts"
+        bb = b.to(torch.float64 if dt == np.float64 else torch.float32)
+        xx = torch.empty_like(bb)
+        t0 = time.time()
+        with pytest.raises(lab.LAError) as e:
+            bad(bb, xx)
+        assert e.value.name == "LA_ERR_TIMEOUT"
+        assert time.time() - t0 < 30
+        monkeypatch.delenv("LA_TRSV_STALL_TEST")
+    good = lab.OptimizedTriangularSolve("L").analysis(n, 0, t_ai, t_aj, t_av, d)
+    good(b, x)
+    lv, ip, pf = good.levels()
+    ref = np.zeros(n)
+    P = orc.ptr
+    bn = b.cpu().numpy()
+    orc.port().oracle_level_solve(lv, P(ip), P(pf), 0, P(t_ai), P(t_aj), P(t_av), P(d),
+                                  P(bn), P(ref))
+    assert np.array_equal(x.cpu().numpy(), ref)
+
+
 def test_trsv_levels_validation(lab):
     ai, aj, av = _chain(8)
     with pytest.raises(lab.LAError):  # not a permutation
