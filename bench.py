@@ -274,6 +274,10 @@ def extras(la, torch, peak):
     out["pcg"], mats = pcg_case(la, torch, "C3_lap3d_128_rcm", gen.laplacian_3d(128))
     out["pcg_c5"], mats_c5 = pcg_case(la, torch, "C5_aniso7_192_rcm", gen.aniso7(192, seed=0))
     out["adjoint_c4"] = adjoint_case(la, torch, peak)
+    try:
+        out["ingest"] = ingest_case(la)
+    except Exception as e:  # reported, never silently replaced
+        out["ingest"] = {"error": str(e)}
     return out, {"pcg": mats, "pcg_c5": mats_c5}
 
 
@@ -335,6 +339,45 @@ def adjoint_case(la, torch, peak):
             "sddmm_pattern": {"us": sd_ms * 1e3, "GB/s": sddmm_b / (sd_ms * 1e-3) / 1e9,
                               "frac_of_measured_hbm": sddmm_b / (sd_ms * 1e-3) / 1e9 / peak},
             "timing": "back to back after one warm-up call; inputs larger than L2 except x/g"}
+
+
+def ingest_case(la):
+    """Ingest (utils/utils.h:23-91): the 128^3 Laplacian's 14.6M entries,
+    shuffled, written in ReadFromBinaryCOO's layout (base 1), read into a
+    device CSR by ReadFromBinaryCSR's drop-in -- against the reference's own
+    ReadFromBinaryCSR (compiled in place) on the host; the CSRs compared."""
+    import tempfile
+    import oracle
+    from linearalgebra_b200 import gen
+    n, ai, aj, av = gen.laplacian_3d(128)
+    rows = np.repeat(np.arange(n, dtype=np.int32), np.diff(ai))
+    order = np.random.default_rng(0).permutation(len(aj))
+    rec = np.zeros(len(aj), np.dtype([("v", "<f8"), ("c", "<i4"), ("r", "<i4")]))
+    rec["r"], rec["c"], rec["v"] = rows[order] + 1, aj[order] + 1, av[order]
+    with tempfile.TemporaryDirectory() as d:
+        path = Path(d) / "lap3d_128.bin"
+        with open(path, "wb") as f:
+            f.write(np.int64(len(rec)).tobytes())
+            f.write(rec.tobytes())
+        la.ReadFromBinaryCSR(path, 1)  # warm
+        t0 = time.perf_counter()
+        A = la.ReadFromBinaryCSR(path, 1)
+        t_dev = time.perf_counter() - t0
+        out = {"config": "lap3d_128 shuffled, 14,581,760 entries, base 1",
+               "file_bytes": path.stat().st_size, "device_csr_s": t_dev}
+        rf = oracle.ref()
+        if rf is not None:
+            P = oracle.ptr
+            m_, n_ = np.zeros(1, np.int32), np.zeros(1, np.int32)
+            rai, raj, rav = np.zeros(n + 1, np.int32), np.zeros(len(aj), np.int32), np.zeros(len(aj))
+            t0 = time.perf_counter()
+            rf.la_ref_read_binary_csr(str(path).encode(), 1, P(rai), P(raj), P(rav), P(m_), P(n_))
+            out["reference_host_s"] = time.perf_counter() - t0
+            g = A.host
+            out["identical_to_reference"] = bool(np.array_equal(g[0], rai) and
+                                                 np.array_equal(g[1], raj) and
+                                                 np.array_equal(g[2], rav))
+    return out
 
 
 def pcg_iteration_bytes(n, nnz, nnz_tri, vb):

@@ -476,12 +476,11 @@ la_status la_pcg_solve_host(la_pcg_t s, const double *b, double *x,
 la_status la_pcg_adjoint(la_pcg_t s, const double *g, const double *u,
                          double *dl_db, double *dl_dvalues, double rtol,
                          int maxit, la_pcg_info *info, la_stream_t stream);
-/* Whether the solver runs each iteration's vector work fused (no reference
- * counterpart): *fused = 1 when the dot products, the x / r update and the
- * direction update run in two cooperative kernels per iteration that finish
- * their own dot products, 0 for separate dot and update launches (set
- * LA_PCG_FUSED=0 in the environment before la_pcg_create; the iterates are
- * the same bit for bit). */
+/* Whether the solver fuses the step after each SpMV (no reference
+ * counterpart): *fused = 1 when (p, A p), alpha, the x / r update and
+ * ||r||^2 run in one cooperative kernel that finishes its own dot products,
+ * 0 for separate dot and update launches (set LA_PCG_FUSED=0 in the
+ * environment before la_pcg_create; the iterates are the same bit for bit). */
 la_status la_pcg_fused(la_pcg_t s, int *fused);
 la_status la_pcg_destroy(la_pcg_t s);
 

@@ -23,8 +23,8 @@ la_status spmv_noalloc(la_spmv_kind kind, int n, int nnz, int base, const int *a
 la_status spmv_plan_build(la_spmv_plan_t P);
 la_status spmv_host_chunked(la_spmv_plan_t P, double alpha, const double *x, double beta,
                             double *y);
-la_status trsv_launch(la_trsv_plan_t P, const void *b, void *x, cudaStream_t st,
-                      bool prefilled = false);
+la_status trsv_launch(la_trsv_plan_t P, const void *b, void *x,
+                      cudaStream_t st);
 la_status trsv_build(la_trsv_plan_t P, const int *ai, const int *aj,
                      const double *av, const double *diag, const int *iperm = nullptr,
                      const int *prefix = nullptr, int nlevels = 0);

@@ -51,6 +51,7 @@ namespace {
 constexpr int kFactorThreads = 256;
 constexpr int kFactorChunk = 32;
 constexpr unsigned long long kFactorWaitNs = 1000000000ull; // 1 s
+constexpr int kGroup = 8; // flags polled / pair sources loaded together
 
 enum FactorKind { kIC0 = 0, kILU0 = 1 };
 
@@ -74,6 +75,13 @@ void symbolic_ic0(int n, int base, const int *ai, const int *aj, Symbolic &S) {
   S.uptr.assign(n + 1, 0);
   S.pptr.assign(1, 0);
   S.diag.resize(n);
+  // one update per strict upper entry; each holds at least its diagonal pair
+  const size_t upd = (size_t)(ai[n] - base) - (size_t)n;
+  S.uk.reserve(upd);
+  S.us.reserve(upd);
+  S.pptr.reserve(upd + 1);
+  S.ptgt.reserve(3 * upd);
+  S.psrc.reserve(3 * upd);
   for (int j = 0; j < n; j++) {
     const int rs = ai[j] - base, re = ai[j + 1] - base;
     S.diag[j] = rs;
@@ -88,7 +96,6 @@ void symbolic_ic0(int n, int base, const int *ai, const int *aj, Symbolic &S) {
       }
       S.uk.push_back(k);
       S.us.push_back(ck0);
-      S.upiv.push_back(0);
       for (int p = rs, ck = ck0; ck < ke && p < re;) {
         if (aj[ck] == aj[p]) {
           S.ptgt.push_back(p++);
@@ -196,29 +203,67 @@ __global__ void __launch_bounds__(kFactorThreads)
     if (KIND == kIC0)
       v[rs] = __dmul_rn(__ldg(vin + rs), diag_scale); // the (1 + omega) shift
     bool gave_up = false;
-    for (int u = __ldg(uptr + j); u < __ldg(uptr + j + 1) && !gave_up; u++) {
-      const int k = __ldg(uk + u);
-      const unsigned long long t0 = factor_ns();
-      for (unsigned pass = 1; ld_acquire(done + k) == 0; pass++)
-        if ((pass & 63u) == 0u &&
+    const int u0 = __ldg(uptr + j), u1 = __ldg(uptr + j + 1);
+    const unsigned long long t0 = factor_ns();
+    // every source row published: their flags polled kGroup at a time
+    for (int g = u0; g < u1 && !gave_up; g += kGroup) {
+      int kk[kGroup];
+      unsigned pending = 0;
+#pragma unroll
+      for (int q = 0; q < kGroup; q++)
+        if (g + q < u1) {
+          kk[q] = __ldg(uk + g + q);
+          pending |= 1u << q;
+        }
+      for (unsigned pass = 1; pending; pass++) {
+        int f[kGroup];
+#pragma unroll
+        for (int q = 0; q < kGroup; q++)
+          f[q] = (pending >> q) & 1u ? ld_acquire(done + kk[q]) : 1;
+#pragma unroll
+        for (int q = 0; q < kGroup; q++)
+          if (f[q] != 0)
+            pending &= ~(1u << q);
+        if (pending && (pass & 63u) == 0u &&
             (ld_acquire(state + 1) != 0 || factor_ns() - t0 > kFactorWaitNs)) {
           atomicExch(state + 1, 1);
           gave_up = true;
           break;
         }
-      if (gave_up)
-        break;
-      double s;
-      if (KIND == kIC0) {
-        s = __ldcg(v + __ldg(us + u)); // U_kj, final
-      } else {
-        const int own = __ldg(us + u); // L_jk = a_jk / u_kk
-        s = __ddiv_rn(v[own], __ldcg(v + __ldg(upiv + u)));
-        v[own] = s;
       }
-      for (int e = __ldg(pptr + u); e < __ldg(pptr + u + 1); e++) {
-        const int t = __ldg(ptgt + e);
-        v[t] = __dsub_rn(v[t], __dmul_rn(s, __ldcg(v + __ldg(psrc + e))));
+    }
+    // the updates in their order; an update's scalar operand and its pairs'
+    // sources (final values of its source row) are loaded together, kGroup
+    // pairs at a time, then applied in order -- the same operations in the
+    // same order as one at a time
+    for (int u = u0; u < u1 && !gave_up; u++) {
+      const int e0 = __ldg(pptr + u), e1 = __ldg(pptr + u + 1);
+      const double sv = __ldcg(v + __ldg(KIND == kIC0 ? us + u : upiv + u));
+      double s = 0.0;
+      for (int eg = e0; eg == e0 || eg < e1; eg += kGroup) {
+        int tg[kGroup];
+        double src[kGroup];
+#pragma unroll
+        for (int q = 0; q < kGroup; q++)
+          if (eg + q < e1) {
+            tg[q] = __ldg(ptgt + eg + q);
+            src[q] = __ldcg(v + __ldg(psrc + eg + q));
+          }
+        if (eg == e0) {
+          if (KIND == kIC0) {
+            s = sv; // U_kj, final
+          } else {
+            const int own = __ldg(us + u); // L_jk = a_jk / u_kk
+            s = __ddiv_rn(v[own], sv);
+            v[own] = s;
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < kGroup; q++)
+          if (eg + q < e1)
+            v[tg[q]] = __dsub_rn(v[tg[q]], __dmul_rn(s, src[q]));
+        if (eg + kGroup >= e1)
+          break;
       }
     }
     if (gave_up) // the row stays unpublished; the warp stops at its next claim

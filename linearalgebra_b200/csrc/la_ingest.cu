@@ -48,14 +48,18 @@ constexpr int kWarps = kSortThreads / 32;
 
 // is the input already ordered by (row, col)?  flag = 1 if some neighbour
 // pair is out of order
+// (one store per warp that saw a pair out of order: a store per pair made
+// every thread of a shuffled input write the same word)
 __global__ void order_check_kernel(const long long nnz, const unsigned *row, const unsigned *col,
                                    int *flag) {
+  bool out_of_order = false;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i + 1 < nnz;
        i += (long long)gridDim.x * blockDim.x) {
     const unsigned r0 = row[i], r1 = row[i + 1];
-    if (r0 > r1 || (r0 == r1 && col[i] > col[i + 1]))
-      *flag = 1;
+    out_of_order |= r0 > r1 || (r0 == r1 && col[i] > col[i + 1]);
   }
+  if (__any_sync(0xffffffffu, out_of_order) && (threadIdx.x & 31) == 0)
+    *flag = 1;
 }
 
 __device__ __forceinline__ int digit_of(unsigned key, int shift) { return (key >> shift) & 255; }

@@ -30,6 +30,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr unsigned long long kWaitNs = 1000000000ull;
+constexpr int kGroup = 8; // dependencies polled together
 
 __device__ __forceinline__ unsigned long long level_ns() {
   unsigned long long t;
@@ -63,21 +64,44 @@ __global__ void __launch_bounds__(kThreads)
     const int i = UPPER ? n - 1 - k : k;
     int d = 0;
     bool gave_up = false;
-    for (int e = __ldg(ai + i) - base; e < __ldg(ai + i + 1) - base && !gave_up; e++) {
-      const int j = __ldg(aj + e) - base;
-      if (UPPER ? j <= i : j >= i) { // not a dependency on an earlier row
-        atomicExch(state + 2, 1);
-        continue;
+    // the row's dependencies kGroup at a time: their depths loaded together,
+    // the unpublished ones re-polled until they arrive
+    const int e0 = __ldg(ai + i) - base, e1 = __ldg(ai + i + 1) - base;
+    const unsigned long long t0 = level_ns();
+    for (int g = e0; g < e1 && !gave_up; g += kGroup) {
+      int jj[kGroup];
+      unsigned pending = 0;
+#pragma unroll
+      for (int q = 0; q < kGroup; q++) {
+        jj[q] = -1;
+        if (g + q < e1) {
+          const int j = __ldg(aj + g + q) - base;
+          if (UPPER ? j <= i : j >= i) // not a dependency on an earlier row
+            atomicExch(state + 2, 1);
+          else {
+            jj[q] = j;
+            pending |= 1u << q;
+          }
+        }
       }
-      int dj;
-      const unsigned long long t0 = level_ns();
-      for (unsigned pass = 1; (dj = ld_acq(depth + j)) < 0; pass++)
-        if ((pass & 63u) == 0u && (ld_acq(state + 1) != 0 || level_ns() - t0 > kWaitNs)) {
+      for (unsigned pass = 1; pending; pass++) {
+        int dq[kGroup];
+#pragma unroll
+        for (int q = 0; q < kGroup; q++)
+          dq[q] = (pending >> q) & 1u ? ld_acq(depth + jj[q]) : -1;
+#pragma unroll
+        for (int q = 0; q < kGroup; q++)
+          if (((pending >> q) & 1u) && dq[q] >= 0) {
+            d = max(d, dq[q] + 1);
+            pending &= ~(1u << q);
+          }
+        if (pending && (pass & 63u) == 0u &&
+            (ld_acq(state + 1) != 0 || level_ns() - t0 > kWaitNs)) {
           atomicExch(state + 1, 1);
           gave_up = true;
           break;
         }
-      d = max(d, dj + 1);
+      }
     }
     if (gave_up)
       continue;

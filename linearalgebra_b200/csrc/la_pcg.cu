@@ -32,8 +32,8 @@ namespace la {
 la_status spmv_launch(la_spmv_plan_t P, double alpha, const void *x,
                       double beta, void *y, const void *yin, la_dtype vd,
                       cudaStream_t st);
-la_status trsv_launch(la_trsv_plan_t P, const void *b, void *x, cudaStream_t st,
-                      bool prefilled = false);
+la_status trsv_launch(la_trsv_plan_t P, const void *b, void *x,
+                      cudaStream_t st);
 la_status trsv_check(la_trsv_plan_t P, cudaStream_t st);
 la_status trsv_build(la_trsv_plan_t P, const int *ai, const int *aj,
                      const double *av, const double *diag, const int *iperm = nullptr,
@@ -167,19 +167,26 @@ __global__ void p_update_kernel(const int n, X *p, const X *z,
 }
 
 // ------------------------------------------------------ fused iteration
-// Two cooperative kernels carry all of an iteration's vector work (the role
-// of the RCI loop's dot products and axpys, mkl_solver.cpp:190-238):
-//   pcg_update_kernel:    alpha = (r, z) / (p, q); x += alpha p; r -= alpha q;
-//                         ||r||^2; the next solves' outputs filled with the
-//                         sentinel they wait on;
-//   pcg_direction_kernel: beta = (r, z)_new / (r, z)_old; p' = z + beta p.
-// A dot product ends in a grid-wide barrier, after which every block adds the
-// block totals itself, in block order, so no extra launch is needed to
-// finish it.  Grid, element assignment, per-thread order and reduction tree
-// are those of dot_kernel, and each update is the same single fused
-// multiply-add as in xr_update_kernel / p_update_kernel: the iterates are
-// bit-identical to the unfused sequence's.  Launched cooperatively (all
-// blocks resident); the barrier's wait is bounded by the global timer.
+// One cooperative kernel carries the step after the SpMV (the role of the
+// RCI loop's dot products and axpys there, mkl_solver.cpp:190-238):
+//   pcg_update_kernel: alpha = (r, z) / (p, q); x += alpha p; r -= alpha q;
+//                      ||r||^2 -- three launches of the unfused sequence.
+// Its first dot product ends in a grid-wide barrier, after which every block
+// adds the block totals itself, in block order, so no extra launch finishes
+// it; the last one is finished by the last block, as in dot_kernel.  Grid,
+// element assignment, per-thread order and reduction tree are dot_kernel's,
+// and each update is the same single fused multiply-add as in
+// xr_update_kernel: the iterates are bit-identical to the unfused sequence's.
+// Launched cooperatively (all blocks resident); the barrier's wait is bounded
+// by the global timer.  Measured on the 128^3 workload (us per iteration,
+// events between launches): this kernel 54.0 against 56.3 for the three it
+// replaces.  Two further fusions measured slower and are not used: the
+// direction step as one cooperative kernel (beta and p = z + beta p after a
+// grid barrier: 38.2 against 28.3 for dot_kernel + p_update_kernel), and the
+// solves' sentinel fill folded into this kernel (the partitioned solves then
+// took 470 / 475 instead of 454 / 454 -- their outputs are no longer hot in
+// L2 when written amid this kernel's other traffic, where a memset right
+// before each solve leaves them there).
 constexpr unsigned long long kBarrierNs = 1000000000ull; // 1 s
 
 __device__ __forceinline__ unsigned long long pcg_global_ns() {
@@ -214,20 +221,12 @@ __device__ void grid_barrier(unsigned *bar) {
   __syncthreads();
 }
 
-template <typename X> struct AllOnes;
-template <> struct AllOnes<double> {
-  static __device__ __forceinline__ double v() { return __longlong_as_double(-1ll); }
-};
-template <> struct AllOnes<float> {
-  static __device__ __forceinline__ float v() { return __int_as_float(-1); }
-};
-
 // partials: 2 * gridDim.x doubles ((p, q) totals, then ||r||^2 totals).
 template <typename X>
 __global__ void __launch_bounds__(kDotThreads)
     pcg_update_kernel(const int n, X *x, X *r, const X *__restrict__ p,
-                      const X *__restrict__ q, X *t_fill, X *z_fill, double *partials,
-                      unsigned *ticket, double *scal, unsigned *bar) {
+                      const X *__restrict__ q, double *partials, unsigned *ticket,
+                      double *scal, unsigned *bar) {
   __shared__ double red[kDotThreads / 32];
   __shared__ double alpha_s;
   __shared__ bool last;
@@ -248,15 +247,12 @@ __global__ void __launch_bounds__(kDotThreads)
   }
   __syncthreads();
   const double al = alpha_s;
-  const X sentinel = AllOnes<X>::v();
   s = 0.0;
   auto step = [&](int i, X pi, X qi, X xi, X ri) {
     x[i] = X(__fma_rn(al, double(pi), double(xi)));
     const X rn = X(__fma_rn(-al, double(qi), double(ri)));
     r[i] = rn;
     s = __fma_rn(double(rn), double(rn), s);
-    t_fill[i] = sentinel;
-    z_fill[i] = sentinel;
   };
   int i = i0;
   for (; i + 3 * stride < n; i += 4 * stride) { // loads first, then the k-order steps
@@ -287,49 +283,6 @@ __global__ void __launch_bounds__(kDotThreads)
   __threadfence();
   scal[S_DOT] = sum_partials(partials + gridDim.x, gridDim.x);
   *ticket = 0u;
-}
-
-// pn = z + beta p (pn may equal p); beta and the new (r, z) into scal.
-template <typename X>
-__global__ void __launch_bounds__(kDotThreads)
-    pcg_direction_kernel(const int n, X *pn, const X *p, const X *__restrict__ r,
-                         const X *__restrict__ z, double *partials, double *scal,
-                         unsigned *bar) {
-  __shared__ double red[kDotThreads / 32];
-  __shared__ double beta_s;
-  const int stride = gridDim.x * kDotThreads, i0 = blockIdx.x * kDotThreads + threadIdx.x;
-  const double rz_old = scal[S_RZ]; // read before block 0 replaces it
-  const double s = thread_dot(n, r, z);
-  const double bt = block_sum(s, red);
-  if (threadIdx.x == 0)
-    partials[blockIdx.x] = bt;
-  grid_barrier(bar);
-  if (threadIdx.x == 0) {
-    const double rz = sum_partials(partials, gridDim.x);
-    const double be = rz / rz_old;
-    beta_s = be;
-    if (blockIdx.x == 0) {
-      scal[S_BETA] = be;
-      scal[S_RZ0] = rz_old;
-      scal[S_RZ] = rz;
-    }
-  }
-  __syncthreads();
-  const double be = beta_s;
-  int i = i0;
-  for (; i + 3 * stride < n; i += 4 * stride) {
-    X pv[4], zv[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      pv[k] = p[i + k * stride];
-      zv[k] = z[i + k * stride];
-    }
-#pragma unroll
-    for (int k = 0; k < 4; k++)
-      pn[i + k * stride] = X(__fma_rn(be, double(pv[k]), double(zv[k])));
-  }
-  for (; i < n; i += stride)
-    pn[i] = X(__fma_rn(be, double(p[i]), double(z[i])));
 }
 
 // out = X(scale * in)
@@ -375,25 +328,12 @@ la_status dot(la_pcg_t S, const XA *a, const XB *b, int op, cudaStream_t st) {
 }
 
 template <typename X>
-la_status fused_update(la_pcg_t S, X *x, X *r, const X *p, const X *q, X *t, X *z,
-                       cudaStream_t st) {
+la_status fused_update(la_pcg_t S, X *x, X *r, const X *p, const X *q, cudaStream_t st) {
   int n = S->n;
   double *partials = S->partials.as<double>(), *scal = S->scal.as<double>();
   unsigned *ticket = S->ticket.as<unsigned>(), *bar = S->bar.as<unsigned>();
-  void *args[] = {&n, &x, &r, &p, &q, &t, &z, &partials, &ticket, &scal, &bar};
+  void *args[] = {&n, &x, &r, &p, &q, &partials, &ticket, &scal, &bar};
   LA_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)pcg_update_kernel<X>,
-                                          dim3(S->dot_blocks), dim3(kDotThreads), args, 0, st));
-  return LA_OK;
-}
-
-template <typename X>
-la_status fused_direction(la_pcg_t S, X *pn, const X *p, const X *r, const X *z,
-                          cudaStream_t st) {
-  int n = S->n;
-  double *partials = S->partials.as<double>(), *scal = S->scal.as<double>();
-  unsigned *bar = S->bar.as<unsigned>();
-  void *args[] = {&n, &pn, &p, &r, &z, &partials, &scal, &bar};
-  LA_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)pcg_direction_kernel<X>,
                                           dim3(S->dot_blocks), dim3(kDotThreads), args, 0, st));
   return LA_OK;
 }
@@ -463,7 +403,7 @@ la_status pcg_run(la_pcg_t S, const X *rhs, X *y, X *r, X *z, X *p, X *q,
   for (int it = 1; it <= maxit; it++) {
     LA_TRY(spmv_launch(S->Ap, 1.0, p, 0.0, q, q, vd, st));
     if (S->fused) {
-      LA_TRY(fused_update<X>(S, y, r, p, q, t, z, st));
+      LA_TRY(fused_update<X>(S, y, r, p, q, st));
     } else {
       LA_TRY(dot(S, p, q, OP_ALPHA, st));
       xr_update_kernel<X><<<g, 256, 0, st>>>(n, y, r, p, q, S->scal.as<double>());
@@ -476,14 +416,10 @@ la_status pcg_run(la_pcg_t S, const X *rhs, X *y, X *r, X *z, X *p, X *q,
     LA_CUDA_TRY(cudaMemcpyAsync(S->h_rr, S->scal.as<double>() + S_DOT, sizeof(double),
                                 cudaMemcpyDeviceToHost, st));
     LA_CUDA_TRY(cudaEventRecord(S->ev_rr, st));
-    LA_TRY(trsv_launch(S->L, r, t, st, S->fused));
-    LA_TRY(trsv_launch(S->U, t, z, st, S->fused));
-    if (S->fused) {
-      LA_TRY(fused_direction<X>(S, p, p, r, z, st));
-    } else {
-      LA_TRY(dot(S, r, z, OP_BETA, st));
-      p_update_kernel<X><<<g, 256, 0, st>>>(n, p, z, S->scal.as<double>());
-    }
+    LA_TRY(trsv_launch(S->L, r, t, st));
+    LA_TRY(trsv_launch(S->U, t, z, st));
+    LA_TRY(dot(S, r, z, OP_BETA, st));
+    p_update_kernel<X><<<g, 256, 0, st>>>(n, p, z, S->scal.as<double>());
     LA_CUDA_TRY(cudaEventSynchronize(S->ev_rr));
     const double rr = *S->h_rr;
     *iters = it;
@@ -545,13 +481,12 @@ la_status pcg_mixed(la_pcg_t S, const double *b, double *x, double bn, double rt
   for (it = 1; it <= maxit; it++) {
     LA_TRY(spmv_launch(S->Ap, 1.0, p32, 0.0, q32, q32, LA_F32, st));
     if (S->fused) {
-      LA_TRY(fused_update<float>(S, d32, r32, p32, q32, t32, z32, st));
+      LA_TRY(fused_update<float>(S, d32, r32, p32, q32, st));
     } else {
       LA_TRY(dot(S, p32, q32, OP_ALPHA, st));
       xr_update_kernel<float><<<g, 256, 0, st>>>(n, d32, r32, p32, q32, S->scal.as<double>());
       LA_TRY(dot(S, r32, r32, OP_STORE, st));
     }
-    bool filled = S->fused; // t32 / z32 hold the solves' sentinel
     // As in pcg_run: ||r||^2 travels to the host while the next step's
     // preconditioner and direction are queued -- when the last residual was
     // well above the reliable-update threshold, so that no update is likely
@@ -564,15 +499,10 @@ la_status pcg_mixed(la_pcg_t S, const double *b, double *x, double bn, double rt
     LA_CUDA_TRY(cudaEventRecord(S->ev_rr, st));
     const bool ahead = rn_prev > 0.13 * rmax && rn_prev > 2.0 * rtol * bn;
     auto precondition = [&]() -> la_status {
-      LA_TRY(trsv_launch(S->L, r32, t32, st, filled));
-      LA_TRY(trsv_launch(S->U, t32, z32, st, filled));
-      filled = false;
-      if (S->fused) {
-        LA_TRY(fused_direction<float>(S, pn32, p32, r32, z32, st));
-      } else {
-        LA_TRY(dot(S, r32, z32, OP_BETA, st));
-        p_next_kernel<float><<<g, 256, 0, st>>>(n, pn32, p32, z32, S->scal.as<double>());
-      }
+      LA_TRY(trsv_launch(S->L, r32, t32, st));
+      LA_TRY(trsv_launch(S->U, t32, z32, st));
+      LA_TRY(dot(S, r32, z32, OP_BETA, st));
+      p_next_kernel<float><<<g, 256, 0, st>>>(n, pn32, p32, z32, S->scal.as<double>());
       return LA_OK;
     };
     if (ahead)
@@ -708,9 +638,7 @@ la_status pcg_create(la_csr_t A, const int *u_ai, const int *u_aj,
     S->fused = std::atoi(e) != 0;
   if (S->fused) {
     const void *fns[] = {(const void *)pcg_update_kernel<double>,
-                         (const void *)pcg_update_kernel<float>,
-                         (const void *)pcg_direction_kernel<double>,
-                         (const void *)pcg_direction_kernel<float>};
+                         (const void *)pcg_update_kernel<float>};
     for (const void *f : fns) {
       int per_sm = 0;
       if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, kDotThreads, 0) !=

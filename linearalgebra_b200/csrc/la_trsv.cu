@@ -645,14 +645,11 @@ cudaError_t launch_parts(la_trsv_plan_t P, const X *b, X *x, cudaStream_t st) {
   }
 }
 
-// prefilled: x already holds the all-ones sentinel (a caller that wrote it
-// in a pass of its own, e.g. the PCG update kernel), so no memset is issued.
 template <typename V, typename X>
-la_status launch_typed(la_trsv_plan_t P, const X *b, X *x, cudaStream_t st, bool prefilled) {
+la_status launch_typed(la_trsv_plan_t P, const X *b, X *x, cudaStream_t st) {
   if (P->n == 0)
     return LA_OK;
-  if (!prefilled)
-    LA_CUDA_TRY(cudaMemsetAsync(x, 0xff, sizeof(X) * (size_t)P->n, st));
+  LA_CUDA_TRY(cudaMemsetAsync(x, 0xff, sizeof(X) * (size_t)P->n, st));
   if (P->sched == 1) {
     const cudaError_t e = P->unit ? launch_parts<V, X, true>(P, b, x, st)
                                   : launch_parts<V, X, false>(P, b, x, st);
@@ -706,11 +703,11 @@ template <typename V, typename X> int grid_for(int nchunks, int kd) {
 
 } // namespace
 
-la_status trsv_launch(la_trsv_plan_t P, const void *b, void *x, cudaStream_t st,
-                      bool prefilled) {
+la_status trsv_launch(la_trsv_plan_t P, const void *b, void *x,
+                      cudaStream_t st) {
   if (P->dtype == LA_F64)
-    return launch_typed<double, double>(P, (const double *)b, (double *)x, st, prefilled);
-  return launch_typed<float, float>(P, (const float *)b, (float *)x, st, prefilled);
+    return launch_typed<double, double>(P, (const double *)b, (double *)x, st);
+  return launch_typed<float, float>(P, (const float *)b, (float *)x, st);
 }
 
 // The plans of one preconditioner (L and U = L^T, FP64 and FP32) share one
