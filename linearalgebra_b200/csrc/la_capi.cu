@@ -507,16 +507,15 @@ la_status la_rcm(int n, int base, const int *ai, const int *aj, int *iperm,
 
 la_status la_rcm_device(int n, int base, const int *ai, const int *aj, int *iperm,
                         int *perm) {
-  LA_CHECK_ARG(ai && iperm && perm && n >= 0, "arguments");
-  const int nnz = ai[n] - base;
-  std::vector<int> tai(n + 1), taj(std::max(nnz, 1));
-  transpose(n, n, base, ai, aj, nullptr, tai.data(), taj.data(), nullptr);
-  if (std::memcmp(tai.data(), ai, sizeof(int) * (n + 1)) != 0 ||
-      std::memcmp(taj.data(), aj, sizeof(int) * nnz) != 0) {
-    set_error("la_rcm_device needs a structurally symmetric pattern");
-    return LA_ERR_INVALID_ARG;
-  }
+  LA_CHECK_ARG(ai && iperm && perm && n >= 0 && (base == 0 || base == 1), "arguments");
+  LA_CHECK_ARG(ai[n] - base == 0 || aj, "aj");
+  if (n == 0)
+    return LA_OK;
   LA_TRY(require_device());
+  bool handled = false; // pattern checked on the device; connected: ordered there too
+  LA_TRY(rcm_device_connected(n, base, ai, aj, iperm, perm, &handled));
+  if (handled)
+    return LA_OK;
   return rcm(n, base, ai, aj, iperm, perm, true);
 }
 

@@ -127,6 +127,8 @@ RcmDevice *rcm_device_create(int n, int base, const int *ai, const int *aj, cons
                              la_status *st);
 void rcm_device_destroy(RcmDevice *D);
 la_status rcm_device_component(RcmDevice *D, const int *members, int size, int *out);
+la_status rcm_device_connected(int n, int base, const int *ai, const int *aj, int *iperm,
+                               int *perm, bool *handled);
 la_status rcm(int n, int base, const int *ai, const int *aj, int *iperm, int *perm,
               bool device = false);
 // Row partition for the partitioned triangular solve (la_partition.cpp):

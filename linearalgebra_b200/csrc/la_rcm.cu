@@ -357,3 +357,105 @@ la_status rcm_device_component(RcmDevice *D, const int *members, int size, int *
 }
 
 } // namespace la
+
+namespace la {
+namespace {
+
+// pattern check on the device: columns in range, rows non-decreasing, and
+// every entry (j, i) stored as often in row j as (i, j) is in row i -- the
+// condition the host's transpose comparison tests.  flag = 1 if it fails.
+__global__ void symmetric_check_kernel(const int n, const int base, const int *__restrict__ ai,
+                                       const int *__restrict__ aj, int *flag) {
+  bool bad = false;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int a = __ldg(ai + i) - base, e = __ldg(ai + i + 1) - base;
+    for (int k = a; k < e && !bad; k++) {
+      const int j = __ldg(aj + k) - base;
+      if (j < 0 || j >= n || (k > a && __ldg(aj + k - 1) > __ldg(aj + k))) {
+        bad = true;
+        break;
+      }
+      if (k > a && __ldg(aj + k - 1) == __ldg(aj + k))
+        continue; // a run of equal entries is counted at its first
+      int run = 1;
+      while (k + run < e && __ldg(aj + k + run) == __ldg(aj + k))
+        run++;
+      // count i in row j (non-decreasing: lower / upper bound)
+      int lo = __ldg(ai + j) - base, hi = __ldg(ai + j + 1) - base;
+      int l = lo, h = hi;
+      while (l < h) {
+        const int m = (l + h) >> 1;
+        if (__ldg(aj + m) - base < i)
+          l = m + 1;
+        else
+          h = m;
+      }
+      int u = l;
+      while (u < hi && __ldg(aj + u) - base == i)
+        u++;
+      if (u - l != run)
+        bad = true;
+    }
+  }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0)
+    *flag = 1;
+}
+
+} // namespace
+
+// la_rcm_device's front: the pattern check on the device and, for a
+// connected pattern that qualifies, the whole ordering there (*handled);
+// otherwise the caller runs rcm() (host components, large ones on the
+// device).
+la_status rcm_device_connected(int n, int base, const int *ai, const int *aj, int *iperm,
+                               int *perm, bool *handled) {
+  *handled = false;
+  std::vector<int> deg(n);
+  int maxdeg = 0;
+  for (int i = 0; i < n; i++) {
+    deg[i] = ai[i + 1] - ai[i];
+    maxdeg = std::max(maxdeg, deg[i]);
+  }
+  la_status st = LA_OK;
+  RcmDevice *D = rcm_device_create(n, base, ai, aj, deg.data(), &st);
+  if (!D)
+    return st;
+  struct Owner {
+    RcmDevice *d;
+    ~Owner() { rcm_device_destroy(d); }
+  } own{D};
+  LA_CUDA_TRY(cudaMemset(D->count.p, 0, sizeof(int)));
+  symmetric_check_kernel<<<blocks_for(n), kThreads>>>(n, base, D->ai.as<int>(), D->aj.as<int>(),
+                                                      D->count.as<int>());
+  LA_CUDA_TRY(cudaGetLastError());
+  int bad = 0;
+  LA_CUDA_TRY(cudaMemcpy(&bad, D->count.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (bad) {
+    set_error("la_rcm_device needs a structurally symmetric pattern");
+    return LA_ERR_INVALID_ARG;
+  }
+  if (n < kRcmDeviceMin || maxdeg > kRcmMaxDegree)
+    return LA_OK; // the caller's path
+  // connected?  one device BFS from node 0
+  std::vector<int> ls;
+  int reached = 0, height = 0;
+  LA_TRY(D->bfs(0, reached, ls, &height));
+  const int all = reached;
+  bfs_reset_kernel<<<blocks_for(reached), kThreads>>>(reached, D->queue.as<int>(),
+                                                       D->level.as<int>());
+  LA_CUDA_TRY(cudaGetLastError());
+  if (all != n)
+    return LA_OK; // several components: the caller's path
+  // one component, members 0 .. n-1 ascending
+  std::vector<int> members(n);
+  for (int i = 0; i < n; i++)
+    members[i] = i;
+  LA_TRY(rcm_device_component(D, members.data(), n, iperm));
+  std::reverse(iperm, iperm + n);
+  for (int i = 0; i < n; i++)
+    perm[iperm[i] - base] = i + base;
+  *handled = true;
+  return LA_OK;
+}
+
+} // namespace la

@@ -70,3 +70,22 @@ def test_rcm_device_timing_c5_size(lab):
     t_dev = time.perf_counter() - t0
     assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
     print(f"RCM 192^3: host {t_host:.3f} s, with the device ordering {t_dev:.3f} s")
+
+
+def test_rcm_device_rejects_what_the_host_rejects(lab):
+    """The pattern check runs on the device for la_rcm_device: an
+    unsymmetric pattern and a symmetric one with an unsorted row are both
+    rejected, as la_rcm's transpose comparison rejects them."""
+    from linearalgebra_b200 import gen
+    n, ai, aj, av = gen.laplacian_3d(42)  # 74,088 nodes: above the device threshold
+    unsym_aj = aj.copy()
+    r = 5000
+    lo, hi = int(ai[r]), int(ai[r + 1])
+    unsym_aj[hi - 1] = min(n - 1, int(unsym_aj[hi - 1]) + 1)  # (r, c) with no (c, r)
+    unsorted_aj = aj.copy()
+    unsorted_aj[lo], unsorted_aj[lo + 1] = aj[lo + 1], aj[lo]
+    for bad in (unsym_aj, unsorted_aj):
+        for dev in (False, True):
+            with pytest.raises(lab.LAError) as e:
+                lab.SerialCM(n, 0, ai, bad, device=dev)
+            assert e.value.name == "LA_ERR_INVALID_ARG", dev
