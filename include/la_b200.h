@@ -315,14 +315,15 @@ la_status la_icc0_shifted(int n, int base, const int *u_ai, const int *u_aj,
                           double *shift_used);
 
 /* The same factorisations on the GPU: a symbolic plan built once per
- * pattern on the host (the sequential algorithm replayed on the pattern,
- * recording every row's updates in their order), then numeric passes on the
+ * pattern on the host (every row's updates in the order the sequential
+ * algorithm applies them, found in parallel over rows), then numeric passes on the
  * device, one persistent launch each, level-scheduled by the rows'
  * dependencies -- bit-identical to la_icc0 / la_ilu0 (same operations, same
  * order).  For a pattern factored more than once (new values, shift
  * retries) the numeric pass replaces the host's.
  * la_icc0_plan_create: u_ai/u_aj as la_icc0 takes them (ICCLevelNumeric,
- * precond.hpp:615-693).  la_ilu0_plan_create: a full pattern, every row
+ * precond.hpp:615-693), each row's columns strictly ascending from its
+ * diagonal (LA_ERR_INVALID_ARG otherwise).  la_ilu0_plan_create: a full pattern, every row
  * holding its diagonal, as la_ilu0 takes it.  HOST arrays. */
 la_status la_icc0_plan_create(int n, int base, const int *u_ai, const int *u_aj,
                               la_factor_plan_t *out);

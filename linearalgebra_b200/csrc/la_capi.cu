@@ -653,11 +653,19 @@ la_status la_icc0_plan_create(int n, int base, const int *u_ai, const int *u_aj,
                               la_factor_plan_t *out) {
   LA_CHECK_ARG(u_ai && out && n >= 0 && (base == 0 || base == 1), "arguments");
   LA_CHECK_ARG(u_ai[n] - base == 0 || u_aj, "u_aj");
-  for (int i = 0; i < n; i++)
-    if (u_ai[i + 1] == u_ai[i] || u_aj[u_ai[i] - base] - base != i) {
+  for (int i = 0; i < n; i++) {
+    if (u_ai[i + 1] <= u_ai[i] || u_aj[u_ai[i] - base] - base != i) {
       set_error("IC(0): row %d of the upper triangle does not start with its diagonal", i);
       return LA_ERR_INVALID_ARG;
     }
+    // the symbolic pass orders updates by walking rows backwards from a
+    // column: columns must ascend strictly and stay below n
+    for (int k = u_ai[i] - base + 1; k < u_ai[i + 1] - base; k++)
+      if (u_aj[k] <= u_aj[k - 1] || u_aj[k] - base >= n) {
+        set_error("IC(0): row %d of the upper triangle is not sorted within [%d, %d)", i, i, n);
+        return LA_ERR_INVALID_ARG;
+      }
+  }
   LA_TRY(require_device());
   return factor_plan_create(0, n, base, u_ai, u_aj, out);
 }

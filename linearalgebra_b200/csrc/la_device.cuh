@@ -77,6 +77,42 @@ __device__ __forceinline__ int ld_relaxed(const int *p) {
   return v;
 }
 
+// Grid-wide barrier for a cooperative launch.  bar[0]: arrivals, bar[1]:
+// generation, bar[2]: error word, set to 1 when a wait gave up after 1 s
+// (the waiting block then carries on; callers that loop over barriers read
+// bar[2] after each one and leave).  The fences on both sides make the
+// writes before the barrier visible to every block after it.
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ inline void grid_barrier(unsigned *bar) {
+  constexpr unsigned long long kLimitNs = 1000000000ull;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned *gen = bar + 1;
+    const unsigned g = *gen; // read before arriving: the generation to leave
+    __threadfence();
+    if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      const unsigned long long t0 = global_ns();
+      while (*gen == g) {
+        if (global_ns() - t0 > kLimitNs) {
+          atomicExch(bar + 2, 1u);
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
 // Asynchronous 4- or 8-byte copy global -> shared (one element; both
 // addresses aligned to its size), tracked by the issuing thread's groups.
 template <typename T>

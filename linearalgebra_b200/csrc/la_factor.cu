@@ -11,12 +11,12 @@
 // B200 design.  The factorisation is split into a symbolic plan, built once
 // per pattern on the host, and a numeric pass on the GPU that can run many
 // times (new values, or the shift retries after a breakdown):
-//  * symbolic: the host replays the sequential algorithm on the pattern
-//    alone and records, for every row j, the ordered list of updates it
-//    receives -- for IC(0) the rows k with U_kj != 0 in the order the
-//    up-looking algorithm's linked lists deliver them, for ILU(0) the stored
-//    k < j in ascending order -- and, for each update, the (target entry of
-//    row j, source entry of row k) pairs it subtracts.  Row j depends exactly
+//  * symbolic: the host records, for every row j, the ordered list of
+//    updates it receives -- for IC(0) the rows k with U_kj != 0 in the order
+//    the up-looking algorithm's linked lists deliver them (a rule on the
+//    pattern alone, update_before, applied to each row in parallel), for
+//    ILU(0) the stored k < j in ascending order -- and, for each update, the
+//    (target entry of row j, source entry of row k) pairs it subtracts.  Row j depends exactly
 //    on the rows of its updates, so their level sets (by longest path, as
 //    TopologicalSort2 computes them) order the rows for the device;
 //  * numeric: one persistent launch; warps claim 32-row chunks in level
@@ -41,6 +41,7 @@
 #include "la_internal.h"
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <memory>
 #include <vector>
@@ -69,53 +70,117 @@ struct Symbolic {
   std::vector<int> uptr, uk, us, upiv, pptr, ptgt, psrc, diag;
 };
 
+// The (target entry of row j, source entry of row k) pairs of one update:
+// the columns row k holds from entry ck0 on that row j also holds.  Calls
+// emit(p, ck) per pair, in ascending column order.
+template <typename F>
+inline void merge_pairs(const int *aj, int rs, int re, int ck0, int ke, F emit) {
+  for (int p = rs, ck = ck0; ck < ke && p < re;) {
+    if (aj[ck] == aj[p])
+      emit(p++, ck++);
+    else if (aj[ck] < aj[p])
+      ck++;
+    else
+      p++;
+  }
+}
+
+// Whether update x precedes update y in the list of the row they both
+// update.  The up-looking algorithm keeps a LIFO list per row: row k joins
+// row c's list when its cursor reaches column c, which happens while row r =
+// the column before c in row k is processed (r = k for k's first
+// off-diagonal; row k itself joins last, after r's own updates were
+// delivered).  So a list holds its rows by descending r; among rows with the
+// same r, row r itself first, then the updates of row r in the reverse of
+// the order row r received them -- the same rule one column further back,
+// with the direction flipped.  px / py: the entries before the target
+// column in rows x and y; lx / ly: their diagonal entries.
+inline bool update_before(const int *aj, int px, int lx, int py, int ly) {
+  for (bool flip = false;; flip = !flip) {
+    const int cx = aj[px], cy = aj[py];
+    if (cx != cy)
+      return (cx > cy) != flip;
+    if (px == lx) // x is row cx itself
+      return !flip;
+    if (py == ly)
+      return flip;
+    px--;
+    py--;
+  }
+}
+
+// Row j receives one update per strict upper entry (k, j) of its column, in
+// the order of its list (update_before), found per row in parallel; each
+// update's (target, source) pairs are then merged in parallel, counted first
+// and written second.  The rows' columns must ascend (checked by the caller).
 void symbolic_ic0(int n, int base, const int *ai, const int *aj, Symbolic &S) {
-  constexpr int kEnd = 0x7fffffff;
-  std::vector<int> next(n, kEnd), cursor(n, 0);
   S.uptr.assign(n + 1, 0);
-  S.pptr.assign(1, 0);
   S.diag.resize(n);
-  // one update per strict upper entry; each holds at least its diagonal pair
-  const size_t upd = (size_t)(ai[n] - base) - (size_t)n;
-  S.uk.reserve(upd);
-  S.us.reserve(upd);
-  S.pptr.reserve(upd + 1);
-  S.ptgt.reserve(3 * upd);
-  S.psrc.reserve(3 * upd);
+  for (int j = 0; j < n; j++)
+    S.diag[j] = ai[j] - base;
+  for (int k = 0; k < n; k++)
+    for (int e = ai[k] - base + 1; e < ai[k + 1] - base; e++)
+      S.uptr[aj[e] - base + 1]++;
+  for (int j = 0; j < n; j++)
+    S.uptr[j + 1] += S.uptr[j];
+  const int nu = S.uptr[n];
+  S.uk.resize(nu);
+  S.us.resize(nu);
+  {
+    std::vector<int> fill(S.uptr.begin(), S.uptr.end() - 1);
+    for (int k = 0; k < n; k++)
+      for (int e = ai[k] - base + 1; e < ai[k + 1] - base; e++) {
+        const int w = fill[aj[e] - base]++;
+        S.uk[w] = k;
+        S.us[w] = e;
+      }
+  }
+#pragma omp parallel
+  {
+    std::vector<std::pair<int, int>> t; // (entry, row) of one row's updates
+#pragma omp for schedule(dynamic, 4096)
+    for (int j = 0; j < n; j++) {
+      const int u0 = S.uptr[j], u1 = S.uptr[j + 1];
+      if (u1 - u0 < 2)
+        continue;
+      t.clear();
+      for (int u = u0; u < u1; u++)
+        t.emplace_back(S.us[u], S.uk[u]);
+      std::sort(t.begin(), t.end(), [&](const std::pair<int, int> &x,
+                                        const std::pair<int, int> &y) {
+        return update_before(aj, x.first - 1, ai[x.second] - base, y.first - 1,
+                             ai[y.second] - base);
+      });
+      for (int u = u0; u < u1; u++) {
+        S.us[u] = t[u - u0].first;
+        S.uk[u] = t[u - u0].second;
+      }
+    }
+  }
+  S.pptr.assign((size_t)nu + 1, 0);
+#pragma omp parallel for schedule(dynamic, 4096)
   for (int j = 0; j < n; j++) {
     const int rs = ai[j] - base, re = ai[j + 1] - base;
-    S.diag[j] = rs;
-    for (int k = next[j]; k < j;) {
-      const int ck0 = cursor[k]++;
-      const int ke = ai[k + 1] - base;
-      const int after = next[k];
-      if (ck0 + 1 < ke) {
-        const int c = aj[ck0 + 1] - base;
-        next[k] = next[c];
-        next[c] = k;
-      }
-      S.uk.push_back(k);
-      S.us.push_back(ck0);
-      for (int p = rs, ck = ck0; ck < ke && p < re;) {
-        if (aj[ck] == aj[p]) {
-          S.ptgt.push_back(p++);
-          S.psrc.push_back(ck++);
-        } else if (aj[ck] < aj[p]) {
-          ck++;
-        } else {
-          p++;
-        }
-      }
-      S.pptr.push_back((int)S.ptgt.size());
-      k = after;
+    for (int u = S.uptr[j]; u < S.uptr[j + 1]; u++) {
+      int c = 0;
+      merge_pairs(aj, rs, re, S.us[u], ai[S.uk[u] + 1] - base, [&](int, int) { c++; });
+      S.pptr[u + 1] = c;
     }
-    if (re - rs > 1) {
-      const int c = aj[rs + 1] - base;
-      next[j] = next[c];
-      next[c] = j;
-      cursor[j] = rs + 1;
+  }
+  for (int u = 0; u < nu; u++)
+    S.pptr[u + 1] += S.pptr[u];
+  S.ptgt.resize(S.pptr[nu]);
+  S.psrc.resize(S.pptr[nu]);
+#pragma omp parallel for schedule(dynamic, 4096)
+  for (int j = 0; j < n; j++) {
+    const int rs = ai[j] - base, re = ai[j + 1] - base;
+    for (int u = S.uptr[j]; u < S.uptr[j + 1]; u++) {
+      int w = S.pptr[u];
+      merge_pairs(aj, rs, re, S.us[u], ai[S.uk[u] + 1] - base, [&](int p, int ck) {
+        S.ptgt[w] = p;
+        S.psrc[w++] = ck;
+      });
     }
-    S.uptr[j + 1] = (int)S.uk.size();
   }
 }
 
@@ -345,8 +410,13 @@ la_status plan_build(la_factor_plan_s *P, const int *ai, const int *aj, Symbolic
   int per_sm = 0;
   LA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
       &per_sm, (const void *)factor_kernel<kIC0>, kFactorThreads, 0));
+  // LA_FACTOR_CTAS_PER_SM caps the CTAs per SM (tuning override; default:
+  // as many as fit).  Warps beyond what the widest levels use only poll.
+  per_sm = std::max(per_sm, 1);
+  if (const char *e = std::getenv("LA_FACTOR_CTAS_PER_SM"))
+    per_sm = std::min(per_sm, std::max(1, std::atoi(e)));
   const int need = (P->nchunks + kFactorThreads / 32 - 1) / (kFactorThreads / 32);
-  P->grid = std::max(1, std::min(std::max(per_sm, 1) * sm_count(), need));
+  P->grid = std::max(1, std::min(per_sm * sm_count(), need));
   return LA_OK;
 }
 

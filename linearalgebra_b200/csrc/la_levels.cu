@@ -23,6 +23,7 @@
 #include "la_internal.h"
 
 #include <algorithm>
+#include <cstdlib>
 #include <vector>
 
 namespace la {
@@ -158,8 +159,11 @@ la_status topological_sort2_device(int uplo, int n, int base, const int *ai, con
   const void *fn = uplo == LA_LOWER ? (const void *)depth_kernel<false>
                                     : (const void *)depth_kernel<true>;
   LA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, 0));
+  per_sm = std::max(per_sm, 1);
+  if (const char *e = std::getenv("LA_LEVELS_CTAS_PER_SM")) // tuning override
+    per_sm = std::min(per_sm, std::max(1, std::atoi(e)));
   const int need = ((n + 31) / 32 + kThreads / 32 - 1) / (kThreads / 32);
-  const int grid = std::max(1, std::min(std::max(per_sm, 1) * sm_count(), need));
+  const int grid = std::max(1, std::min(per_sm * sm_count(), need));
   if (uplo == LA_LOWER)
     depth_kernel<false><<<grid, kThreads, 0, st>>>(n, base, dai.as<int>(), daj.as<int>(),
                                                    depth.as<int>(), kh[0].as<unsigned>(),

@@ -187,40 +187,6 @@ __global__ void p_update_kernel(const int n, X *p, const X *z,
 // took 470 / 475 instead of 454 / 454 -- their outputs are no longer hot in
 // L2 when written amid this kernel's other traffic, where a memset right
 // before each solve leaves them there).
-constexpr unsigned long long kBarrierNs = 1000000000ull; // 1 s
-
-__device__ __forceinline__ unsigned long long pcg_global_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-  return t;
-}
-
-// bar[0]: arrivals, bar[1]: generation, bar[2]: error word (1 = a wait gave up)
-__device__ void grid_barrier(unsigned *bar) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    volatile unsigned *gen = bar + 1;
-    const unsigned g = *gen; // read before arriving: the generation to leave
-    __threadfence();
-    if (atomicAdd(bar, 1u) == gridDim.x - 1) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 1, 1u);
-    } else {
-      const unsigned long long t0 = pcg_global_ns();
-      while (*gen == g) {
-        if (pcg_global_ns() - t0 > kBarrierNs) {
-          atomicExch(bar + 2, 1u);
-          break;
-        }
-        __nanosleep(32);
-      }
-    }
-    __threadfence();
-  }
-  __syncthreads();
-}
-
 // partials: 2 * gridDim.x doubles ((p, q) totals, then ||r||^2 totals).
 template <typename X>
 __global__ void __launch_bounds__(kDotThreads)
@@ -235,7 +201,7 @@ __global__ void __launch_bounds__(kDotThreads)
   const double bt = block_sum(s, red);
   if (threadIdx.x == 0)
     partials[blockIdx.x] = bt;
-  grid_barrier(bar);
+  dev::grid_barrier(bar);
   if (threadIdx.x == 0) {
     const double pq = sum_partials(partials, gridDim.x);
     const double al = scal[S_RZ] / pq; // alpha = (r, z) / (p, A p)

@@ -11,28 +11,32 @@
 // for each node, its not yet claimed neighbours of the next level sorted by
 // (degree, index).
 //
-// B200 design.  A level-synchronous BFS (one launch per level; a vertex is
-// claimed by a compare-and-swap on its level, so the levels are the
-// sequential search's) and packed (degree, index) minimum reductions give
-// the source.  The sweep needs no sequential walk: a node of level l+1 is
-// appended by the first node of level l, in the ordering, that neighbours
-// it, so per level (1) every next-level node finds the smallest ordering
-// position among its level-l neighbours (its parent), (2) every level-l
-// node counts the next-level nodes it is the parent of, (3) a scan of the
-// counts gives each parent's first slot, and (4) every parent sorts its
-// children by (degree, index) into its slots.  Integer work only: the
+// B200 design.  A level-synchronous BFS (a vertex is claimed by a
+// compare-and-swap on its level, so the levels are the sequential search's)
+// and packed (degree, index) minimum reductions give the source.  The sweep
+// needs no sequential walk: a node of level l+1 is appended by the first
+// node of level l, in the ordering, that neighbours it, so per level (1)
+// every next-level node finds the smallest ordering position among its
+// level-l neighbours (its parent), (2) every level-l node counts the
+// next-level nodes it is the parent of, (3) a scan of the counts gives each
+// parent's first slot, and (4) every parent sorts its children by (degree,
+// index) into its slots.  The search and the sweep each run as ONE
+// cooperative launch whose levels are separated by grid barriers (bounded:
+// a wait that exceeds 1 s sets an error word and the launch ends), so the
+// host waits once per search, not once per level.  Integer work only: the
 // ordering equals the host's exactly.  Used for components of at least
 // kRcmDeviceMin nodes whose rows hold at most kRcmMaxDegree entries (a
 // parent's children are sorted in registers); the host orders the rest.
 //
-// Roofline: latency-bound (a few launches per BFS level); each level reads
-// its nodes' rows once per step.
+// Roofline: latency-bound (a grid barrier per BFS level, three per sweep
+// level); each level reads its nodes' rows once per step.
 
 #include "la_device.cuh"
 #include "la_internal.h"
 
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
 #include <vector>
 
 namespace la {
@@ -40,18 +44,44 @@ namespace {
 
 constexpr int kThreads = 256;
 
-// frontier [qs, qe) of queue, next level appended after qe
-__global__ void bfs_expand_kernel(const int qs, const int qe, const int lev, int *queue,
-                                  int *level, const int *__restrict__ ai,
-                                  const int *__restrict__ aj, const int base, int *cnt) {
-  for (int h = qs + blockIdx.x * blockDim.x + threadIdx.x; h < qe;
-       h += gridDim.x * blockDim.x) {
-    const int u = queue[h];
-    for (int k = __ldg(ai + u) - base; k < __ldg(ai + u + 1) - base; k++) {
-      const int v = __ldg(aj + k) - base;
-      if (level[v] < 0 && atomicCAS(level + v, -1, lev) == -1)
-        queue[qe + atomicAdd(cnt, 1)] = v;
+// The whole search in one cooperative launch.  Level l is queue[lstart[l],
+// lstart[l+1]); at step lev the grid expands level lev-1, appending the
+// vertices it claims after the frontier, then meets at a grid barrier and
+// reads the new level's size.  cnt3 holds three rotating counters: the one
+// step lev+1 uses is cleared during step lev, when every thread has passed
+// the barrier after its last read (at step lev-2).  bar[0..2]: the barrier;
+// bar[3]: the number of levels, written at the end.
+__global__ void __launch_bounds__(kThreads)
+    bfs_kernel(int *queue, int *level, const int *__restrict__ ai, const int *__restrict__ aj,
+               const int base, int *lstart, int *cnt3, unsigned *bar) {
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+  int qs = 0, qe = 1;
+  for (int lev = 1;; lev++) {
+    int *cnt = cnt3 + lev % 3;
+    if (gt == 0)
+      cnt3[(lev + 1) % 3] = 0;
+    for (int h = qs + gt; h < qe; h += gs) {
+      const int u = __ldcg(queue + h);
+      const int a = __ldg(ai + u) - base, e = __ldg(ai + u + 1) - base;
+      for (int k = a; k < e; k++) {
+        const int v = __ldg(aj + k) - base;
+        if (__ldcg(level + v) < 0 && atomicCAS(level + v, -1, lev) == -1)
+          queue[qe + atomicAdd(cnt, 1)] = v;
+      }
     }
+    dev::grid_barrier(bar);
+    if (dev::ld_relaxed((const int *)bar + 2) != 0)
+      return; // a barrier wait gave up
+    const int c = dev::ld_relaxed(cnt);
+    if (c == 0) {
+      if (gt == 0)
+        bar[3] = lev;
+      return;
+    }
+    qs = qe;
+    qe += c;
+    if (gt == 0)
+      lstart[lev + 1] = qe;
   }
 }
 
@@ -61,9 +91,11 @@ __global__ void bfs_reset_kernel(const int m, const int *queue, int *level) {
     level[queue[h]] = -1;
 }
 
-__global__ void bfs_start_kernel(const int src, int *queue, int *level) {
+__global__ void bfs_start_kernel(const int src, int *queue, int *level, int *lstart) {
   queue[0] = src;
   level[src] = 0;
+  lstart[0] = 0;
+  lstart[1] = 1;
 }
 
 // smallest (degree, node) over list[0, m) whose degree is not INT_MAX
@@ -91,109 +123,132 @@ __global__ void mark_kernel(const int sel, int *deg, const int *__restrict__ ai,
     deg[__ldg(aj + k) - base] = INT_MAX;
 }
 
-// (1) parent of each next-level node: smallest ordering position among its
-// level-l neighbours
-__global__ void parent_kernel(const int m, const int *nodes, const int lev, const int *level,
-                              const int *pos, int *parent, const int *__restrict__ ai,
-                              const int *__restrict__ aj, const int base) {
-  for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < m; h += gridDim.x * blockDim.x) {
-    const int v = nodes[h];
-    int p = INT_MAX;
-    for (int k = __ldg(ai + v) - base; k < __ldg(ai + v + 1) - base; k++) {
-      const int u = __ldg(aj + k) - base;
-      if (level[u] == lev)
-        p = min(p, pos[u]);
-    }
-    parent[v] = p;
+// Exclusive scan (and total) of one value per thread over the block.
+__device__ int block_exclusive_scan(int v, int *total) {
+  __shared__ int wsum[kThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int incl = v;
+  for (int k = 1; k < 32; k <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, k);
+    if (lane >= k)
+      incl += t;
   }
-}
-
-// (2) children per level-l position p in [p0, p0 + m)
-__global__ void child_count_kernel(const int p0, const int m, const int *cm, const int lev,
-                                   const int *level, const int *parent, int *cnt,
-                                   const int *__restrict__ ai, const int *__restrict__ aj,
-                                   const int base) {
-  for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < m; h += gridDim.x * blockDim.x) {
-    const int p = p0 + h, u = cm[p];
-    int c = 0;
-    for (int k = __ldg(ai + u) - base; k < __ldg(ai + u + 1) - base; k++) {
-      const int v = __ldg(aj + k) - base;
-      c += level[v] == lev + 1 && parent[v] == p;
-    }
-    cnt[h] = c;
-  }
-}
-
-// (3) exclusive scan of cnt[0, m) in place, one block walking 2048-entry
-// chunks with a running carry
-__global__ void __launch_bounds__(1024) scan_one_block_kernel(int *cnt, const int m) {
-  __shared__ int wsum[32];
-  __shared__ int carry;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  if (tid == 0)
-    carry = 0;
+  if (lane == 31)
+    wsum[warp] = incl;
   __syncthreads();
-  for (int c0 = 0; c0 < m; c0 += 2048) {
-    const int i0 = c0 + 2 * tid;
-    const int a = i0 < m ? cnt[i0] : 0, b = i0 + 1 < m ? cnt[i0 + 1] : 0;
-    int incl = a + b;
+  if (warp == 0) {
+    const int w = lane < kThreads / 32 ? wsum[lane] : 0;
+    int wi = w;
     for (int k = 1; k < 32; k <<= 1) {
-      const int t = __shfl_up_sync(0xffffffffu, incl, k);
+      const int t = __shfl_up_sync(0xffffffffu, wi, k);
       if (lane >= k)
-        incl += t;
+        wi += t;
     }
-    if (lane == 31)
-      wsum[warp] = incl;
-    __syncthreads();
-    if (warp == 0) {
-      const int w = wsum[lane];
-      int wi = w;
-      for (int k = 1; k < 32; k <<= 1) {
-        const int t = __shfl_up_sync(0xffffffffu, wi, k);
-        if (lane >= k)
-          wi += t;
-      }
+    if (lane < kThreads / 32)
       wsum[lane] = wi - w;
-    }
-    __syncthreads();
-    const int ex = carry + wsum[warp] + incl - (a + b);
-    if (i0 < m)
-      cnt[i0] = ex;
-    if (i0 + 1 < m)
-      cnt[i0 + 1] = ex + a;
-    __syncthreads();
-    if (tid == 1023)
-      carry = ex + a + b;
-    __syncthreads();
+    if (lane == kThreads / 32 - 1)
+      *total = wi;
   }
+  __syncthreads();
+  const int ex = wsum[warp] + incl - v;
+  __syncthreads(); // wsum is reused by the next call
+  return ex;
 }
 
-// (4) each parent's children, sorted by (degree, node), into its slots
+// The Cuthill-McKee sweep in one cooperative launch, for the search whose
+// level starts are lstart[0, height]; cm[0] = source and pos[source] = 0 on
+// entry.  Per level l, three steps separated by grid barriers:
+//  (1) parent[v] of each level-(l+1) node: the smallest ordering position
+//      among its level-l neighbours;
+//  (2) each level-l position p counts its children (level-(l+1) neighbours
+//      whose parent is p); the counts are scanned within tiles of kThreads
+//      positions (cnt) and each tile's total kept (tile_sum);
+//  (4) each position's first slot is q0 + (tiles before its own) + cnt; it
+//      sorts its children by (degree, node) and writes them to cm and pos.
+// Arrays written inside the launch are read with __ldcg (L2, coherent).
 template <int MAXC>
-__global__ void place_kernel(const int p0, const int m, const int q0, int *cm, int *pos,
-                             const int lev, const int *level, const int *parent, const int *off,
-                             const int *deg, const int *__restrict__ ai,
-                             const int *__restrict__ aj, const int base) {
-  for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < m; h += gridDim.x * blockDim.x) {
-    const int p = p0 + h, u = cm[p];
-    int ch[MAXC];
-    int c = 0;
-    for (int k = __ldg(ai + u) - base; k < __ldg(ai + u + 1) - base && c < MAXC; k++) {
-      const int v = __ldg(aj + k) - base;
-      if (level[v] == lev + 1 && parent[v] == p) {
-        int i = c++; // insertion by (degree, node)
-        while (i > 0 && (deg[ch[i - 1]] > deg[v] || (deg[ch[i - 1]] == deg[v] && ch[i - 1] > v))) {
-          ch[i] = ch[i - 1];
-          i--;
+__global__ void __launch_bounds__(kThreads)
+    cm_sweep_kernel(const int height, const int *__restrict__ lstart,
+                    const int *__restrict__ queue, const int *__restrict__ level, int *pos,
+                    int *parent, int *cm, int *cnt, int *tile_sum, const int *__restrict__ deg,
+                    const int *__restrict__ ai, const int *__restrict__ aj, const int base,
+                    unsigned *bar) {
+  __shared__ int tile_total, tile_base;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+  for (int l = 0; l + 1 < height; l++) {
+    const int p0 = __ldg(lstart + l), q0 = __ldg(lstart + l + 1);
+    const int m = q0 - p0, mq = __ldg(lstart + l + 2) - q0;
+    // (1)
+    for (int h = gt; h < mq; h += gs) {
+      const int v = __ldg(queue + q0 + h);
+      int p = INT_MAX;
+      for (int k = __ldg(ai + v) - base; k < __ldg(ai + v + 1) - base; k++) {
+        const int u = __ldg(aj + k) - base;
+        if (__ldg(level + u) == l)
+          p = min(p, __ldcg(pos + u));
+      }
+      parent[v] = p;
+    }
+    dev::grid_barrier(bar);
+    if (dev::ld_relaxed((const int *)bar + 2) != 0)
+      return;
+    // (2)
+    const int ntiles = (m + kThreads - 1) / kThreads;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      const int h = t * kThreads + threadIdx.x;
+      int c = 0;
+      if (h < m) {
+        const int p = p0 + h, u = __ldcg(cm + p);
+        for (int k = __ldg(ai + u) - base; k < __ldg(ai + u + 1) - base; k++) {
+          const int v = __ldg(aj + k) - base;
+          c += __ldg(level + v) == l + 1 && __ldcg(parent + v) == p;
         }
-        ch[i] = v;
+      }
+      const int ex = block_exclusive_scan(c, &tile_total);
+      if (h < m)
+        cnt[h] = ex;
+      if (threadIdx.x == 0)
+        tile_sum[t] = tile_total;
+    }
+    dev::grid_barrier(bar);
+    if (dev::ld_relaxed((const int *)bar + 2) != 0)
+      return;
+    // (4)
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      int s = 0;
+      for (int k = threadIdx.x; k < t; k += kThreads)
+        s += __ldcg(tile_sum + k);
+      block_exclusive_scan(s, &tile_base);
+      const int h = t * kThreads + threadIdx.x;
+      if (h < m) {
+        const int p = p0 + h, u = __ldcg(cm + p);
+        int ch[MAXC];
+        int c = 0;
+        for (int k = __ldg(ai + u) - base; k < __ldg(ai + u + 1) - base && c < MAXC; k++) {
+          const int v = __ldg(aj + k) - base;
+          if (__ldg(level + v) == l + 1 && __ldcg(parent + v) == p) {
+            const int dv = __ldg(deg + v);
+            int i = c++; // insertion by (degree, node)
+            while (i > 0) {
+              const int w = ch[i - 1], dw = __ldg(deg + w);
+              if (dw < dv || (dw == dv && w < v))
+                break;
+              ch[i] = w;
+              i--;
+            }
+            ch[i] = v;
+          }
+        }
+        const int o = q0 + tile_base + __ldcg(cnt + h);
+        for (int i = 0; i < c; i++) {
+          cm[o + i] = ch[i];
+          pos[ch[i]] = o + i;
+        }
       }
     }
-    const int o = q0 + off[h];
-    for (int i = 0; i < c; i++) {
-      cm[o + i] = ch[i];
-      pos[ch[i]] = o + i;
-    }
+    dev::grid_barrier(bar);
+    if (dev::ld_relaxed((const int *)bar + 2) != 0)
+      return;
   }
 }
 
@@ -210,8 +265,8 @@ int blocks_for(int m) { return std::max(1, std::min((m + kThreads - 1) / kThread
 namespace la {
 
 struct RcmDevice {
-  int n = 0, base = 0;
-  DevBuf ai, aj, deg, level, queue, pos, parent, cm, cnt, best, count;
+  int n = 0, base = 0, grid = 0;
+  DevBuf ai, aj, deg, level, queue, pos, parent, cm, cnt, best, count, lstart, tiles, cnt3, bar;
   cudaStream_t st = nullptr;
 
   la_status init(int n_, int base_, const int *h_ai, const int *h_aj, const int *h_deg) {
@@ -223,41 +278,97 @@ struct RcmDevice {
     LA_TRY(deg.upload(h_deg, sizeof(int) * n));
     for (DevBuf *b : {&level, &queue, &pos, &parent, &cm, &cnt})
       LA_TRY(b->alloc(sizeof(int) * n));
+    LA_TRY(lstart.alloc(sizeof(int) * (n + 2)));
+    LA_TRY(tiles.alloc(sizeof(int) * (n / kThreads + 2)));
+    LA_TRY(cnt3.alloc(sizeof(int) * 3));
+    LA_TRY(bar.alloc(sizeof(unsigned) * 4));
     LA_TRY(best.alloc(sizeof(unsigned long long)));
     LA_TRY(count.alloc(sizeof(int)));
     LA_CUDA_TRY(cudaMemset(level.p, 0xff, sizeof(int) * n));
+    // Cooperative grid: LA_RCM_CTAS_PER_SM CTAs per SM (tuning override;
+    // default 2), capped by what fits for both kernels.  A level is a few
+    // thousand to a few hundred thousand nodes; more CTAs only lengthen the
+    // barriers.
+    int fit = 1 << 30;
+    for (const void *f : {(const void *)bfs_kernel,
+                          (const void *)cm_sweep_kernel<kRcmMaxDegree>}) {
+      int per_sm = 0;
+      LA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, kThreads, 0));
+      fit = std::min(fit, per_sm);
+    }
+    if (fit < 1) {
+      set_error("RCM: the cooperative kernels do not fit on an SM");
+      return LA_ERR_CUDA;
+    }
+    int want = 2;
+    if (const char *e = std::getenv("LA_RCM_CTAS_PER_SM"))
+      want = std::max(1, std::atoi(e));
+    grid = std::min(want, fit) * sm_count();
     return LA_OK;
   }
 
-  // BFS from src; lstart[l] = first queue slot of level l; returns levels.
-  // The previous search's reached set (reached) is reset first.
-  la_status bfs(int src, int &reached, std::vector<int> &lstart, int *height) {
+  la_status barrier_status() {
+    unsigned b[4];
+    LA_CUDA_TRY(cudaMemcpyAsync(b, bar.p, sizeof(b), cudaMemcpyDeviceToHost, st));
+    LA_CUDA_TRY(cudaStreamSynchronize(st));
+    if (b[2]) {
+      set_error("RCM: a grid barrier wait exceeded its 1 s bound");
+      return LA_ERR_TIMEOUT;
+    }
+    return LA_OK;
+  }
+
+  // BFS from src; lstart[l] = first queue slot of level l (l <= height);
+  // the previous search's reached set (reached) is reset first.
+  la_status bfs(int src, int &reached, std::vector<int> &ls, int *height) {
     if (reached > 0) {
       bfs_reset_kernel<<<blocks_for(reached), kThreads, 0, st>>>(reached, queue.as<int>(),
                                                                  level.as<int>());
       LA_CUDA_TRY(cudaGetLastError());
     }
-    bfs_start_kernel<<<1, 1, 0, st>>>(src, queue.as<int>(), level.as<int>());
+    bfs_start_kernel<<<1, 1, 0, st>>>(src, queue.as<int>(), level.as<int>(), lstart.as<int>());
     LA_CUDA_TRY(cudaGetLastError());
-    lstart.assign(1, 0);
-    int qs = 0, qe = 1;
-    for (int lev = 1;; lev++) {
-      lstart.push_back(qe);
-      LA_CUDA_TRY(cudaMemsetAsync(count.p, 0, sizeof(int), st));
-      bfs_expand_kernel<<<blocks_for(qe - qs), kThreads, 0, st>>>(
-          qs, qe, lev, queue.as<int>(), level.as<int>(), ai.as<int>(), aj.as<int>(), base,
-          count.as<int>());
-      LA_CUDA_TRY(cudaGetLastError());
-      int c = 0;
-      LA_CUDA_TRY(cudaMemcpy(&c, count.p, sizeof(int), cudaMemcpyDeviceToHost));
-      if (c == 0)
-        break;
-      qs = qe;
-      qe += c;
+    LA_CUDA_TRY(cudaMemsetAsync(bar.p, 0, sizeof(unsigned) * 4, st));
+    LA_CUDA_TRY(cudaMemsetAsync(cnt3.p, 0, sizeof(int) * 3, st));
+    int *q = queue.as<int>(), *lv = level.as<int>(), *ls_d = lstart.as<int>();
+    int *c3 = cnt3.as<int>(), b = base;
+    const int *dai = ai.as<int>(), *daj = aj.as<int>();
+    unsigned *br = bar.as<unsigned>();
+    void *args[] = {&q, &lv, &dai, &daj, &b, &ls_d, &c3, &br};
+    LA_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)bfs_kernel, dim3(grid),
+                                            dim3(kThreads), args, 0, st));
+    unsigned s4[4];
+    LA_CUDA_TRY(cudaMemcpyAsync(s4, bar.p, sizeof(s4), cudaMemcpyDeviceToHost, st));
+    LA_CUDA_TRY(cudaStreamSynchronize(st));
+    if (s4[2]) {
+      set_error("RCM: a grid barrier wait exceeded its 1 s bound");
+      return LA_ERR_TIMEOUT;
     }
-    reached = qe;
-    *height = (int)lstart.size() - 1;
+    const int h = (int)s4[3];
+    ls.resize(h + 1);
+    LA_CUDA_TRY(cudaMemcpy(ls.data(), lstart.p, sizeof(int) * (h + 1), cudaMemcpyDeviceToHost));
+    reached = ls[h];
+    *height = h;
     return LA_OK;
+  }
+
+  // the sweep for the last search (from src, height levels): cm, pos
+  la_status sweep(int src, int height) {
+    LA_CUDA_TRY(cudaMemcpyAsync(cm.p, &src, sizeof(int), cudaMemcpyHostToDevice, st));
+    const int zero = 0;
+    LA_CUDA_TRY(cudaMemcpyAsync(pos.as<int>() + src, &zero, sizeof(int),
+                                cudaMemcpyHostToDevice, st));
+    LA_CUDA_TRY(cudaMemsetAsync(bar.p, 0, sizeof(unsigned) * 4, st));
+    int h = height, b = base;
+    const int *ls_d = lstart.as<int>(), *q = queue.as<int>(), *lv = level.as<int>();
+    int *ps = pos.as<int>(), *pa = parent.as<int>(), *c = cm.as<int>(), *ct = cnt.as<int>();
+    int *ts = tiles.as<int>();
+    const int *dg = deg.as<int>(), *dai = ai.as<int>(), *daj = aj.as<int>();
+    unsigned *br = bar.as<unsigned>();
+    void *args[] = {&h, &ls_d, &q, &lv, &ps, &pa, &c, &ct, &ts, &dg, &dai, &daj, &b, &br};
+    LA_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)cm_sweep_kernel<kRcmMaxDegree>,
+                                            dim3(grid), dim3(kThreads), args, 0, st));
+    return barrier_status();
   }
 
   // smallest (degree, node) among list[0, m) with degree != INT_MAX; -1 if none
@@ -324,28 +435,11 @@ la_status rcm_device_component(RcmDevice *D, const int *members, int size, int *
     set_error("RCM: a component's search reached %d of its %d nodes", ls[height], size);
     return LA_ERR_INVALID_ARG;
   }
-  int *cm = D->cm.as<int>(), *pos = D->pos.as<int>();
-  LA_CUDA_TRY(cudaMemcpyAsync(cm, &src, sizeof(int), cudaMemcpyHostToDevice, D->st));
-  const int zero = 0;
-  LA_CUDA_TRY(cudaMemcpyAsync(pos + src, &zero, sizeof(int), cudaMemcpyHostToDevice, D->st));
-  for (int l = 0; l + 1 < height; l++) {
-    const int p0 = ls[l], m = ls[l + 1] - ls[l];
-    const int q0 = ls[l + 1], mq = ls[l + 2] - ls[l + 1];
-    parent_kernel<<<blocks_for(mq), kThreads, 0, D->st>>>(
-        mq, D->queue.as<int>() + q0, l, D->level.as<int>(), pos, D->parent.as<int>(),
-        D->ai.as<int>(), D->aj.as<int>(), D->base);
-    child_count_kernel<<<blocks_for(m), kThreads, 0, D->st>>>(
-        p0, m, cm, l, D->level.as<int>(), D->parent.as<int>(), D->cnt.as<int>(),
-        D->ai.as<int>(), D->aj.as<int>(), D->base);
-    scan_one_block_kernel<<<1, 1024, 0, D->st>>>(D->cnt.as<int>(), m);
-    place_kernel<kRcmMaxDegree><<<blocks_for(m), kThreads, 0, D->st>>>(
-        p0, m, q0, cm, pos, l, D->level.as<int>(), D->parent.as<int>(), D->cnt.as<int>(),
-        D->deg.as<int>(), D->ai.as<int>(), D->aj.as<int>(), D->base);
-    LA_CUDA_TRY(cudaGetLastError());
-  }
+  LA_TRY(D->sweep(src, height));
   DevBuf o;
   LA_TRY(o.alloc(sizeof(int) * size));
-  add_base_copy_kernel<<<blocks_for(size), kThreads, 0, D->st>>>(size, cm, D->base, o.as<int>());
+  add_base_copy_kernel<<<blocks_for(size), kThreads, 0, D->st>>>(size, D->cm.as<int>(), D->base,
+                                                                  o.as<int>());
   LA_CUDA_TRY(cudaGetLastError());
   LA_CUDA_TRY(cudaMemcpy(out, o.p, sizeof(int) * size, cudaMemcpyDeviceToHost));
   // leave the level array clear for the next component

@@ -45,6 +45,29 @@ def test_factor_plan_needs_a_device(lab):
     assert e.value.name == "LA_ERR_NO_DEVICE"
 
 
+def test_ic0_plan_rejects_unsorted_rows(lab):
+    """The IC(0) plan orders each row's updates from the pattern, which needs
+    every row's columns strictly ascending from its diagonal: a row out of
+    order, a repeated column or a column past n is rejected before any device
+    work (so also without a GPU)."""
+    from linearalgebra_b200 import gen
+    n, ua, uj, uv = _ic_inputs(lab, gen.laplacian_2d(8), False)
+    r = 5
+    a, b = ua[r], ua[r + 1]
+    assert b - a >= 3
+    for bad in ("swap", "repeat", "past_n"):
+        uj2 = uj.copy()
+        if bad == "swap":
+            uj2[a + 1], uj2[a + 2] = uj2[a + 2], uj2[a + 1]
+        elif bad == "repeat":
+            uj2[a + 2] = uj2[a + 1]
+        else:
+            uj2[b - 1] = n
+        with pytest.raises(lab.LAError) as e:
+            lab.FactorPlan("ic0", n, 0, ua, uj2)
+        assert e.value.name == "LA_ERR_INVALID_ARG", bad
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("rcm", [False, True])
 def test_ic0_device_bit_identical(lab, rcm):
@@ -64,6 +87,51 @@ def test_ic0_device_bit_identical(lab, rcm):
         plan.factor(torch.as_tensor(uv).cuda(), out=out)
         torch.cuda.synchronize()
         assert np.array_equal(out.cpu().numpy(), want)
+
+
+def _random_spd(m, seed):
+    """An irregular symmetric M-matrix: random off-diagonal pattern (rows of
+    1 to ~40 entries, a few long ones), negative off-diagonals, a dominant
+    diagonal -- IC(0) exists, and the updates a row receives come in many
+    different orders."""
+    rng = np.random.default_rng(seed)
+    rows = [set() for _ in range(m)]
+    for i in range(m):
+        k = rng.integers(0, 40) if rng.random() < 0.05 else rng.integers(0, 5)
+        for j in rng.choice(m, k, replace=False):
+            if j != i:
+                rows[i].add(int(j))
+                rows[j].add(i)
+    ai = [0]
+    aj, av = [], []
+    for i in range(m):
+        cols = sorted(rows[i] | {i})
+        off = -rng.uniform(0.1, 1.0, len(cols))
+        aj += cols
+        av += list(off)
+        ai.append(len(aj))
+    ai, aj, av = np.array(ai, np.int32), np.array(aj, np.int32), np.array(av)
+    r = np.repeat(np.arange(m), np.diff(ai))
+    # symmetric values: the mean of (i, j) and (j, i), then a dominant diagonal
+    key = np.minimum(r, aj).astype(np.int64) * m + np.maximum(r, aj)
+    _, inv = np.unique(key, return_inverse=True)
+    av = (np.bincount(inv, av) / np.bincount(inv))[inv]
+    dsum = np.bincount(r, np.where(aj == r, 0.0, np.abs(av)), minlength=m)
+    av[aj == r] = dsum + 1.0
+    return m, ai, aj, av
+
+
+@pytest.mark.gpu
+def test_ic0_device_irregular_patterns(lab):
+    """Irregular patterns, natural and RCM order: the device factor equals the
+    host's bit for bit, so every row received its updates in the host's
+    order."""
+    for seed in range(4):
+        for rcm in (False, True):
+            n, ua, uj, uv = _ic_inputs(lab, _random_spd(4000 + 1000 * seed, seed), rcm)
+            want = lab.ICCLevelNumeric0(n, 0, ua, uj, uv)
+            got = lab.FactorPlan("ic0", n, 0, ua, uj).factor(uv)
+            assert np.array_equal(got, want), (seed, rcm, np.abs(got - want).max())
 
 
 @pytest.mark.gpu
