@@ -14,6 +14,7 @@
 #include <climits>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <numeric>
 
 namespace la {
@@ -136,20 +137,94 @@ int topological_sort2(int uplo, int n, int base, const int *ai, const int *aj,
 void transpose(int rows, int cols, int base, const int *ai, const int *aj,
                const double *av, int *t_ai, int *t_aj, double *t_av) {
   const int nnz = ai[rows] - base;
-  std::vector<int> pos(cols + 1, 0);
-  for (int k = 0; k < nnz; k++)
-    pos[aj[k] - base + 1]++;
-  std::partial_sum(pos.begin(), pos.end(), pos.begin());
-  for (int c = 0; c <= cols; c++)
-    t_ai[c] = pos[c] + base;
   const bool vals = av && t_av;
-  for (int i = 0; i < rows; i++)
-    for (int k = ai[i] - base; k < ai[i + 1] - base; k++) {
-      const int q = pos[aj[k] - base]++;
-      t_aj[q] = i + base;
-      if (vals)
-        t_av[q] = av[k];
+  if (nnz < (1 << 18)) { // small: one pass in row order
+    std::vector<int> pos(cols + 1, 0);
+    for (int k = 0; k < nnz; k++)
+      pos[aj[k] - base + 1]++;
+    std::partial_sum(pos.begin(), pos.end(), pos.begin());
+    for (int c = 0; c <= cols; c++)
+      t_ai[c] = pos[c] + base;
+    for (int i = 0; i < rows; i++)
+      for (int k = ai[i] - base; k < ai[i + 1] - base; k++) {
+        const int q = pos[aj[k] - base]++;
+        t_aj[q] = i + base;
+        if (vals)
+          t_av[q] = av[k];
+      }
+    return;
+  }
+  // large: on the host's threads, in two stable passes.  (1) rows are cut
+  // into T chunks of about equal entries; each chunk's entries go to column
+  // blocks of 2^shift columns, blocks major, chunks in order -- so inside a
+  // block the entries stay in row order.  (2) each block is counting-sorted by column
+  // on its own (stable).  The result is the one-pass order exactly.
+  const int T = std::max(1, omp_get_max_threads());
+  int shift = 0; // column blocks of 2^shift columns, about 8 per thread
+  while (((long long)cols >> shift) > 8LL * T)
+    shift++;
+  const int B = (int)(((long long)cols + (1LL << shift) - 1) >> shift);
+  std::vector<int> r0(T + 1);
+  for (int t = 0; t <= T; t++) {
+    const long long want = (long long)nnz * t / T;
+    r0[t] = (int)(std::lower_bound(ai, ai + rows + 1, (int)(want + base)) - ai);
+  }
+  r0[T] = rows;
+  std::vector<long long> off((size_t)T * B, 0); // [chunk][block]: a chunk's own row
+#pragma omp parallel for schedule(static, 1)
+  for (int t = 0; t < T; t++) {
+    long long *o = off.data() + (size_t)t * B;
+    for (int k = ai[r0[t]] - base; k < ai[r0[t + 1]] - base; k++)
+      o[(aj[k] - base) >> shift]++;
+  }
+  long long run = 0;
+  std::vector<long long> bstart(B + 1);
+  for (int b = 0; b < B; b++) {
+    bstart[b] = run;
+    for (int t = 0; t < T; t++) {
+      const long long c = off[(size_t)t * B + b];
+      off[(size_t)t * B + b] = run;
+      run += c;
     }
+  }
+  bstart[B] = run;
+  // scratch left uninitialised (every slot is written below), so its pages
+  // are first touched by the threads that fill them
+  std::unique_ptr<int[]> tc(new int[nnz]), tr(new int[nnz]);
+  std::unique_ptr<double[]> tv(vals ? new double[nnz] : nullptr);
+#pragma omp parallel for schedule(static, 1)
+  for (int t = 0; t < T; t++)
+    for (int i = r0[t]; i < r0[t + 1]; i++)
+      for (int k = ai[i] - base; k < ai[i + 1] - base; k++) {
+        const int c = aj[k] - base;
+        const long long q = off[(size_t)t * B + (c >> shift)]++;
+        tc[q] = c;
+        tr[q] = i;
+        if (vals)
+          tv[q] = av[k];
+      }
+  t_ai[cols] = nnz + base;
+#pragma omp parallel
+  {
+    std::vector<int> cnt;
+#pragma omp for schedule(dynamic, 1)
+    for (int b = 0; b < B; b++) {
+      const int c0 = b << shift, c1 = (int)std::min<long long>(cols, (long long)(b + 1) << shift);
+      cnt.assign(c1 - c0 + 1, 0);
+      for (long long q = bstart[b]; q < bstart[b + 1]; q++)
+        cnt[tc[q] - c0 + 1]++;
+      for (int c = 0; c < c1 - c0; c++)
+        cnt[c + 1] += cnt[c];
+      for (int c = c0; c < c1; c++)
+        t_ai[c] = (int)(bstart[b] + cnt[c - c0]) + base;
+      for (long long q = bstart[b]; q < bstart[b + 1]; q++) {
+        const long long w = bstart[b] + cnt[tc[q] - c0]++;
+        t_aj[w] = tr[q] + base;
+        if (vals)
+          t_av[w] = tv[q];
+      }
+    }
+  }
 }
 
 // matrix_utils.hpp:429-472 permute / :474-480 permuteRow: row i of the
@@ -285,10 +360,28 @@ int ilu0(int n, int base, const int *ai, const int *aj, const double *av, double
 void split_ldu(int n, int base, const int *ai, const int *aj, const double *av,
                int *l_ai, int *l_aj, double *l_av, double *d, int *u_ai,
                int *u_aj, double *u_av, int *lnnz, int *unnz) {
-  int lp = 0, up = 0;
+  // rows are independent once their output starts are known: counted and
+  // filled on the host's threads (the same arrays as one pass in row order)
   l_ai[0] = base;
   u_ai[0] = base;
+#pragma omp parallel for schedule(static)
   for (int i = 0; i < n; i++) {
+    int lc = 0, uc = 0;
+    for (int k = ai[i] - base; k < ai[i + 1] - base; k++) {
+      const int c = aj[k] - base;
+      lc += c < i;
+      uc += c > i;
+    }
+    l_ai[i + 1] = lc;
+    u_ai[i + 1] = uc;
+  }
+  for (int i = 0; i < n; i++) {
+    l_ai[i + 1] += l_ai[i];
+    u_ai[i + 1] += u_ai[i];
+  }
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; i++) {
+    int lp = l_ai[i] - base, up = u_ai[i] - base;
     d[i] = 0;
     for (int k = ai[i] - base; k < ai[i + 1] - base; k++) {
       const int c = aj[k] - base;
@@ -302,29 +395,35 @@ void split_ldu(int n, int base, const int *ai, const int *aj, const double *av,
         d[i] = av[k];
       }
     }
-    l_ai[i + 1] = lp + base;
-    u_ai[i + 1] = up + base;
   }
-  *lnnz = lp;
-  *unnz = up;
+  *lnnz = l_ai[n] - base;
+  *unnz = u_ai[n] - base;
 }
 
 // matrix_utils.hpp:805-879 SplitTriangle<L|U>: the triangle incl. diagonal.
 int split_triangle(int uplo, int n, int base, const int *ai, const int *aj,
                    const double *av, int *t_ai, int *t_aj, double *t_av) {
-  int p = 0;
+  auto keep = [uplo](int c, int i) { return uplo == LA_UPPER ? c >= i : c <= i; };
   t_ai[0] = base;
+#pragma omp parallel for schedule(static)
   for (int i = 0; i < n; i++) {
-    for (int k = ai[i] - base; k < ai[i + 1] - base; k++) {
-      const int c = aj[k] - base;
-      if (uplo == LA_UPPER ? c >= i : c <= i) {
+    int cnt = 0;
+    for (int k = ai[i] - base; k < ai[i + 1] - base; k++)
+      cnt += keep(aj[k] - base, i);
+    t_ai[i + 1] = cnt;
+  }
+  for (int i = 0; i < n; i++)
+    t_ai[i + 1] += t_ai[i];
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; i++) {
+    int p = t_ai[i] - base;
+    for (int k = ai[i] - base; k < ai[i + 1] - base; k++)
+      if (keep(aj[k] - base, i)) {
         t_aj[p] = aj[k];
         t_av[p++] = av[k];
       }
-    }
-    t_ai[i + 1] = p + base;
   }
-  return p;
+  return t_ai[n] - base;
 }
 
 // precond.hpp:615-693 ICCLevelNumeric on the IC(0) pattern (the upper

@@ -136,8 +136,18 @@ la_status rcm(int n, int base, const int *ai, const int *aj, int *iperm, int *pe
 // row j for every stored (i, j) of dep_ptr/dep_col, which carry `base`), so
 // the parts' dependency graph is acyclic.  xadj/adj: the 0-based undirected
 // graph; lvl: the rows' levels.  Returns the number of coordinates used.
+// device: the landmark searches run on the GPU (bfs_device_*; same
+// distances), else on the host's threads.
 int monotone_partition(int n, const int *xadj, const int *adj, const int *dep_ptr,
-                       const int *dep_col, int base, const int *lvl, int nparts, int *part);
+                       const int *dep_col, int base, const int *lvl, int nparts, int *part,
+                       bool device = false);
+// Breadth-first distances on the GPU over one 0-based undirected graph, for
+// any number of sources (la_rcm.cu's cooperative search): d[v] = distance
+// from src, -1 where unreachable; *reached = vertices reached.
+struct BfsDevice;
+BfsDevice *bfs_device_create(int n, const int *xadj, const int *adj, la_status *st);
+la_status bfs_device_dist(BfsDevice *B, int src, int *d, int *reached);
+void bfs_device_destroy(BfsDevice *B);
 // The triangle's pattern made undirected and 0-based (both directions of
 // every stored entry), the graph monotone_partition walks.
 void undirected_pattern(int n, int base, const int *ai, const int *aj, std::vector<int> &xadj,

@@ -31,6 +31,7 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <functional>
 #include <numeric>
 #include <vector>
 
@@ -83,29 +84,61 @@ int bfs_dist(int n, const int *xadj, const int *adj, int src, std::vector<int> &
 
 } // namespace
 
+// Vertex v's neighbours: its own row's columns, then the rows that store v
+// (the transpose's row v, ascending), both 0-based; built on the host's
+// threads from the transpose.
 void undirected_pattern(int n, int base, const int *ai, const int *aj, std::vector<int> &xadj,
                         std::vector<int> &adj) {
+  const int nnz = ai[n] - base;
+  std::vector<int> t_ai(n + 1), t_aj(std::max(nnz, 1));
+  transpose(n, n, base, ai, aj, nullptr, t_ai.data(), t_aj.data(), nullptr);
   xadj.assign(n + 1, 0);
-  adj.resize(2 * (size_t)(ai[n] - base));
-  for (int i = 0; i < n; i++)
-    for (int k = ai[i] - base; k < ai[i + 1] - base; k++) {
-      xadj[i + 1]++;
-      xadj[aj[k] - base + 1]++;
-    }
-  std::partial_sum(xadj.begin(), xadj.end(), xadj.begin());
-  std::vector<int> fill(xadj.begin(), xadj.end() - 1);
-  for (int i = 0; i < n; i++)
-    for (int k = ai[i] - base; k < ai[i + 1] - base; k++) {
-      const int j = aj[k] - base;
-      adj[fill[i]++] = j;
-      adj[fill[j]++] = i;
-    }
+  adj.resize(2 * (size_t)nnz);
+  for (int v = 0; v < n; v++)
+    xadj[v + 1] = xadj[v] + (ai[v + 1] - ai[v]) + (t_ai[v + 1] - t_ai[v]);
+#pragma omp parallel for schedule(dynamic, 4096)
+  for (int v = 0; v < n; v++) {
+    int w = xadj[v];
+    for (int k = ai[v] - base; k < ai[v + 1] - base; k++)
+      adj[w++] = aj[k] - base;
+    for (int k = t_ai[v] - base; k < t_ai[v + 1] - base; k++)
+      adj[w++] = t_aj[k] - base;
+  }
 }
 
 int monotone_partition(int n, const int *xadj, const int *adj, const int *dep_ptr,
-                       const int *dep_col, int base, const int *lvl, int nparts, int *part) {
+                       const int *dep_col, int base, const int *lvl, int nparts, int *part,
+                       bool device) {
   if (n == 0)
     return 0;
+  // the landmark searches: on the GPU when asked (one upload of the graph,
+  // a cooperative launch per search), else on the host's threads
+  BfsDevice *bdev = nullptr;
+  struct Owner {
+    BfsDevice *&b;
+    ~Owner() {
+      if (b)
+        bfs_device_destroy(b);
+    }
+  } own{bdev};
+  if (device) {
+    la_status st = LA_OK;
+    bdev = bfs_device_create(n, xadj, adj, &st);
+    if (!bdev)
+      cudaGetLastError(); // e.g. out of memory: the host's searches instead
+  }
+  auto search = [&](int src, std::vector<int> &d) {
+    if (bdev) {
+      d.resize(n);
+      int reached = 0;
+      if (bfs_device_dist(bdev, src, d.data(), &reached) == LA_OK)
+        return reached;
+      bfs_device_destroy(bdev); // a failed search: the host's from here on
+      bdev = nullptr;
+      cudaGetLastError();
+    }
+    return bfs_dist(n, xadj, adj, src, d);
+  };
   std::vector<std::vector<int>> coords; // chosen coordinates
   std::vector<std::vector<double>> basis;
   // candidate: orientation-normalised values, ascending range order later
@@ -124,7 +157,7 @@ int monotone_partition(int n, const int *xadj, const int *adj, const int *dep_pt
       if (xadj[v + 1] - xadj[v] == dmin)
         low.push_back(v);
     std::vector<int> d, mind;
-    bool connected = bfs_dist(n, xadj, adj, low[0], d) == n;
+    bool connected = search(low[0], d) == n;
     if (connected) {
       dist.push_back(d);
       mind = d;
@@ -135,8 +168,9 @@ int monotone_partition(int n, const int *xadj, const int *adj, const int *dep_pt
             best = v;
         if (best < 0 || mind[best] == 0)
           break;
-        bfs_dist(n, xadj, adj, best, d);
+        search(best, d);
         dist.push_back(d);
+#pragma omp parallel for schedule(static)
         for (int v = 0; v < n; v++)
           mind[v] = std::min(mind[v], d[v]);
       }
@@ -187,40 +221,55 @@ int monotone_partition(int n, const int *xadj, const int *adj, const int *dep_pt
                      [](const Cand &x, const Cand &y) { return x.range < y.range; });
   }
   // greedy selection: narrowest first, each with a Gram-Schmidt residual of
-  // at least half its norm against those already chosen
+  // at least half its norm against those already chosen.  The sums run over
+  // fixed 64K-vertex chunks on the host's threads and add the chunks' sums in
+  // chunk order, so they do not depend on the number of threads.
+  auto chunked_sum = [n](auto term) {
+    constexpr int kChunk = 1 << 16;
+    const int nc = (n + kChunk - 1) / kChunk;
+    std::vector<double> part(nc);
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < nc; c++) {
+      double s = 0;
+      for (int v = c * kChunk; v < std::min(n, (c + 1) * kChunk); v++)
+        s += term(v);
+      part[c] = s;
+    }
+    double s = 0;
+    for (double x : part)
+      s += x;
+    return s;
+  };
   for (const Cand &c : cands) {
     if (coords.size() == 3)
       break;
     std::vector<int> f(n);
-    for (int v = 0; v < n; v++)
+    long long fsum = 0; // integer: exact in any order
+#pragma omp parallel for schedule(static) reduction(+ : fsum)
+    for (int v = 0; v < n; v++) {
       f[v] = c.a < 0 ? lvl[v] : c.sign * (dist[c.a][v] - dist[c.b][v]);
-    double mean = 0, var = 0;
-    for (int v = 0; v < n; v++)
-      mean += f[v];
-    mean /= n;
-    for (int v = 0; v < n; v++)
-      var += (f[v] - mean) * (f[v] - mean);
-    var /= n;
+      fsum += f[v];
+    }
+    const double mean = (double)fsum / n;
+    const double var =
+        chunked_sum([&](int v) { return (f[v] - mean) * (f[v] - mean); }) / n;
     if (var <= 0)
       continue;
     const double sd = std::sqrt(var);
     std::vector<double> r(n);
+#pragma omp parallel for schedule(static)
     for (int v = 0; v < n; v++)
       r[v] = (f[v] - mean) / sd;
     for (const std::vector<double> &q : basis) {
-      double dot = 0;
-      for (int v = 0; v < n; v++)
-        dot += r[v] * q[v];
-      dot /= n;
+      const double dot = chunked_sum([&](int v) { return r[v] * q[v]; }) / n;
+#pragma omp parallel for schedule(static)
       for (int v = 0; v < n; v++)
         r[v] -= dot * q[v];
     }
-    double nr = 0;
-    for (int v = 0; v < n; v++)
-      nr += r[v] * r[v];
-    nr = std::sqrt(nr / n);
+    const double nr = std::sqrt(chunked_sum([&](int v) { return r[v] * r[v]; }) / n);
     if (nr < 0.5)
       continue;
+#pragma omp parallel for schedule(static)
     for (int v = 0; v < n; v++)
       r[v] /= nr;
     basis.push_back(std::move(r));
@@ -229,49 +278,45 @@ int monotone_partition(int n, const int *xadj, const int *adj, const int *dep_pt
   dist.clear();
   basis.clear();
 
-  // k-d tree of value-threshold cuts
+  // k-d tree of value-threshold cuts; the two halves of a node are cut as
+  // independent tasks on the host's threads (disjoint ranges of `order`)
   std::vector<int> order(n);
   std::iota(order.begin(), order.end(), 0);
-  struct Task {
-    int lo, hi, k, p0;
-  };
-  std::vector<Task> stack{{0, n, std::max(1, nparts), 0}};
-  std::vector<long long> hist;
-  while (!stack.empty()) {
-    const Task t = stack.back();
-    stack.pop_back();
-    if (t.k == 1 || t.hi - t.lo <= 1) {
-      for (int q = t.lo; q < t.hi; q++)
-        part[order[q]] = t.p0;
+  std::function<void(int, int, int, int)> split = [&](int lo, int hi, int k, int p0) {
+    if (k == 1 || hi - lo <= 1) {
+      for (int q = lo; q < hi; q++)
+        part[order[q]] = p0;
       // a single row split further leaves parts empty
-      continue;
+      return;
     }
-    const int k1 = t.k / 2;
-    const long long want = (long long)(t.hi - t.lo) * k1 / t.k;
+    const int k1 = k / 2;
+    const long long want = (long long)(hi - lo) * k1 / k;
     // coordinates by span, widest first; take the first that splits
     std::vector<std::pair<long long, int>> spans;
+    std::vector<int> lows;
     for (int a = 0; a < (int)coords.size(); a++) {
-      int lo = INT_MAX, hi = INT_MIN;
-      for (int q = t.lo; q < t.hi; q++) {
+      int mn = INT_MAX, mx = INT_MIN;
+      for (int q = lo; q < hi; q++) {
         const int f = coords[a][order[q]];
-        lo = std::min(lo, f);
-        hi = std::max(hi, f);
+        mn = std::min(mn, f);
+        mx = std::max(mx, f);
       }
-      spans.push_back({(long long)hi - lo, a});
+      spans.push_back({(long long)mx - mn, a});
+      lows.push_back(mn);
     }
-    std::sort(spans.begin(), spans.end(), [](auto &x, auto &y) { return x.first > y.first; });
+    std::stable_sort(spans.begin(), spans.end(),
+                     [](auto &x, auto &y) { return x.first > y.first; });
     int cut = -1;
+    std::vector<long long> hist;
     for (const auto &sa : spans) {
       if (sa.first == 0)
         break;
       const std::vector<int> &f = coords[sa.second];
-      int lo = INT_MAX;
-      for (int q = t.lo; q < t.hi; q++)
-        lo = std::min(lo, f[order[q]]);
+      const int mn = lows[sa.second];
       // histogram of the node's values; the threshold keeps f < thr low
       hist.assign((size_t)sa.first + 2, 0);
-      for (int q = t.lo; q < t.hi; q++)
-        hist[f[order[q]] - lo]++;
+      for (int q = lo; q < hi; q++)
+        hist[f[order[q]] - mn]++;
       long long below = 0, bdev = LLONG_MAX;
       int thr = 0;
       bool found = false;
@@ -280,27 +325,38 @@ int monotone_partition(int n, const int *xadj, const int *adj, const int *dep_pt
         if (hist[v] == 0 && v + 1 < hist.size())
           continue; // only thresholds just below a present value
         const long long dev = std::llabs(below - want);
-        if (below > 0 && below < t.hi - t.lo && dev < bdev) {
+        if (below > 0 && below < hi - lo && dev < bdev) {
           bdev = dev;
-          thr = lo + (int)v;
+          thr = mn + (int)v;
           found = true;
         }
       }
       if (!found)
         continue;
-      const auto mid = std::stable_partition(order.begin() + t.lo, order.begin() + t.hi,
+      const auto mid = std::stable_partition(order.begin() + lo, order.begin() + hi,
                                              [&](int v) { return f[v] < thr; });
       cut = (int)(mid - order.begin());
       break;
     }
     if (cut < 0) { // no coordinate separates these rows: keep them together
-      for (int q = t.lo; q < t.hi; q++)
-        part[order[q]] = t.p0;
-      continue;
+      for (int q = lo; q < hi; q++)
+        part[order[q]] = p0;
+      return;
     }
-    stack.push_back({cut, t.hi, t.k - k1, t.p0 + k1});
-    stack.push_back({t.lo, cut, k1, t.p0});
-  }
+    if (hi - lo >= (1 << 15)) {
+#pragma omp task shared(split)
+      split(lo, cut, k1, p0);
+#pragma omp task shared(split)
+      split(cut, hi, k - k1, p0 + k1);
+#pragma omp taskwait
+    } else {
+      split(lo, cut, k1, p0);
+      split(cut, hi, k - k1, p0 + k1);
+    }
+  };
+#pragma omp parallel
+#pragma omp single
+  split(0, n, std::max(1, nparts), 0);
   return (int)coords.size();
 }
 

@@ -25,6 +25,7 @@
 
 #include <cmath>
 #include <cstdlib>
+#include <memory>
 #include <utility>
 
 namespace la {
@@ -540,19 +541,26 @@ la_status pcg_create(la_csr_t A, const int *u_ai, const int *u_aj,
   };
   // Preconditioner factors: strict U + diag, and strict L = U^T (same diag).
   const int unnz = u_ai[n] - base;
-  std::vector<int> l_ai(n + 1), l_aj(std::max(unnz, 1)), s_ai(n + 1),
-      s_aj(std::max(unnz, 1)), t_ai(n + 1), t_aj(std::max(unnz, 1));
-  std::vector<double> l_av(std::max(unnz, 1)), s_av(std::max(unnz, 1)),
-      t_av(std::max(unnz, 1)), d(n);
-  int lnnz = 0, snnz = 0;
-  split_ldu(n, base, u_ai, u_aj, icc_av, l_ai.data(), l_aj.data(), l_av.data(),
-            d.data(), s_ai.data(), s_aj.data(), s_av.data(), &lnnz, &snnz);
-  if (lnnz != 0) {
+  bool lower = false; // an entry below the diagonal: not an IC factor
+#pragma omp parallel for schedule(static) reduction(|| : lower)
+  for (int i = 0; i < n; i++)
+    for (int k = u_ai[i] - base; k < u_ai[i + 1] - base; k++)
+      lower = lower || u_aj[k] - base < i;
+  if (lower) {
     set_error("IC factor must be upper triangular");
     return fail(LA_ERR_INVALID_ARG);
   }
-  transpose(n, n, base, s_ai.data(), s_aj.data(), s_av.data(), t_ai.data(),
-            t_aj.data(), t_av.data());
+  // scratch left uninitialised: every entry is written before it is read
+  const size_t m = std::max(unnz, 1);
+  std::unique_ptr<int[]> s_aj(new int[m]), t_aj(new int[m]);
+  std::unique_ptr<double[]> s_av(new double[m]), t_av(new double[m]);
+  std::vector<int> l_ai(n + 1), l_aj(1), s_ai(n + 1), t_ai(n + 1);
+  std::vector<double> l_av(1), d(n);
+  int lnnz = 0, snnz = 0;
+  split_ldu(n, base, u_ai, u_aj, icc_av, l_ai.data(), l_aj.data(), l_av.data(), d.data(),
+            s_ai.data(), s_aj.get(), s_av.get(), &lnnz, &snnz);
+  transpose(n, n, base, s_ai.data(), s_aj.get(), s_av.get(), t_ai.data(), t_aj.get(),
+            t_av.get());
   const la_dtype fd = mode == LA_PCG_MIXED ? LA_F32 : LA_F64;
   la_status s;
   S->L = new la_trsv_plan_s();
@@ -562,7 +570,7 @@ la_status pcg_create(la_csr_t A, const int *u_ai, const int *u_aj,
   S->L->uplo = LA_LOWER;
   S->L->dtype = fd;
   S->L->unit = false;
-  if ((s = trsv_build(S->L, t_ai.data(), t_aj.data(), t_av.data(), d.data())) != LA_OK)
+  if ((s = trsv_build(S->L, t_ai.data(), t_aj.get(), t_av.get(), d.data())) != LA_OK)
     return fail(s);
   S->U = new la_trsv_plan_s();
   S->U->n = n;
@@ -571,7 +579,7 @@ la_status pcg_create(la_csr_t A, const int *u_ai, const int *u_aj,
   S->U->uplo = LA_UPPER;
   S->U->dtype = fd;
   S->U->unit = false;
-  if ((s = trsv_build(S->U, s_ai.data(), s_aj.data(), s_av.data(), d.data())) != LA_OK)
+  if ((s = trsv_build(S->U, s_ai.data(), s_aj.get(), s_av.get(), d.data())) != LA_OK)
     return fail(s);
   S->Ap = new la_spmv_plan_s();
   S->Ap->A = A;

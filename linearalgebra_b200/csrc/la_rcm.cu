@@ -275,7 +275,8 @@ struct RcmDevice {
     const int nnz = h_ai[n] - base;
     LA_TRY(ai.upload(h_ai, sizeof(int) * (n + 1)));
     LA_TRY(aj.upload(h_aj, sizeof(int) * std::max(nnz, 1)));
-    LA_TRY(deg.upload(h_deg, sizeof(int) * n));
+    if (h_deg) // the searches alone (bfs_device_*) need no degrees
+      LA_TRY(deg.upload(h_deg, sizeof(int) * n));
     for (DevBuf *b : {&level, &queue, &pos, &parent, &cm, &cnt})
       LA_TRY(b->alloc(sizeof(int) * n));
     LA_TRY(lstart.alloc(sizeof(int) * (n + 2)));
@@ -397,6 +398,33 @@ RcmDevice *rcm_device_create(int n, int base, const int *ai, const int *aj, cons
 }
 
 void rcm_device_destroy(RcmDevice *D) { delete D; }
+
+struct BfsDevice {
+  RcmDevice D;
+  int reached = 0;
+};
+
+BfsDevice *bfs_device_create(int n, const int *xadj, const int *adj, la_status *st) {
+  auto *B = new BfsDevice();
+  *st = B->D.init(n, 0, xadj, adj, nullptr);
+  if (*st != LA_OK) {
+    delete B;
+    return nullptr;
+  }
+  return B;
+}
+
+la_status bfs_device_dist(BfsDevice *B, int src, int *d, int *reached) {
+  std::vector<int> ls;
+  int height = 0;
+  LA_TRY(B->D.bfs(src, B->reached, ls, &height));
+  // level[] holds the distances of this search's vertices, -1 elsewhere
+  LA_CUDA_TRY(cudaMemcpy(d, B->D.level.p, sizeof(int) * B->D.n, cudaMemcpyDeviceToHost));
+  *reached = B->reached;
+  return LA_OK;
+}
+
+void bfs_device_destroy(BfsDevice *B) { delete B; }
 
 // One component (members ascending, more than two nodes): its Cuthill-McKee
 // order, node + base, into out[0, size).

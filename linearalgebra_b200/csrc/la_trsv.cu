@@ -51,6 +51,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <numeric>
 #include <vector>
@@ -724,18 +725,21 @@ struct PartEntry {
 };
 std::vector<PartEntry> g_part_cache; // most recent last, at most 4
 
-void cached_partition(int n, const std::vector<int> &xadj, const std::vector<int> &adj,
-                      const int *ai, const int *aj, int base, const std::vector<int> &lvl,
-                      int nparts, std::vector<int> &part) {
+void cached_partition(int n, const int *ai, const int *aj, int base,
+                      const std::vector<int> &lvl, int nparts, std::vector<int> &part) {
+  // the key: a sum over the stored entries, each hashed as its undirected
+  // edge (smaller row first) -- the same for a triangle and its transpose,
+  // independent of the order, and computed in parallel (integer sums)
   unsigned long long h = 0x9e3779b97f4a7c15ull * (unsigned long long)(n + 1);
+#pragma omp parallel for schedule(static) reduction(+ : h)
   for (int i = 0; i < n; i++)
-    for (int k = xadj[i]; k < xadj[i + 1]; k++) {
-      const int j = adj[k];
-      if (j <= i)
-        continue;
-      unsigned long long z = (unsigned long long)i * 0x100000001b3ull ^ (unsigned long long)j;
+    for (int k = ai[i] - base; k < ai[i + 1] - base; k++) {
+      const int j = aj[k] - base;
+      const unsigned long long a = (unsigned long long)std::min(i, j),
+                               b = (unsigned long long)std::max(i, j);
+      unsigned long long z = a * 0x100000001b3ull ^ b;
       z = (z ^ (z >> 31)) * 0xbf58476d1ce4e5b9ull;
-      h += z ^ (z >> 29); // sum: independent of the edge order
+      h += z ^ (z >> 29);
     }
   {
     std::lock_guard<std::mutex> lock(g_part_mu);
@@ -745,8 +749,11 @@ void cached_partition(int n, const std::vector<int> &xadj, const std::vector<int
         return;
       }
   }
+  std::vector<int> xadj, adj;
+  undirected_pattern(n, base, ai, aj, xadj, adj);
   part.assign(n, 0);
-  monotone_partition(n, xadj.data(), adj.data(), ai, aj, base, lvl.data(), nparts, part.data());
+  monotone_partition(n, xadj.data(), adj.data(), ai, aj, base, lvl.data(), nparts, part.data(),
+                     true);
   std::lock_guard<std::mutex> lock(g_part_mu);
   if (g_part_cache.size() == 4)
     g_part_cache.erase(g_part_cache.begin());
@@ -768,15 +775,13 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
   int nparts = std::min(sm_count(), std::max(1, (n + 2047) / 2048));
   if (const char *e = std::getenv("LA_TRSV_PARTS")) // tuning override
     nparts = std::max(1, std::min(sm_count(), std::atoi(e)));
-  // rows' levels, and the triangle's graph made undirected
+  // rows' levels, then the partition (of the triangle's graph made undirected)
   std::vector<int> lvl(n);
   for (int l = 0; l < P->levels; l++)
     for (int p = P->h_prefix[l]; p < P->h_prefix[l + 1]; p++)
       lvl[P->h_iperm[p] - base] = l;
-  std::vector<int> xadj, adj;
-  undirected_pattern(n, base, ai, aj, xadj, adj);
   std::vector<int> part;
-  cached_partition(n, xadj, adj, ai, aj, base, lvl, nparts, part);
+  cached_partition(n, ai, aj, base, lvl, nparts, part);
   std::vector<int> pstart(nparts + 1, 0);
   for (int i = 0; i < n; i++)
     pstart[part[i] + 1]++;
@@ -941,21 +946,31 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
   // g + 2 minus the ring size: d's slot is refilled by row d + ring, whose b
   // is copied in while level (d + ring's level) - 2 is still being solved, so
   // d + ring must lie beyond level g + 2.  Older rows are read from x.
+  // Values go straight into the solve's type X (the same rounding as a
+  // conversion afterwards).  Scratch is left uninitialised: each row writes
+  // all of its own cells, on the host's threads.
   const size_t cells = (size_t)ks * n;
-  std::vector<int> ej(cells, kEmptySlot);
-  std::vector<double> ev(cells, 0.0), ediag(n, 1.0);
-  std::vector<int> eai, eaj;
-  std::vector<double> eav;
+  std::unique_ptr<int[]> ej(new int[cells]);
+  std::unique_ptr<X[]> ev(new X[cells]), ediag(new X[std::max(n, 1)]);
+  std::vector<int> eai;
+  std::unique_ptr<int[]> eaj;
+  std::unique_ptr<X[]> eav;
   if (!kd) {
     eai.assign(n + 1, 0);
-    eaj.resize(std::max(nnz, 1));
-    eav.resize(std::max(nnz, 1));
+    for (int r = 0; r < n; r++)
+      eai[r + 1] = eai[r] + (ai[erow[r] + 1] - ai[erow[r]]);
+    eaj.reset(new int[std::max(nnz, 1)]);
+    eav.reset(new X[std::max(nnz, 1)]);
   }
-  int w = 0;
+#pragma omp parallel for schedule(dynamic, 4096)
   for (int r = 0; r < n; r++) {
     const int i = erow[r], pi = part[i];
-    if (diag)
-      ediag[r] = diag[i];
+    ediag[r] = diag ? (X)diag[i] : (X)1;
+    for (int s = 0; s < ks; s++) {
+      ej[(size_t)s * n + r] = kEmptySlot;
+      ev[(size_t)s * n + r] = (X)0;
+    }
+    int w = kd ? 0 : eai[r];
     for (int k = ai[i] - base, s = 0; k < ai[i + 1] - base; k++, s++, w++) {
       const int j = aj[k] - base;
       int c = j;
@@ -968,19 +983,18 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
       }
       if (s < ks) {
         ej[(size_t)s * n + r] = c;
-        ev[(size_t)s * n + r] = av[k];
+        ev[(size_t)s * n + r] = (X)av[k];
       }
       if (!kd) {
         eaj[w] = c;
-        eav[w] = av[k];
+        eav[w] = (X)av[k];
       }
     }
-    if (!kd)
-      eai[r + 1] = w;
   }
   if (!kd) {
     LA_TRY(P->ai.upload(eai.data(), sizeof(int) * eai.size()));
-    LA_TRY(P->aj.upload(eaj.data(), sizeof(int) * eaj.size()));
+    LA_TRY(P->aj.upload(eaj.get(), sizeof(int) * std::max(nnz, 1)));
+    LA_TRY(P->av.upload(eav.get(), sizeof(X) * std::max(nnz, 1)));
   }
   // Testing override (the partitioned kernel's bounded wait): the first row
   // with a stored entry reads its own value through global memory instead,
@@ -993,25 +1007,13 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
           ej[r] = erow[r];
           break;
         }
-  LA_TRY(P->ej.upload(ej.data(), sizeof(int) * cells));
+  LA_TRY(P->ej.upload(ej.get(), sizeof(int) * cells));
   LA_TRY(P->exec_row.upload(erow.data(), sizeof(int) * erow.size()));
   LA_TRY(P->pstart.upload(pstart.data(), sizeof(int) * pstart.size()));
   LA_TRY(P->psub.upload(psub.data(), sizeof(int) * psub.size()));
   LA_TRY(P->sb.upload(sb.data(), sizeof(int) * sb.size()));
-  if (P->dtype == LA_F64) {
-    if (!kd)
-      LA_TRY(P->av.upload(eav.data(), sizeof(double) * eav.size()));
-    LA_TRY(P->ev.upload(ev.data(), sizeof(double) * cells));
-    LA_TRY(P->diag.upload(ediag.data(), sizeof(double) * n));
-  } else {
-    if (!kd) {
-      std::vector<float> f(eav.begin(), eav.end());
-      LA_TRY(P->av.upload(f.data(), sizeof(float) * f.size()));
-    }
-    std::vector<float> f(ev.begin(), ev.end()), fd(ediag.begin(), ediag.end());
-    LA_TRY(P->ev.upload(f.data(), sizeof(float) * cells));
-    LA_TRY(P->diag.upload(fd.data(), sizeof(float) * n));
-  }
+  LA_TRY(P->ev.upload(ev.get(), sizeof(X) * cells));
+  LA_TRY(P->diag.upload(ediag.get(), sizeof(X) * n));
   P->kd = kd;
   P->nparts = nparts;
   P->part_rows = ring ? ring : rows_max;
@@ -1084,20 +1086,28 @@ la_status trsv_build(la_trsv_plan_t P, const int *ai, const int *aj,
       return LA_OK;
   }
   std::vector<int> eai(n + 1), erow(n), cstart;
-  std::vector<int> eaj(std::max(P->nnz, 1));
-  std::vector<double> eav(std::max(P->nnz, 1)), ediag(n, 1.0);
+  // filled below on the host's threads, every entry written: no initialisation
+  std::unique_ptr<int[]> eaj(new int[std::max(P->nnz, 1)]);
+  std::unique_ptr<double[]> eav(new double[std::max(P->nnz, 1)]);
+  std::vector<double> ediag(n, 1.0);
+  eaj[0] = 0; // the one placeholder entry of an empty triangle
+  eav[0] = 0;
   eai[0] = base;
-  int w = 0;
   for (int p = 0; p < n; p++) {
     const int i = P->h_iperm[p] - base;
     erow[p] = i;
+    eai[p + 1] = eai[p] + (ai[i + 1] - ai[i]);
+  }
+  // rows in execution order, copied on the host's threads
+#pragma omp parallel for schedule(dynamic, 4096)
+  for (int p = 0; p < n; p++) {
+    const int i = erow[p];
     if (diag)
       ediag[p] = diag[i];
-    for (int k = ai[i] - base; k < ai[i + 1] - base; k++, w++) {
+    for (int k = ai[i] - base, w = eai[p] - base; k < ai[i + 1] - base; k++, w++) {
       eaj[w] = aj[k];
       eav[w] = av[k];
     }
-    eai[p + 1] = w + base;
   }
   int longest = 0;
   for (int p = 0; p < n; p++)
@@ -1109,15 +1119,15 @@ la_status trsv_build(la_trsv_plan_t P, const int *ai, const int *aj,
   cstart.push_back(n);
   P->nchunks = (int)cstart.size() - 1;
   LA_TRY(P->ai.upload(eai.data(), sizeof(int) * eai.size()));
-  LA_TRY(P->aj.upload(eaj.data(), sizeof(int) * eaj.size()));
+  LA_TRY(P->aj.upload(eaj.get(), sizeof(int) * std::max(P->nnz, 1)));
   LA_TRY(P->exec_row.upload(erow.data(), sizeof(int) * erow.size()));
   LA_TRY(P->chunk_start.upload(cstart.data(), sizeof(int) * cstart.size()));
   if (P->dtype == LA_F64) {
-    LA_TRY(P->av.upload(eav.data(), sizeof(double) * eav.size()));
+    LA_TRY(P->av.upload(eav.get(), sizeof(double) * std::max(P->nnz, 1)));
     LA_TRY(P->diag.upload(ediag.data(), sizeof(double) * n));
     P->grid = grid_for<double, double>(P->nchunks, P->kd);
   } else {
-    std::vector<float> f(eav.begin(), eav.end()), fd(ediag.begin(), ediag.end());
+    std::vector<float> f(eav.get(), eav.get() + std::max(P->nnz, 1)), fd(ediag.begin(), ediag.end());
     LA_TRY(P->av.upload(f.data(), sizeof(float) * f.size()));
     LA_TRY(P->diag.upload(fd.data(), sizeof(float) * n));
     P->grid = grid_for<float, float>(P->nchunks, P->kd);

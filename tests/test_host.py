@@ -147,6 +147,54 @@ def test_split_transpose_permute(lab, golden, orc):
             assert np.array_equal(b_ai, r_ai) and np.array_equal(b_aj, r_aj) and np.array_equal(b_av, r_av)
 
 
+def test_split_transpose_large_threaded(lab, orc):
+    """Above 2^18 entries the transpose, SplitLDU and SplitTriangle run on the
+    host's threads: the same arrays as the one-pass restatements -- the
+    compiled reference's transpose where available, scipy's otherwise, the
+    oracle's SplitTriangle -- on a 27-point stencil (1.7M entries) and a
+    random rectangular pattern with repeated-column-free ragged rows."""
+    import scipy.sparse as sp
+    from linearalgebra_b200 import gen
+    P = orc.ptr
+    n, ai, aj, av = gen.stencil27(40, seed=3)
+    rng = np.random.default_rng(11)
+    # ragged random rows (0 to 14 distinct sorted columns) over 70,000 columns
+    lens = rng.integers(0, 15, 50_000)
+    r_aj = np.concatenate([np.sort(rng.choice(70_000, k, replace=False)) for k in lens])
+    r_ai = np.concatenate([[0], np.cumsum(lens)])
+    cases = [(n, n, np.asarray(ai, np.int32), np.asarray(aj, np.int32), np.asarray(av)),
+             (50_000, 70_000, r_ai.astype(np.int32), r_aj.astype(np.int32),
+              rng.uniform(-1, 1, len(r_aj)))]
+    for m, c, ai, aj, av in cases:
+        assert ai[-1] >= (1 << 18)
+        t_ai, t_aj, t_av = lab.Transpose(m, c, 0, ai, aj, av)
+        T = sp.csr_matrix((av, aj, ai), shape=(m, c)).T.tocsr()
+        T.sort_indices()
+        assert np.array_equal(t_ai, T.indptr) and np.array_equal(t_aj, T.indices)
+        assert np.array_equal(t_av, T.data)
+        rf = orc.ref()
+        if rf is not None and m == c:
+            r_ai, r_aj, r_av = np.empty(m + 1, np.int32), np.empty(len(aj), np.int32), np.empty(len(aj))
+            rf.la_ref_transpose(m, c, 0, P(ai), P(aj), P(av), P(r_ai), P(r_aj), P(r_av))
+            assert np.array_equal(t_ai, r_ai) and np.array_equal(t_aj, r_aj)
+            assert np.array_equal(t_av, r_av)
+    # SplitLDU / SplitTriangle on the square case
+    m, _, ai, aj, av = cases[0]
+    (l_ai, l_aj, l_av), d, (u_ai, u_aj, u_av) = lab.SplitLDU(m, 0, ai, aj, av)
+    for lower, (x_ai, x_aj, x_av) in ((True, (l_ai, l_aj, l_av)), (False, (u_ai, u_aj, u_av))):
+        e_ai, e_aj, e_av = strict_triangle(m, ai, aj, av, lower)
+        assert np.array_equal(x_ai, e_ai) and np.array_equal(x_aj, e_aj)
+        assert np.array_equal(x_av, e_av)
+    rows = np.repeat(np.arange(m), np.diff(ai))
+    assert np.array_equal(d, av[aj == rows])
+    for uplo, code in (("U", 1), ("L", 0)):
+        t_ai, t_aj, t_av = lab.SplitTriangle(uplo, m, 0, ai, aj, av)
+        o_ai, o_aj, o_av = (np.empty(m + 1, np.int32), np.empty(len(aj), np.int32), np.empty(len(aj)))
+        k = orc.port().oracle_split_triangle(code, m, 0, P(ai), P(aj), P(av), P(o_ai), P(o_aj), P(o_av))
+        assert np.array_equal(t_ai, o_ai) and np.array_equal(t_aj, o_aj[:k])
+        assert np.array_equal(t_av, o_av[:k])
+
+
 def test_valid_csr_rejects_bad_input(lab):
     ai = np.array([0, 2, 3], np.int32)
     assert lab.ValidCSR(2, 2, 0, ai, np.array([0, 1, 1], np.int32))
