@@ -378,6 +378,8 @@ void schedule(int n, const Symbolic &S, std::vector<int> &erow, std::vector<int>
   cstart.push_back(n);
 }
 
+la_status plan_finish(la_factor_plan_s *P);
+
 la_status plan_build(la_factor_plan_s *P, const int *ai, const int *aj, Symbolic &S) {
   const int n = P->n;
   std::vector<int> erow, cstart;
@@ -404,6 +406,12 @@ la_status plan_build(la_factor_plan_s *P, const int *ai, const int *aj, Symbolic
   LA_TRY(up(P->pptr, S.pptr));
   LA_TRY(up(P->ptgt, S.ptgt));
   LA_TRY(up(P->psrc, S.psrc));
+  return plan_finish(P);
+}
+
+// The numeric pass's work buffers and grid (either plan builder).
+la_status plan_finish(la_factor_plan_s *P) {
+  const int n = P->n;
   LA_TRY(P->vin.alloc(sizeof(double) * std::max(P->nnz, 1)));
   LA_TRY(P->done.alloc(sizeof(int) * std::max(n, 1)));
   LA_TRY(P->state.alloc(sizeof(int) * 4));
@@ -417,6 +425,239 @@ la_status plan_build(la_factor_plan_s *P, const int *ai, const int *aj, Symbolic
     per_sm = std::min(per_sm, std::max(1, std::atoi(e)));
   const int need = (P->nchunks + kFactorThreads / 32 - 1) / (kFactorThreads / 32);
   P->grid = std::max(1, std::min(per_sm * sm_count(), need));
+  return LA_OK;
+}
+
+// ---- The IC(0) plan built on the device (large patterns).  The same
+// lists as symbolic_ic0 + schedule, step for step: each row's updates are
+// the strict upper entries of its column (counted, placed in any order,
+// then insertion-sorted per row by update_before), the pairs are counted,
+// scanned and written per update, the levels come from the depth solve
+// over the updates, and the rows are sorted by (level, row) with 32-row
+// chunks inside levels.  Integer work only: the plan equals the host's.
+
+constexpr int kDevicePlanRows = 65536; // smaller patterns: the host's plan
+constexpr int kDeviceSortMax = 512;    // a longer update list: the host's plan
+
+int plan_grid(int n) { return std::max(1, std::min((n + 255) / 256, 8 * sm_count())); }
+
+__global__ void sym_rebase_kernel(const int m, const int base, int *v) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+    v[i] -= base;
+}
+
+// cnt[c] = strict upper entries in column c
+__global__ void sym_col_count_kernel(const int n, const int *__restrict__ ai,
+                                     const int *__restrict__ aj, int *cnt) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    for (int e = ai[k] + 1; e < ai[k + 1]; e++)
+      atomicAdd(cnt + aj[e], 1);
+}
+
+// each strict upper entry e = (k, c) becomes an update of row c (any order)
+__global__ void sym_col_fill_kernel(const int n, const int *__restrict__ ai,
+                                    const int *__restrict__ aj, int *cursor, int *uk, int *us) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    for (int e = ai[k] + 1; e < ai[k + 1]; e++) {
+      const int q = atomicAdd(cursor + aj[e], 1);
+      uk[q] = k;
+      us[q] = e;
+    }
+}
+
+// update_before on the device (the same rule)
+__device__ bool update_before_dev(const int *__restrict__ aj, int px, int lx, int py, int ly) {
+  for (bool flip = false;; flip = !flip) {
+    const int cx = __ldg(aj + px), cy = __ldg(aj + py);
+    if (cx != cy)
+      return (cx > cy) != flip;
+    if (px == lx)
+      return !flip;
+    if (py == ly)
+      return flip;
+    px--;
+    py--;
+  }
+}
+
+// row j's updates sorted in place (insertion sort on its own slice)
+__global__ void sym_order_kernel(const int n, const int *__restrict__ ai,
+                                 const int *__restrict__ aj, const int *__restrict__ uptr,
+                                 int *uk, int *us, int *too_long) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const int u0 = uptr[j], u1 = uptr[j + 1];
+    if (u1 - u0 > kDeviceSortMax) {
+      atomicExch(too_long, 1);
+      continue;
+    }
+    for (int u = u0 + 1; u < u1; u++) {
+      const int e = us[u], k = uk[u], lk = ai[k];
+      int w = u;
+      while (w > u0) {
+        const int e2 = us[w - 1], k2 = uk[w - 1];
+        if (!update_before_dev(aj, e - 1, lk, e2 - 1, ai[k2]))
+          break;
+        us[w] = e2;
+        uk[w] = k2;
+        w--;
+      }
+      us[w] = e;
+      uk[w] = k;
+    }
+  }
+}
+
+// the pairs of update u of row j: columns of row k from entry us[u] on that
+// row j holds (visit(u, p, ck) per pair, ascending)
+template <typename F>
+__device__ void sym_pairs(const int *__restrict__ ai, const int *__restrict__ aj, int j, int k,
+                          int ck0, F visit) {
+  const int re = ai[j + 1], ke = ai[k + 1];
+  for (int p = ai[j], ck = ck0; ck < ke && p < re;) {
+    const int a = __ldg(aj + ck), b = __ldg(aj + p);
+    if (a == b)
+      visit(p++, ck++);
+    else if (a < b)
+      ck++;
+    else
+      p++;
+  }
+}
+
+__global__ void sym_pair_count_kernel(const int n, const int *__restrict__ ai,
+                                      const int *__restrict__ aj, const int *__restrict__ uptr,
+                                      const int *__restrict__ uk, const int *__restrict__ us,
+                                      int *pcount) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    for (int u = uptr[j]; u < uptr[j + 1]; u++) {
+      int c = 0;
+      sym_pairs(ai, aj, j, uk[u], us[u], [&](int, int) { c++; });
+      pcount[u] = c;
+    }
+}
+
+__global__ void sym_pair_fill_kernel(const int n, const int *__restrict__ ai,
+                                     const int *__restrict__ aj, const int *__restrict__ uptr,
+                                     const int *__restrict__ uk, const int *__restrict__ us,
+                                     const int *__restrict__ pptr, int *ptgt, int *psrc) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    for (int u = uptr[j]; u < uptr[j + 1]; u++) {
+      int w = pptr[u];
+      sym_pairs(ai, aj, j, uk[u], us[u], [&](int p, int ck) {
+        ptgt[w] = p;
+        psrc[w++] = ck;
+      });
+    }
+}
+
+// flag[p] = 1 where a 32-row chunk starts (level start, then every 32 rows)
+__global__ void chunk_flag_kernel(const int n, const unsigned *__restrict__ level,
+                                  const int *__restrict__ starts, int *flag) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p <= n; p += gridDim.x * blockDim.x)
+    flag[p] = p < n && ((p - starts[level[p]]) & (kFactorChunk - 1)) == 0;
+}
+
+__global__ void chunk_scatter_kernel(const int n, const unsigned *__restrict__ level,
+                                     const int *__restrict__ starts, const int *__restrict__ pos,
+                                     int *chunk_start) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p <= n; p += gridDim.x * blockDim.x)
+    if (p == n)
+      chunk_start[pos[n]] = n;
+    else if (((p - starts[level[p]]) & (kFactorChunk - 1)) == 0)
+      chunk_start[pos[p]] = p;
+}
+
+void take(DevBuf &dst, DevBuf &src) {
+  std::swap(dst.p, src.p);
+  std::swap(dst.bytes, src.bytes);
+}
+
+// *ok = false (nothing built): a row receives more than kDeviceSortMax
+// updates; the caller builds the host's plan instead.
+la_status plan_build_ic0_device(la_factor_plan_s *P, const int *ai, const int *aj, bool *ok) {
+  *ok = false;
+  const int n = P->n, nnz = P->nnz, base = P->base;
+  cudaStream_t st = nullptr;
+  const int g = plan_grid(n);
+  DevBuf dai, daj, uptr, cursor, uk, us, flag, pptr, ptgt, psrc;
+  LA_TRY(dai.upload(ai, sizeof(int) * (n + 1)));
+  LA_TRY(daj.upload(aj, sizeof(int) * std::max(nnz, 1)));
+  sym_rebase_kernel<<<g, 256, 0, st>>>(n + 1, base, dai.as<int>());
+  sym_rebase_kernel<<<plan_grid(nnz), 256, 0, st>>>(nnz, base, daj.as<int>());
+  LA_TRY(uptr.alloc(sizeof(int) * (n + 1)));
+  LA_CUDA_TRY(cudaMemsetAsync(uptr.p, 0, sizeof(int) * (n + 1), st));
+  sym_col_count_kernel<<<g, 256, 0, st>>>(n, dai.as<int>(), daj.as<int>(), uptr.as<int>());
+  LA_CUDA_TRY(cudaGetLastError());
+  LA_TRY(scan_exclusive(uptr.as<int>(), n + 1, st));
+  int nu = 0;
+  LA_CUDA_TRY(cudaMemcpyAsync(&nu, uptr.as<int>() + n, sizeof(int), cudaMemcpyDeviceToHost, st));
+  LA_CUDA_TRY(cudaStreamSynchronize(st));
+  LA_TRY(uk.alloc(sizeof(int) * std::max(nu, 1)));
+  LA_TRY(us.alloc(sizeof(int) * std::max(nu, 1)));
+  LA_TRY(cursor.alloc(sizeof(int) * (n + 1)));
+  LA_CUDA_TRY(cudaMemcpyAsync(cursor.p, uptr.p, sizeof(int) * (n + 1), cudaMemcpyDeviceToDevice,
+                              st));
+  sym_col_fill_kernel<<<g, 256, 0, st>>>(n, dai.as<int>(), daj.as<int>(), cursor.as<int>(),
+                                         uk.as<int>(), us.as<int>());
+  LA_CUDA_TRY(cudaMemsetAsync(cursor.p, 0, sizeof(int), st)); // the too-long flag
+  sym_order_kernel<<<g, 256, 0, st>>>(n, dai.as<int>(), daj.as<int>(), uptr.as<int>(),
+                                      uk.as<int>(), us.as<int>(), cursor.as<int>());
+  LA_CUDA_TRY(cudaGetLastError());
+  int too_long = 0;
+  LA_CUDA_TRY(cudaMemcpyAsync(&too_long, cursor.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  LA_CUDA_TRY(cudaStreamSynchronize(st));
+  if (too_long)
+    return LA_OK;
+  LA_TRY(pptr.alloc(sizeof(int) * ((size_t)nu + 1)));
+  LA_CUDA_TRY(cudaMemsetAsync(pptr.as<int>() + nu, 0, sizeof(int), st));
+  sym_pair_count_kernel<<<g, 256, 0, st>>>(n, dai.as<int>(), daj.as<int>(), uptr.as<int>(),
+                                           uk.as<int>(), us.as<int>(), pptr.as<int>());
+  LA_CUDA_TRY(cudaGetLastError());
+  LA_TRY(scan_exclusive(pptr.as<int>(), nu + 1, st));
+  int npairs = 0;
+  LA_CUDA_TRY(cudaMemcpyAsync(&npairs, pptr.as<int>() + nu, sizeof(int), cudaMemcpyDeviceToHost,
+                              st));
+  LA_CUDA_TRY(cudaStreamSynchronize(st));
+  LA_TRY(ptgt.alloc(sizeof(int) * std::max(npairs, 1)));
+  LA_TRY(psrc.alloc(sizeof(int) * std::max(npairs, 1)));
+  sym_pair_fill_kernel<<<g, 256, 0, st>>>(n, dai.as<int>(), daj.as<int>(), uptr.as<int>(),
+                                          uk.as<int>(), us.as<int>(), pptr.as<int>(),
+                                          ptgt.as<int>(), psrc.as<int>());
+  LA_CUDA_TRY(cudaGetLastError());
+  // levels: row j depends on the rows of its updates, all earlier rows
+  DevBuf order, keys, starts;
+  int lv = 0;
+  LA_TRY(levels_on_device(LA_LOWER, n, 0, uptr.as<int>(), uk.as<int>(), order, keys, starts, &lv,
+                          st));
+  LA_TRY(flag.alloc(sizeof(int) * (n + 1)));
+  chunk_flag_kernel<<<g, 256, 0, st>>>(n, keys.as<unsigned>(), starts.as<int>(), flag.as<int>());
+  LA_CUDA_TRY(cudaGetLastError());
+  LA_TRY(scan_exclusive(flag.as<int>(), n + 1, st));
+  int nchunks = 0;
+  LA_CUDA_TRY(cudaMemcpyAsync(&nchunks, flag.as<int>() + n, sizeof(int), cudaMemcpyDeviceToHost,
+                              st));
+  LA_CUDA_TRY(cudaStreamSynchronize(st));
+  LA_TRY(P->chunk_start.alloc(sizeof(int) * (nchunks + 1)));
+  chunk_scatter_kernel<<<g, 256, 0, st>>>(n, keys.as<unsigned>(), starts.as<int>(),
+                                          flag.as<int>(), P->chunk_start.as<int>());
+  LA_CUDA_TRY(cudaGetLastError());
+  LA_TRY(P->diag.alloc(sizeof(int) * n));
+  LA_CUDA_TRY(cudaMemcpyAsync(P->diag.p, dai.p, sizeof(int) * n, cudaMemcpyDeviceToDevice, st));
+  LA_TRY(P->upiv.alloc(sizeof(int)));
+  LA_CUDA_TRY(cudaMemsetAsync(P->upiv.p, 0, sizeof(int), st));
+  LA_CUDA_TRY(cudaStreamSynchronize(st));
+  take(P->rs, dai);
+  take(P->exec_row, order);
+  take(P->uptr, uptr);
+  take(P->uk, uk);
+  take(P->us, us);
+  take(P->pptr, pptr);
+  take(P->ptgt, ptgt);
+  take(P->psrc, psrc);
+  P->levels = lv;
+  P->nchunks = nchunks;
+  LA_TRY(plan_finish(P));
+  *ok = true;
   return LA_OK;
 }
 
@@ -477,6 +718,14 @@ la_status factor_plan_create(int kind, int n, int base, const int *ai, const int
   P->base = base;
   P->nnz = ai[n] - base;
   P->h_ai.assign(ai, ai + n + 1);
+  if (kind == kIC0 && n >= kDevicePlanRows) {
+    bool ok = false;
+    LA_TRY(plan_build_ic0_device(P.get(), ai, aj, &ok));
+    if (ok) {
+      *out = P.release();
+      return LA_OK;
+    }
+  }
   Symbolic S;
   if (kind == kIC0) {
     symbolic_ic0(n, base, ai, aj, S);

@@ -175,6 +175,8 @@ __global__ void scan_add_kernel(int *d, const int m, const int *sums) {
     d[i + kScanThreads] += add;
 }
 
+} // namespace
+
 la_status scan_exclusive(int *d, int m, cudaStream_t st) {
   if (m <= 0)
     return LA_OK;
@@ -194,6 +196,8 @@ la_status scan_exclusive(int *d, int m, cudaStream_t st) {
   LA_CUDA_TRY(cudaStreamSynchronize(st)); // sums is released on return
   return LA_OK;
 }
+
+namespace {
 
 // ai[r] = base + (entries with row < r): lower bound of r in the sorted rows
 __global__ void row_pointer_kernel(const int n, const int nnz, const unsigned *row,

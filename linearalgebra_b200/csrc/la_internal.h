@@ -91,6 +91,14 @@ la_status run_starts(int n, const unsigned *sorted, int nq, int base, int *out, 
 // topological_sort2; the triangle must be strict.
 la_status topological_sort2_device(int uplo, int n, int base, const int *ai, const int *aj,
                                    int *iperm, int *prefix, int *levels);
+// The same on a triangle already on the device (d_ai/d_aj carry base):
+// order = rows sorted by (level, row), 0-based; keys = their levels; starts =
+// the levels' first positions, levels + 1 entries.  Buffers are allocated.
+la_status levels_on_device(int uplo, int n, int base, const int *d_ai, const int *d_aj,
+                           DevBuf &order, DevBuf &keys, DevBuf &starts, int *levels,
+                           cudaStream_t st);
+// In-place exclusive prefix sum of d[0, m) on the device (la_ingest.cu).
+la_status scan_exclusive(int *d, int m, cudaStream_t st);
 // The optional FP32 copy of an FP64 matrix's values (LA_CSR_KEEP_F32).
 la_status csr_finish(la_csr_t A, int flags);
 

@@ -134,16 +134,13 @@ __global__ void add_base_kernel(const int n, const int *pos, const int base, int
 
 } // namespace
 
-la_status topological_sort2_device(int uplo, int n, int base, const int *ai, const int *aj,
-                                   int *iperm, int *prefix, int *levels) {
+la_status levels_on_device(int uplo, int n, int base, const int *d_ai, const int *d_aj,
+                           DevBuf &order, DevBuf &keys, DevBuf &starts, int *levels,
+                           cudaStream_t st) {
   *levels = 0;
   if (n == 0)
     return LA_OK;
-  const int nnz = ai[n] - base;
-  cudaStream_t st = nullptr;
-  DevBuf dai, daj, depth, state, kh[2], kl[2], kp[2], out;
-  LA_TRY(dai.upload(ai, sizeof(int) * (n + 1)));
-  LA_TRY(daj.upload(aj, sizeof(int) * std::max(nnz, 1)));
+  DevBuf depth, state, kh[2], kl[2], kp[2];
   LA_TRY(depth.alloc(sizeof(int) * n));
   LA_TRY(state.alloc(sizeof(int) * 4));
   for (int s = 0; s < 2; s++) {
@@ -151,7 +148,6 @@ la_status topological_sort2_device(int uplo, int n, int base, const int *ai, con
     LA_TRY(kl[s].alloc(sizeof(unsigned) * n));
     LA_TRY(kp[s].alloc(sizeof(int) * n));
   }
-  LA_TRY(out.alloc(sizeof(int) * (n + 1)));
   LA_CUDA_TRY(cudaMemsetAsync(depth.p, 0xff, sizeof(int) * n, st));
   LA_CUDA_TRY(cudaMemsetAsync(state.p, 0, sizeof(int) * 4, st));
   LA_CUDA_TRY(cudaMemsetAsync(kl[0].p, 0, sizeof(unsigned) * n, st));
@@ -165,13 +161,11 @@ la_status topological_sort2_device(int uplo, int n, int base, const int *ai, con
   const int need = ((n + 31) / 32 + kThreads / 32 - 1) / (kThreads / 32);
   const int grid = std::max(1, std::min(per_sm * sm_count(), need));
   if (uplo == LA_LOWER)
-    depth_kernel<false><<<grid, kThreads, 0, st>>>(n, base, dai.as<int>(), daj.as<int>(),
-                                                   depth.as<int>(), kh[0].as<unsigned>(),
-                                                   state.as<int>());
+    depth_kernel<false><<<grid, kThreads, 0, st>>>(n, base, d_ai, d_aj, depth.as<int>(),
+                                                   kh[0].as<unsigned>(), state.as<int>());
   else
-    depth_kernel<true><<<grid, kThreads, 0, st>>>(n, base, dai.as<int>(), daj.as<int>(),
-                                                  depth.as<int>(), kh[0].as<unsigned>(),
-                                                  state.as<int>());
+    depth_kernel<true><<<grid, kThreads, 0, st>>>(n, base, d_ai, d_aj, depth.as<int>(),
+                                                  kh[0].as<unsigned>(), state.as<int>());
   LA_CUDA_TRY(cudaGetLastError());
   const int g = std::max(1, std::min((n + 255) / 256, 8 * sm_count()));
   max_kernel<<<g, 256, 0, st>>>(n, depth.as<int>(), state.as<int>() + 3);
@@ -191,11 +185,37 @@ la_status topological_sort2_device(int uplo, int n, int base, const int *ai, con
   const int lv = hs[3] + 1;
   int cur = 0;
   LA_TRY(radix_sort_pairs(n, (unsigned)lv, 1u, kh, kl, kp, &cur, st));
-  add_base_kernel<<<g, 256, 0, st>>>(n, kp[cur].as<int>(), base, out.as<int>());
+  LA_TRY(starts.alloc(sizeof(int) * (lv + 1)));
+  LA_TRY(run_starts(n, kh[cur].as<unsigned>(), lv, 0, starts.as<int>(), st));
+  std::swap(order.p, kp[cur].p);
+  std::swap(order.bytes, kp[cur].bytes);
+  std::swap(keys.p, kh[cur].p);
+  std::swap(keys.bytes, kh[cur].bytes);
+  LA_CUDA_TRY(cudaStreamSynchronize(st)); // the sort's scratch is released on return
+  *levels = lv;
+  return LA_OK;
+}
+
+la_status topological_sort2_device(int uplo, int n, int base, const int *ai, const int *aj,
+                                   int *iperm, int *prefix, int *levels) {
+  *levels = 0;
+  if (n == 0)
+    return LA_OK;
+  const int nnz = ai[n] - base;
+  cudaStream_t st = nullptr;
+  DevBuf dai, daj, order, keys, starts, out;
+  LA_TRY(dai.upload(ai, sizeof(int) * (n + 1)));
+  LA_TRY(daj.upload(aj, sizeof(int) * std::max(nnz, 1)));
+  int lv = 0;
+  LA_TRY(levels_on_device(uplo, n, base, dai.as<int>(), daj.as<int>(), order, keys, starts, &lv,
+                          st));
+  LA_TRY(out.alloc(sizeof(int) * n));
+  const int g = std::max(1, std::min((n + 255) / 256, 8 * sm_count()));
+  add_base_kernel<<<g, 256, 0, st>>>(n, order.as<int>(), base, out.as<int>());
   LA_CUDA_TRY(cudaGetLastError());
   LA_CUDA_TRY(cudaMemcpyAsync(iperm, out.p, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
-  LA_TRY(run_starts(n, kh[cur].as<unsigned>(), lv, 0, out.as<int>(), st));
-  LA_CUDA_TRY(cudaMemcpyAsync(prefix, out.p, sizeof(int) * (lv + 1), cudaMemcpyDeviceToHost, st));
+  LA_CUDA_TRY(cudaMemcpyAsync(prefix, starts.p, sizeof(int) * (lv + 1), cudaMemcpyDeviceToHost,
+                              st));
   LA_CUDA_TRY(cudaStreamSynchronize(st));
   *levels = lv;
   return LA_OK;

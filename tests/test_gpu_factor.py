@@ -134,6 +134,44 @@ def test_ic0_device_irregular_patterns(lab):
             assert np.array_equal(got, want), (seed, rcm, np.abs(got - want).max())
 
 
+def _arrow(m):
+    """Tridiagonal plus a full last row and column, dominant diagonal: the
+    last row receives m - 1 updates."""
+    rows = [set([i - 1, i, i + 1]) & set(range(m)) for i in range(m)]
+    for i in range(m - 1):
+        rows[i].add(m - 1)
+        rows[m - 1].add(i)
+    ai = np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(np.int32)
+    aj = np.concatenate([sorted(r) for r in rows]).astype(np.int32)
+    r = np.repeat(np.arange(m), np.diff(ai))
+    av = np.where(aj == r, 0.0, -0.5)
+    av[aj == r] = np.bincount(r, np.abs(av), minlength=m) + 1.0
+    return m, ai, aj, av
+
+
+@pytest.mark.gpu
+def test_ic0_device_plan_large_patterns(lab):
+    """From 65,536 rows the IC(0) plan itself is built on the device (update
+    order, pairs, levels, chunks); the factor equals the host's bit for bit on
+    stencils in natural and RCM order, an irregular pattern, base 1, and a
+    pattern one of whose rows receives more updates than the device sorts
+    (its plan is built on the host)."""
+    from linearalgebra_b200 import gen
+    cases = [("lap3d_48", gen.laplacian_3d(48), False), ("lap3d_48_rcm", gen.laplacian_3d(48), True),
+             ("st27_42_rcm", gen.stencil27(42, seed=5), True),
+             ("irregular_70k", _random_spd(70_000, 9), True), ("arrow_70k", _arrow(70_000), False)]
+    for name, mat, rcm in cases:
+        n, ua, uj, uv = _ic_inputs(lab, mat, rcm)
+        assert n >= 65_536
+        want = lab.ICCLevelNumeric0(n, 0, ua, uj, uv)
+        plan = lab.FactorPlan("ic0", n, 0, ua, uj)
+        got = plan.factor(uv)
+        assert np.array_equal(got, want), (name, np.abs(got - want).max())
+        if name == "lap3d_48_rcm":
+            got1 = lab.FactorPlan("ic0", n, 1, ua + 1, uj + 1).factor(uv)
+            assert np.array_equal(got1, want), name
+
+
 @pytest.mark.gpu
 def test_ic0_device_base1_and_breakdown(lab):
     from linearalgebra_b200 import gen
