@@ -545,7 +545,7 @@ def run_case(case):
         n, ai, aj, av = gen.laplacian_3d(128)
         iperm, perm = la.SerialCM(n, 0, ai, aj)
         b_ai, b_aj, b_av = la.Permute(n, 0, ai, aj, av, iperm, perm)
-        ua, uj, uv = gen.upper_with_diag(n, b_ai, b_aj, b_av)
+        ua, uj, uv = la.SplitTriangle("U", n, 0, b_ai, b_aj, b_av)
         if case == "factor-c3":
             fp = la.FactorPlan("ic0", n, 0, ua, uj)
             for _ in range(3):
@@ -556,6 +556,19 @@ def run_case(case):
             t_ai, t_aj, _ = la.Transpose(n, n, 0, s_ai, s_aj, s_av)
             for _ in range(3):
                 la.TopologicalSort2("L", n, 0, t_ai, t_aj, device=True)
+    elif case == "rcm-c3":
+        # reverse Cuthill-McKee of the 128^3 Laplacian ordered on the GPU
+        n, ai, aj, av = gen.laplacian_3d(128)
+        for _ in range(2):
+            la.SerialCM(n, 0, ai, aj, device=True)
+    elif case == "icplan-c3":
+        # the IC(0) plan of the RCM-ordered 128^3 Laplacian built on the GPU
+        n, ai, aj, av = gen.laplacian_3d(128)
+        iperm, perm = la.SerialCM(n, 0, ai, aj, device=True)
+        b_ai, b_aj, b_av = la.Permute(n, 0, ai, aj, av, iperm, perm)
+        ua, uj, uv = la.SplitTriangle("U", n, 0, b_ai, b_aj, b_av)
+        for _ in range(2):
+            la.FactorPlan("ic0", n, 0, ua, uj)
     elif case == "ingest":
         # 16M shuffled COO entries (4M x 4M) sorted into a device CSR
         rng = np.random.default_rng(0)
@@ -627,7 +640,7 @@ def main():
     ap.add_argument("--case", default=None,
                     choices=["spmv-powerlaw", "spmv-lap3d", "trsv-lap3d", "trsv-c5-f32",
                              "pcg-lap3d", "adjoint-c4", "factor-c3", "levels-c3", "ingest",
-                             "noalloc-c3"],
+                             "noalloc-c3", "rcm-c3", "icplan-c3"],
                     help="run one kernel workload a few times and exit (for ncu)")
     args = ap.parse_args()
     args.steps_given = args.steps is not None

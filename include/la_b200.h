@@ -315,8 +315,9 @@ la_status la_icc0_shifted(int n, int base, const int *u_ai, const int *u_aj,
                           double *shift_used);
 
 /* The same factorisations on the GPU: a symbolic plan built once per
- * pattern on the host (every row's updates in the order the sequential
- * algorithm applies them, found in parallel over rows), then numeric passes on the
+ * pattern (every row's updates in the order the sequential algorithm
+ * applies them, found per row in parallel -- for IC(0) patterns of at least
+ * 65,536 rows on the GPU, else on the host), then numeric passes on the
  * device, one persistent launch each, level-scheduled by the rows'
  * dependencies -- bit-identical to la_icc0 / la_ilu0 (same operations, same
  * order).  For a pattern factored more than once (new values, shift

@@ -137,13 +137,13 @@ def test_ic0_device_irregular_patterns(lab):
 def _arrow(m):
     """Tridiagonal plus a full last row and column, dominant diagonal: the
     last row receives m - 1 updates."""
-    rows = [set([i - 1, i, i + 1]) & set(range(m)) for i in range(m)]
-    for i in range(m - 1):
-        rows[i].add(m - 1)
-        rows[m - 1].add(i)
-    ai = np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(np.int32)
-    aj = np.concatenate([sorted(r) for r in rows]).astype(np.int32)
-    r = np.repeat(np.arange(m), np.diff(ai))
+    i = np.arange(m - 1)
+    r = np.concatenate([i, i[1:], i[:-1], i, np.full(m - 1, m - 1), [m - 1]])
+    c = np.concatenate([i, i[1:] - 1, i[:-1] + 1, np.full(m - 1, m - 1), i, [m - 1]])
+    key = np.unique(r.astype(np.int64) * m + c)  # row-major, duplicates merged
+    r, aj = (key // m).astype(np.int64), (key % m).astype(np.int32)
+    ai = np.zeros(m + 1, np.int32)
+    np.cumsum(np.bincount(r, minlength=m), out=ai[1:])
     av = np.where(aj == r, 0.0, -0.5)
     av[aj == r] = np.bincount(r, np.abs(av), minlength=m) + 1.0
     return m, ai, aj, av
