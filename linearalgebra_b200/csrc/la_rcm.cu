@@ -44,29 +44,71 @@ namespace {
 
 constexpr int kThreads = 256;
 
+constexpr int kNbrGroup = 8; // neighbours whose loads are issued together
+
 // The whole search in one cooperative launch.  Level l is queue[lstart[l],
 // lstart[l+1]); at step lev the grid expands level lev-1, appending the
 // vertices it claims after the frontier, then meets at a grid barrier and
-// reads the new level's size.  cnt3 holds three rotating counters: the one
-// step lev+1 uses is cleared during step lev, when every thread has passed
-// the barrier after its last read (at step lev-2).  bar[0..2]: the barrier;
-// bar[3]: the number of levels, written at the end.
+// reads the new level's size.  A warp walks 32 frontier vertices together,
+// kNbrGroup neighbours per vertex at a time (their column and level loads
+// issued together), and appends what its lanes claimed with one atomic.
+// cnt3 holds three rotating counters: the one step lev+1 uses is cleared
+// during step lev, when every thread has passed the barrier after its last
+// read (at step lev-2).  bar[0..2]: the barrier; bar[3]: the number of
+// levels, written at the end.
 __global__ void __launch_bounds__(kThreads)
     bfs_kernel(int *queue, int *level, const int *__restrict__ ai, const int *__restrict__ aj,
                const int base, int *lstart, int *cnt3, unsigned *bar) {
   const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+  const int lane = threadIdx.x & 31;
   int qs = 0, qe = 1;
   for (int lev = 1;; lev++) {
     int *cnt = cnt3 + lev % 3;
     if (gt == 0)
       cnt3[(lev + 1) % 3] = 0;
-    for (int h = qs + gt; h < qe; h += gs) {
-      const int u = __ldcg(queue + h);
-      const int a = __ldg(ai + u) - base, e = __ldg(ai + u + 1) - base;
-      for (int k = a; k < e; k++) {
-        const int v = __ldg(aj + k) - base;
-        if (__ldcg(level + v) < 0 && atomicCAS(level + v, -1, lev) == -1)
-          queue[qe + atomicAdd(cnt, 1)] = v;
+    // warp-uniform walk: lane h = h0 + lane
+    for (int h0 = qs + gt - lane; h0 < qe; h0 += gs) {
+      const int h = h0 + lane;
+      int a = 0, e = 0;
+      if (h < qe) {
+        const int u = __ldcg(queue + h);
+        a = __ldg(ai + u) - base;
+        e = __ldg(ai + u + 1) - base;
+      }
+      const int groups = __reduce_max_sync(0xffffffffu, (e - a + kNbrGroup - 1) / kNbrGroup);
+      for (int g = 0; g < groups; g++) {
+        int v[kNbrGroup], lv[kNbrGroup];
+#pragma unroll
+        for (int q = 0; q < kNbrGroup; q++) {
+          const int k = a + g * kNbrGroup + q;
+          v[q] = k < e ? __ldg(aj + k) - base : -1;
+        }
+#pragma unroll
+        for (int q = 0; q < kNbrGroup; q++)
+          lv[q] = v[q] >= 0 ? __ldcg(level + v[q]) : 0;
+        int mine = 0; // claimed this round
+#pragma unroll
+        for (int q = 0; q < kNbrGroup; q++) {
+          const bool got = v[q] >= 0 && lv[q] < 0 && atomicCAS(level + v[q], -1, lev) == -1;
+          if (!got)
+            v[q] = -1;
+          mine += got;
+        }
+        int incl = mine; // warp prefix of the claims, one atomic per warp
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int t = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o)
+            incl += t;
+        }
+        int at = 0;
+        if (lane == 31 && incl > 0)
+          at = atomicAdd(cnt, incl);
+        at = __shfl_sync(0xffffffffu, at, 31) + incl - mine;
+#pragma unroll
+        for (int q = 0; q < kNbrGroup; q++)
+          if (v[q] >= 0)
+            queue[qe + at++] = v[q];
       }
     }
     dev::grid_barrier(bar);
@@ -178,14 +220,27 @@ __global__ void __launch_bounds__(kThreads)
   for (int l = 0; l + 1 < height; l++) {
     const int p0 = __ldg(lstart + l), q0 = __ldg(lstart + l + 1);
     const int m = q0 - p0, mq = __ldg(lstart + l + 2) - q0;
-    // (1)
+    // (1) neighbours kNbrGroup at a time: columns, then levels, then the
+    // positions of those on level l, each set of loads issued together
     for (int h = gt; h < mq; h += gs) {
       const int v = __ldg(queue + q0 + h);
+      const int a = __ldg(ai + v) - base, e = __ldg(ai + v + 1) - base;
       int p = INT_MAX;
-      for (int k = __ldg(ai + v) - base; k < __ldg(ai + v + 1) - base; k++) {
-        const int u = __ldg(aj + k) - base;
-        if (__ldg(level + u) == l)
-          p = min(p, __ldcg(pos + u));
+      for (int k0 = a; k0 < e; k0 += kNbrGroup) {
+        int u[kNbrGroup], pu[kNbrGroup];
+#pragma unroll
+        for (int q = 0; q < kNbrGroup; q++)
+          u[q] = k0 + q < e ? __ldg(aj + k0 + q) - base : -1;
+#pragma unroll
+        for (int q = 0; q < kNbrGroup; q++)
+          if (u[q] >= 0 && __ldg(level + u[q]) != l)
+            u[q] = -1;
+#pragma unroll
+        for (int q = 0; q < kNbrGroup; q++)
+          pu[q] = u[q] >= 0 ? __ldcg(pos + u[q]) : INT_MAX;
+#pragma unroll
+        for (int q = 0; q < kNbrGroup; q++)
+          p = min(p, pu[q]);
       }
       parent[v] = p;
     }
@@ -199,9 +254,19 @@ __global__ void __launch_bounds__(kThreads)
       int c = 0;
       if (h < m) {
         const int p = p0 + h, u = __ldcg(cm + p);
-        for (int k = __ldg(ai + u) - base; k < __ldg(ai + u + 1) - base; k++) {
-          const int v = __ldg(aj + k) - base;
-          c += __ldg(level + v) == l + 1 && __ldcg(parent + v) == p;
+        const int a = __ldg(ai + u) - base, e = __ldg(ai + u + 1) - base;
+        for (int k0 = a; k0 < e; k0 += kNbrGroup) {
+          int v[kNbrGroup];
+#pragma unroll
+          for (int q = 0; q < kNbrGroup; q++)
+            v[q] = k0 + q < e ? __ldg(aj + k0 + q) - base : -1;
+#pragma unroll
+          for (int q = 0; q < kNbrGroup; q++)
+            if (v[q] >= 0 && __ldg(level + v[q]) != l + 1)
+              v[q] = -1;
+#pragma unroll
+          for (int q = 0; q < kNbrGroup; q++)
+            c += v[q] >= 0 && __ldcg(parent + v[q]) == p;
         }
       }
       const int ex = block_exclusive_scan(c, &tile_total);
@@ -222,21 +287,37 @@ __global__ void __launch_bounds__(kThreads)
       const int h = t * kThreads + threadIdx.x;
       if (h < m) {
         const int p = p0 + h, u = __ldcg(cm + p);
-        int ch[MAXC];
+        const int a = __ldg(ai + u) - base, e = __ldg(ai + u + 1) - base;
+        int ch[MAXC], cd[MAXC]; // children and their degrees, by (degree, node)
         int c = 0;
-        for (int k = __ldg(ai + u) - base; k < __ldg(ai + u + 1) - base && c < MAXC; k++) {
-          const int v = __ldg(aj + k) - base;
-          if (__ldg(level + v) == l + 1 && __ldcg(parent + v) == p) {
-            const int dv = __ldg(deg + v);
+        for (int k0 = a; k0 < e; k0 += kNbrGroup) {
+          int v[kNbrGroup], dv[kNbrGroup];
+#pragma unroll
+          for (int q = 0; q < kNbrGroup; q++)
+            v[q] = k0 + q < e ? __ldg(aj + k0 + q) - base : -1;
+#pragma unroll
+          for (int q = 0; q < kNbrGroup; q++)
+            if (v[q] >= 0 && __ldg(level + v[q]) != l + 1)
+              v[q] = -1;
+#pragma unroll
+          for (int q = 0; q < kNbrGroup; q++)
+            if (v[q] >= 0 && __ldcg(parent + v[q]) != p)
+              v[q] = -1;
+#pragma unroll
+          for (int q = 0; q < kNbrGroup; q++)
+            dv[q] = v[q] >= 0 ? __ldg(deg + v[q]) : 0;
+#pragma unroll
+          for (int q = 0; q < kNbrGroup; q++) {
+            if (v[q] < 0 || c >= MAXC)
+              continue;
             int i = c++; // insertion by (degree, node)
-            while (i > 0) {
-              const int w = ch[i - 1], dw = __ldg(deg + w);
-              if (dw < dv || (dw == dv && w < v))
-                break;
-              ch[i] = w;
+            while (i > 0 && (cd[i - 1] > dv[q] || (cd[i - 1] == dv[q] && ch[i - 1] > v[q]))) {
+              ch[i] = ch[i - 1];
+              cd[i] = cd[i - 1];
               i--;
             }
-            ch[i] = v;
+            ch[i] = v[q];
+            cd[i] = dv[q];
           }
         }
         const int o = q0 + tile_base + __ldcg(cnt + h);
