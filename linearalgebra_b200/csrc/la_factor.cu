@@ -53,6 +53,9 @@ constexpr int kFactorThreads = 256;
 constexpr int kFactorChunk = 32;
 constexpr unsigned long long kFactorWaitNs = 1000000000ull; // 1 s
 constexpr int kGroup = 8; // flags polled / pair sources loaded together
+// pause between polls of unpublished rows (none: 64 / 256 ns measured no
+// faster on the 128^3 and 192^3 factors, 2% faster on the 27-point one)
+constexpr int kPollSleepNs = 0;
 
 enum FactorKind { kIC0 = 0, kILU0 = 1 };
 
@@ -238,6 +241,162 @@ __device__ __forceinline__ void st_release(int *p, int v) {
 
 // state[0]: chunk ticket, state[1]: a wait gave up, state[2]: smallest row
 // whose pivot broke down (INT_MAX if none).
+constexpr int kRowMax = 16;     // rows this long are worked on in shared memory
+constexpr int kBatch = 4;       // updates whose index data and sources load together
+constexpr int kBatchPairs = 12; // at most this many pairs in such a batch
+// shared memory of the factor kernel: kRowMax values per thread, value-major
+constexpr size_t kFactorSmem = sizeof(double) * kRowMax * kFactorThreads;
+
+// The row being worked on: value q of this thread's row in shared memory,
+// value-major so that a warp's accesses fall in distinct banks.
+struct RowVals {
+  double *base;
+  __device__ double &operator[](int q) const { return base[q * kFactorThreads]; }
+};
+
+// Row j of at most kRowMax entries: its values live in shared memory (w)
+// from the copy of vin to the final store.  The index data of
+// a batch of updates (pair ranges, scalar and pivot indices, the pairs'
+// target and source indices) does not depend on other rows, so the first
+// batch's is loaded before the dependency wait; after it, the batch's source
+// values are loaded together and the updates applied one after the other in
+// their order -- the same exact operations in the same order as the general
+// path, so the factor is unchanged.  A batch is cut short so that its pairs
+// fit kBatchPairs; a single update with more pairs takes its pairs kGroup at
+// a time.
+template <int KIND>
+__device__ void factor_short_row(const int j, const int rs, const int re,
+                                 const int *__restrict__ uptr, const int *__restrict__ uk,
+                                 const int *__restrict__ us, const int *__restrict__ upiv,
+                                 const int *__restrict__ pptr, const int *__restrict__ ptgt,
+                                 const int *__restrict__ psrc, const double *__restrict__ vin,
+                                 double *v, const double diag_scale,
+                                 const int *__restrict__ diag_of, int *done, int *state,
+                                 const int sleep_ns) {
+  const int len = re - rs;
+  extern __shared__ double factor_smem[];
+  const RowVals w{factor_smem + threadIdx.x};
+  for (int q = 0; q < len; q++)
+    w[q] = __ldg(vin + rs + q);
+  if (KIND == kIC0)
+    w[0] = __dmul_rn(w[0], diag_scale); // the (1 + omega) shift
+  const int u0 = __ldg(uptr + j), u1 = __ldg(uptr + j + 1);
+  int u = u0, nb = 0, np = 0;
+  int e[kBatch + 1], sidx[kBatch], oidx[kBatch], tg[kBatchPairs], sr[kBatchPairs];
+  auto load_batch = [&]() {
+    nb = min(kBatch, u1 - u);
+    for (int q = 0; q <= nb; q++)
+      e[q] = __ldg(pptr + u + q);
+    for (int q = 0; q < nb; q++) {
+      sidx[q] = __ldg(KIND == kIC0 ? us + u + q : upiv + u + q);
+      oidx[q] = KIND == kIC0 ? 0 : __ldg(us + u + q) - rs;
+    }
+    while (nb > 1 && e[nb] - e[0] > kBatchPairs)
+      nb--;
+    np = e[nb] - e[0];
+    if (np <= kBatchPairs)
+      for (int t = 0; t < np; t++) {
+        tg[t] = __ldg(ptgt + e[0] + t) - rs;
+        sr[t] = __ldg(psrc + e[0] + t);
+      }
+  };
+  if (u < u1)
+    load_batch();
+  bool gave_up = false;
+  const unsigned long long t0 = factor_ns();
+  // every source row published: their flags polled kGroup at a time
+  for (int g = u0; g < u1 && !gave_up; g += kGroup) {
+    int kk[kGroup];
+    unsigned pending = 0;
+#pragma unroll
+    for (int q = 0; q < kGroup; q++)
+      if (g + q < u1) {
+        kk[q] = __ldg(uk + g + q);
+        pending |= 1u << q;
+      }
+    for (unsigned pass = 1; pending; pass++) {
+      int f[kGroup];
+#pragma unroll
+      for (int q = 0; q < kGroup; q++)
+        f[q] = (pending >> q) & 1u ? ld_acquire(done + kk[q]) : 1;
+#pragma unroll
+      for (int q = 0; q < kGroup; q++)
+        if (f[q] != 0)
+          pending &= ~(1u << q);
+      if (pending && (pass & 63u) == 0u &&
+          (ld_acquire(state + 1) != 0 || factor_ns() - t0 > kFactorWaitNs)) {
+        atomicExch(state + 1, 1);
+        gave_up = true;
+        break;
+      }
+      if (pending && sleep_ns > 0) // back off: fewer polls crowding L2
+        __nanosleep(sleep_ns);
+    }
+  }
+  if (gave_up) // the row stays unpublished; the warp stops at its next claim
+    return;
+  while (u < u1) {
+    double sv[kBatch];
+    for (int q = 0; q < nb; q++)
+      sv[q] = __ldcg(v + sidx[q]);
+    if (np <= kBatchPairs) {
+      double src[kBatchPairs];
+      for (int t = 0; t < np; t++)
+        src[t] = __ldcg(v + sr[t]);
+      for (int q = 0; q < nb; q++) {
+        double s;
+        if (KIND == kIC0) {
+          s = sv[q]; // U_kj, final
+        } else {
+          s = __ddiv_rn(w[oidx[q]], sv[q]); // L_jk = a_jk / u_kk
+          w[oidx[q]] = s;
+        }
+        for (int t = e[q] - e[0]; t < e[q + 1] - e[0]; t++)
+          w[tg[t]] = __dsub_rn(w[tg[t]], __dmul_rn(s, src[t]));
+      }
+    } else { // one update (nb == 1) with more pairs than a batch holds
+      double s;
+      if (KIND == kIC0) {
+        s = sv[0];
+      } else {
+        s = __ddiv_rn(w[oidx[0]], sv[0]);
+        w[oidx[0]] = s;
+      }
+      for (int eg = e[0]; eg < e[1]; eg += kGroup) {
+        int tq[kGroup];
+        double src[kGroup];
+#pragma unroll
+        for (int q = 0; q < kGroup; q++)
+          if (eg + q < e[1]) {
+            tq[q] = __ldg(ptgt + eg + q) - rs;
+            src[q] = __ldcg(v + __ldg(psrc + eg + q));
+          }
+#pragma unroll
+        for (int q = 0; q < kGroup; q++)
+          if (eg + q < e[1])
+            w[tq[q]] = __dsub_rn(w[tq[q]], __dmul_rn(s, src[q]));
+      }
+    }
+    u += nb;
+    if (u < u1)
+      load_batch();
+  }
+  if (KIND == kIC0) {
+    if (w[0] < 0.0)
+      atomicMin(state + 2, j);
+    const double piv = __dsqrt_rn(w[0]);
+    w[0] = piv;
+    for (int q = 1; q < len; q++)
+      w[q] = __ddiv_rn(w[q], piv);
+  } else if (w[__ldg(diag_of + j) - rs] == 0.0) {
+    atomicMin(state + 2, j);
+  }
+  for (int q = 0; q < len; q++)
+    v[rs + q] = w[q];
+  __threadfence();
+  st_release(done + j, 1);
+}
+
 template <int KIND>
 __global__ void __launch_bounds__(kFactorThreads)
     factor_kernel(const int nchunks, const int *__restrict__ chunk_start,
@@ -247,7 +406,7 @@ __global__ void __launch_bounds__(kFactorThreads)
                   const int *__restrict__ upiv, const int *__restrict__ pptr,
                   const int *__restrict__ ptgt, const int *__restrict__ psrc,
                   const double *__restrict__ vin, double *v, const double diag_scale, int *done,
-                  int *state) {
+                  int *state, const int sleep_ns) {
   const int lane = threadIdx.x & 31;
   for (;;) {
     // lane 0 alone decides (a wait gave up somewhere: stop) and broadcasts,
@@ -263,6 +422,11 @@ __global__ void __launch_bounds__(kFactorThreads)
       continue;
     const int j = __ldg(exec_row + p);
     const int rs = __ldg(rs_of + j), re = __ldg(rs_of + j + 1);
+    if (re - rs <= kRowMax) {
+      factor_short_row<KIND>(j, rs, re, uptr, uk, us, upiv, pptr, ptgt, psrc, vin, v, diag_scale,
+                             diag_of, done, state, sleep_ns);
+      continue;
+    }
     for (int q = rs; q < re; q++)
       v[q] = __ldg(vin + q);
     if (KIND == kIC0)
@@ -295,6 +459,8 @@ __global__ void __launch_bounds__(kFactorThreads)
           gave_up = true;
           break;
         }
+        if (pending && sleep_ns > 0)
+          __nanosleep(sleep_ns);
       }
     }
     // the updates in their order; an update's scalar operand and its pairs'
@@ -417,10 +583,13 @@ la_status plan_finish(la_factor_plan_s *P) {
   LA_TRY(P->state.alloc(sizeof(int) * 4));
   int per_sm = 0;
   LA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &per_sm, (const void *)factor_kernel<kIC0>, kFactorThreads, 0));
+      &per_sm, (const void *)factor_kernel<kIC0>, kFactorThreads, kFactorSmem));
   // LA_FACTOR_CTAS_PER_SM caps the CTAs per SM (tuning override; default:
   // as many as fit).  Warps beyond what the widest levels use only poll.
   per_sm = std::max(per_sm, 1);
+  P->sleep_ns = kPollSleepNs;
+  if (const char *e = std::getenv("LA_FACTOR_SLEEP_NS")) // tuning override
+    P->sleep_ns = std::max(0, std::atoi(e));
   if (const char *e = std::getenv("LA_FACTOR_CTAS_PER_SM"))
     per_sm = std::min(per_sm, std::max(1, std::atoi(e)));
   const int need = (P->nchunks + kFactorThreads / 32 - 1) / (kFactorThreads / 32);
@@ -685,11 +854,11 @@ la_status factor_numeric(la_factor_plan_s *P, const double *av, double omega, do
   LA_CUDA_TRY(cudaMemcpyAsync(P->state.p, init, sizeof(init), cudaMemcpyHostToDevice, st));
   LA_CUDA_TRY(cudaMemsetAsync(P->done.p, 0, sizeof(int) * P->n, st));
   auto launch = P->kind == kIC0 ? factor_kernel<kIC0> : factor_kernel<kILU0>;
-  launch<<<P->grid, kFactorThreads, 0, st>>>(
+  launch<<<P->grid, kFactorThreads, kFactorSmem, st>>>(
       P->nchunks, P->chunk_start.as<int>(), P->exec_row.as<int>(), P->rs.as<int>(),
       P->diag.as<int>(), P->uptr.as<int>(), P->uk.as<int>(), P->us.as<int>(), P->upiv.as<int>(),
       P->pptr.as<int>(), P->ptgt.as<int>(), P->psrc.as<int>(), P->vin.as<double>(), v,
-      1.0 + omega, P->done.as<int>(), P->state.as<int>());
+      1.0 + omega, P->done.as<int>(), P->state.as<int>(), P->sleep_ns);
   LA_CUDA_TRY(cudaGetLastError());
   int state[4];
   LA_CUDA_TRY(cudaMemcpyAsync(state, P->state.p, sizeof(state), cudaMemcpyDeviceToHost, st));

@@ -241,6 +241,10 @@ struct la_pcg_s {
   // the iteration's vector work in two cooperative kernels (dot products
   // finished inside them) instead of separate dot / update launches
   bool fused = true;
+  // mixed mode: the reliable update falls due when the FP32 residual has
+  // dropped by this factor; the next step is queued ahead of the residual's
+  // arrival while the last residual is above ahead_margin times that
+  double reliable_delta = 0.1, ahead_margin = 1.3;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double *h_rr = nullptr;       // pinned host copy of the residual norm
   cudaEvent_t ev_rr = nullptr;  // marks its arrival
@@ -250,6 +254,7 @@ struct la_pcg_s {
 struct la_factor_plan_s {
   int kind = 0; // 0: IC(0), 1: ILU(0)
   int n = 0, nnz = 0, base = 0, levels = 0, nchunks = 0, grid = 0;
+  int sleep_ns = 0; // the numeric pass's pause between polls of unpublished rows
   // per row (original numbering): its value range [rs, re) and its diagonal
   la::DevBuf rs, diag;
   // rows in execution order, 32-row chunks that never cross a level

@@ -420,12 +420,13 @@ la_status pcg_run(la_pcg_t S, const X *rhs, X *y, X *r, X *z, X *p, X *q,
 // FP32 matrix and FP32 IC(0) factors (FP32 SpMV and triangular solves, FP32
 // accumulation in those kernels), its dot products and scalars in FP64.  The
 // FP32 iterate is a correction d accumulated since the last update; whenever
-// the FP32 residual has fallen by kReliableDelta since then (or below rtol),
+// the FP32 residual has fallen by a factor delta since then (or below rtol),
 // x += d in FP64, the residual is recomputed as r = b - A x with the FP64
 // matrix, and the FP32 residual is replaced by it -- without restarting the
 // search direction, so the iteration count stays close to the FP64 solver's.
 // The solve stops when that FP64 residual satisfies ||r|| / ||b|| < rtol.
-constexpr double kReliableDelta = 0.1;
+// delta (S->reliable_delta) is 0.1 unless LA_PCG_RELIABLE_DELTA, a
+// tuning override read when the solver is created, says otherwise.
 
 la_status pcg_mixed(la_pcg_t S, const double *b, double *x, double bn, double rtol,
                     int maxit, la_pcg_info *loc, cudaStream_t st) {
@@ -464,7 +465,8 @@ la_status pcg_mixed(la_pcg_t S, const double *b, double *x, double bn, double rt
     LA_CUDA_TRY(cudaMemcpyAsync(S->h_rr, S->scal.as<double>() + S_DOT, sizeof(double),
                                 cudaMemcpyDeviceToHost, st));
     LA_CUDA_TRY(cudaEventRecord(S->ev_rr, st));
-    const bool ahead = rn_prev > 0.13 * rmax && rn_prev > 2.0 * rtol * bn;
+    const bool ahead = rn_prev > S->ahead_margin * S->reliable_delta * rmax &&
+                       rn_prev > 2.0 * rtol * bn;
     auto precondition = [&]() -> la_status {
       LA_TRY(trsv_launch(S->L, r32, t32, st));
       LA_TRY(trsv_launch(S->U, t32, z32, st));
@@ -486,7 +488,7 @@ la_status pcg_mixed(la_pcg_t S, const double *b, double *x, double bn, double rt
       set_error("mixed PCG breakdown: non-finite residual at iteration %d", it);
       return LA_ERR_BREAKDOWN;
     }
-    if (rn < kReliableDelta * rmax || rn / bn < rtol) {
+    if (rn < S->reliable_delta * rmax || rn / bn < rtol) {
       refine_kernel<<<g, 256, 0, st>>>(n, x, d32, 1.0);
       LA_CUDA_TRY(cudaMemsetAsync(d32, 0, sizeof(float) * n, st));
       LA_TRY(spmv_launch(S->Ap, -1.0, x, 1.0, r64, b, LA_F64, st));
@@ -607,6 +609,16 @@ la_status pcg_create(la_csr_t A, const int *u_ai, const int *u_aj,
   // The fused kernels need every block resident at once (cooperative
   // launch); LA_PCG_FUSED=0 keeps the separate dot / update launches (same
   // iterates, bit for bit).
+  if (const char *e = std::getenv("LA_PCG_RELIABLE_DELTA")) { // tuning override
+    const double d = std::atof(e);
+    if (d > 0.0 && d < 1.0)
+      S->reliable_delta = d;
+  }
+  if (const char *e = std::getenv("LA_PCG_AHEAD_MARGIN")) { // tuning override
+    const double m = std::atof(e);
+    if (m >= 1.0)
+      S->ahead_margin = m;
+  }
   S->fused = true;
   if (const char *e = std::getenv("LA_PCG_FUSED"))
     S->fused = std::atoi(e) != 0;

@@ -25,9 +25,12 @@ def _ic_inputs(lab, mat, rcm):
     return n, np.asarray(ua, np.int32), np.asarray(uj, np.int32), np.asarray(uv)
 
 
-def _nonsym(m, seed):
+def _nonsym(m, seed, long_every=0):
+    """Random nonsymmetric pattern, 6 off-diagonal entries a row (every
+    long_every-th row 30: longer than the numeric pass's short-row form)."""
     rng = np.random.default_rng(seed)
-    rows = [np.union1d(rng.choice(m, 6, replace=False), [i]) for i in range(m)]
+    rows = [np.union1d(rng.choice(m, 30 if long_every and i % long_every == 0 else 6,
+                                  replace=False), [i]) for i in range(m)]
     ai = np.concatenate([[0], np.cumsum([len(c) for c in rows])]).astype(np.int32)
     aj = np.concatenate(rows).astype(np.int32)
     av = rng.uniform(-1, 1, len(aj))
@@ -199,7 +202,8 @@ def test_ic0_device_base1_and_breakdown(lab):
 @pytest.mark.gpu
 def test_ilu0_device_bit_identical(lab):
     from linearalgebra_b200 import gen
-    for n, ai, aj, av in (gen.laplacian_3d(20), gen.aniso7(16, seed=3), _nonsym(3000, 5)):
+    for n, ai, aj, av in (gen.laplacian_3d(20), gen.aniso7(16, seed=3), _nonsym(3000, 5),
+                          _nonsym(3000, 6, long_every=7)):
         want = lab.ILU0(n, 0, ai, aj, av)
         plan = lab.FactorPlan("ilu0", n, 0, ai, aj)
         assert np.array_equal(plan.factor(av), want), n
