@@ -33,10 +33,12 @@ constexpr int kThreads = 256;
 constexpr unsigned long long kWaitNs = 1000000000ull;
 constexpr int kGroup = 8; // dependencies polled together
 // pause between polls of unpublished depths: fewer polls leave L2 to the
-// rows being published (measured, 128^3 IC(0) factor's L: median 39 ms
-// without a pause, 12.8 / 12.0 / 10.8 ms with 32 / 128 / 512 ns; 192^3: no
-// change; 96^3 27-point: 19.7 -> 15.7 ms)
-constexpr int kPollSleepNs = 512;
+// rows being published (measured, 128^3 IC(0) factor's L, host arrays in and
+// out: median 39 ms and up to 81 ms without a pause, 12.8 / 12.0 / 10.4 /
+// 10.0 / 10.5 ms with 32 / 128 / 512 / 1024 / 2048 ns, the slowest of eight
+// calls 10.4 ms at 1024; 192^3: 20-21 ms throughout; 96^3 27-point: 19.7 ->
+// 14.6 ms)
+constexpr int kPollSleepNs = 1024;
 
 __device__ __forceinline__ unsigned long long level_ns() {
   unsigned long long t;
