@@ -397,6 +397,171 @@ __device__ void factor_short_row(const int j, const int rs, const int re,
   st_release(done + j, 1);
 }
 
+// ---- One warp per row, for patterns whose rows receive many pairs (the
+// 27-point stencils' ~90 a row): a lane per row would apply them one after
+// another, each batch of indices and sources a dependent round trip.  Here
+// the row's 32 lanes load its update indices, wait on its source rows, load
+// up to kWarpPairs * 32 pairs' targets and source values together, then
+// apply the updates one after another in their order, a lane per pair --
+// an update's pairs have distinct targets, so each entry still sees exactly
+// the host's operations in the host's order.  The row's values live in the
+// warp's slice of shared memory (rows up to kWarpRowMax entries; longer
+// ones are worked on in v, through L2).  Rows are claimed one at a time in
+// level order from the ticket, so the lowest unfinished row always has its
+// inputs and the pass cannot deadlock.
+constexpr int kWarpRowMax = 128;
+constexpr int kWarpPairs = 4;
+constexpr size_t kWarpSmem = sizeof(double) * kWarpRowMax * (kFactorThreads / 32);
+
+struct WarpRow {
+  double *sh; // the warp's shared slice, or nullptr: the row's values in v
+  double *g;  // v + rs
+  __device__ double get(int q) const { return sh ? sh[q] : __ldcg(g + q); }
+  __device__ void set(int q, double x) const {
+    if (sh)
+      sh[q] = x;
+    else
+      __stcg(g + q, x);
+  }
+};
+
+template <int KIND>
+__global__ void __launch_bounds__(kFactorThreads)
+    factor_warp_kernel(const int n, const int *__restrict__ exec_row,
+                       const int *__restrict__ rs_of, const int *__restrict__ diag_of,
+                       const int *__restrict__ uptr, const int *__restrict__ uk,
+                       const int *__restrict__ us, const int *__restrict__ upiv,
+                       const int *__restrict__ pptr, const int *__restrict__ ptgt,
+                       const int *__restrict__ psrc, const double *__restrict__ vin, double *v,
+                       const double diag_scale, int *done, int *state, const int sleep_ns) {
+  extern __shared__ double factor_smem[];
+  const int lane = threadIdx.x & 31;
+  double *slice = factor_smem + (threadIdx.x >> 5) * kWarpRowMax;
+  for (;;) {
+    int p = 0;
+    if (lane == 0) // lane 0 alone decides; the warp leaves together
+      p = ld_acquire(state + 1) != 0 ? n : atomicAdd(state, 1);
+    p = __shfl_sync(0xffffffffu, p, 0);
+    if (p >= n)
+      return;
+    const int j = __ldg(exec_row + p);
+    const int rs = __ldg(rs_of + j), len = __ldg(rs_of + j + 1) - rs;
+    const WarpRow w{len <= kWarpRowMax ? slice : nullptr, v + rs};
+    for (int q = lane; q < len; q += 32)
+      w.set(q, __ldg(vin + rs + q));
+    __syncwarp();
+    if (KIND == kIC0 && lane == 0)
+      w.set(0, __dmul_rn(w.get(0), diag_scale)); // the (1 + omega) shift
+    const int u0 = __ldg(uptr + j), u1 = __ldg(uptr + j + 1);
+    // every source row published: a lane per update, polled together
+    bool gave_up = false;
+    const unsigned long long t0 = factor_ns();
+    for (int ub = u0; ub < u1 && !gave_up; ub += 32) {
+      const int k = ub + lane < u1 ? __ldg(uk + ub + lane) : -1;
+      bool ready = k < 0;
+      for (unsigned pass = 1;; pass++) {
+        if (!ready)
+          ready = ld_acquire(done + k) != 0;
+        if (__all_sync(0xffffffffu, ready))
+          break;
+        if ((pass & 63u) == 0u) {
+          bool stop = false;
+          if (lane == 0)
+            stop = ld_acquire(state + 1) != 0 || factor_ns() - t0 > kFactorWaitNs;
+          if (__shfl_sync(0xffffffffu, stop, 0)) {
+            gave_up = true;
+            break;
+          }
+        }
+        if (sleep_ns > 0)
+          __nanosleep(sleep_ns);
+      }
+    }
+    if (gave_up) { // the row stays unpublished; the warp stops at its next claim
+      if (lane == 0)
+        atomicExch(state + 1, 1);
+      continue;
+    }
+    __syncwarp(); // the lanes' acquires order the source rows' values for all lanes
+    for (int ub = u0; ub < u1; ub += 32) {
+      const int nb = min(32, u1 - ub), u = ub + lane;
+      int e0 = 0, e1 = 0, own = 0;
+      double sv = 0.0;
+      if (lane < nb) {
+        e0 = __ldg(pptr + u);
+        e1 = __ldg(pptr + u + 1);
+        sv = __ldcg(v + __ldg(KIND == kIC0 ? us + u : upiv + u));
+        if (KIND == kILU0)
+          own = __ldg(us + u) - rs;
+      }
+      const int E0 = __shfl_sync(0xffffffffu, e0, 0), E1 = __shfl_sync(0xffffffffu, e1, nb - 1);
+      const bool held = E1 - E0 <= 32 * kWarpPairs; // every pair in registers
+      int tg[kWarpPairs];
+      double src[kWarpPairs];
+      if (held) {
+#pragma unroll
+        for (int r = 0; r < kWarpPairs; r++) {
+          const int e = E0 + r * 32 + lane;
+          tg[r] = e < E1 ? __ldg(ptgt + e) - rs : -1;
+          src[r] = e < E1 ? __ldcg(v + __ldg(psrc + e)) : 0.0;
+        }
+      }
+      for (int q = 0; q < nb; q++) {
+        const int qe0 = __shfl_sync(0xffffffffu, e0, q), qe1 = __shfl_sync(0xffffffffu, e1, q);
+        const double sq = __shfl_sync(0xffffffffu, sv, q);
+        double s;
+        if (KIND == kIC0) {
+          s = sq; // U_kj, final
+        } else {
+          const int oq = __shfl_sync(0xffffffffu, own, q);
+          s = __ddiv_rn(w.get(oq), sq); // L_jk = a_jk / u_kk
+          __syncwarp();
+          if (lane == 0)
+            w.set(oq, s);
+        }
+        if (held) {
+#pragma unroll
+          for (int r = 0; r < kWarpPairs; r++) {
+            const int e = E0 + r * 32 + lane;
+            if (e >= qe0 && e < qe1)
+              w.set(tg[r], __dsub_rn(w.get(tg[r]), __dmul_rn(s, src[r])));
+          }
+        } else {
+          for (int e = qe0 + lane; e < qe1; e += 32) {
+            const int t = __ldg(ptgt + e) - rs;
+            w.set(t, __dsub_rn(w.get(t), __dmul_rn(s, __ldcg(v + __ldg(psrc + e)))));
+          }
+        }
+        __syncwarp();
+      }
+    }
+    if (KIND == kIC0) {
+      double piv = 0.0;
+      if (lane == 0) {
+        const double d = w.get(0);
+        if (d < 0.0)
+          atomicMin(state + 2, j);
+        piv = __dsqrt_rn(d);
+        w.set(0, piv);
+      }
+      piv = __shfl_sync(0xffffffffu, piv, 0);
+      for (int q = 1 + lane; q < len; q += 32)
+        w.set(q, __ddiv_rn(w.get(q), piv));
+    } else if (lane == 0 && w.get(__ldg(diag_of + j) - rs) == 0.0) {
+      atomicMin(state + 2, j);
+    }
+    __syncwarp();
+    if (w.sh)
+      for (int q = lane; q < len; q += 32)
+        v[rs + q] = w.sh[q];
+    __syncwarp();
+    if (lane == 0) {
+      __threadfence();
+      st_release(done + j, 1);
+    }
+  }
+}
+
 template <int KIND>
 __global__ void __launch_bounds__(kFactorThreads)
     factor_kernel(const int nchunks, const int *__restrict__ chunk_start,
@@ -551,6 +716,7 @@ la_status plan_build(la_factor_plan_s *P, const int *ai, const int *aj, Symbolic
   std::vector<int> erow, cstart;
   schedule(n, S, erow, cstart, &P->levels);
   P->nchunks = (int)cstart.size() - 1;
+  P->npairs = (long long)S.ptgt.size();
   std::vector<int> rs(n + 1);
   for (int j = 0; j <= n; j++)
     rs[j] = ai[j] - P->base;
@@ -581,9 +747,18 @@ la_status plan_finish(la_factor_plan_s *P) {
   LA_TRY(P->vin.alloc(sizeof(double) * std::max(P->nnz, 1)));
   LA_TRY(P->done.alloc(sizeof(int) * std::max(n, 1)));
   LA_TRY(P->state.alloc(sizeof(int) * 4));
+  // one warp per row when rows receive many pairs (more than 8 on average);
+  // LA_FACTOR_WARP=0/1 forces either form (testing / tuning override)
+  P->warp = P->npairs > 8LL * n;
+  if (const char *e = std::getenv("LA_FACTOR_WARP"))
+    P->warp = std::atoi(e) != 0;
   int per_sm = 0;
-  LA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &per_sm, (const void *)factor_kernel<kIC0>, kFactorThreads, kFactorSmem));
+  if (P->warp)
+    LA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, (const void *)factor_warp_kernel<kIC0>, kFactorThreads, kWarpSmem));
+  else
+    LA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, (const void *)factor_kernel<kIC0>, kFactorThreads, kFactorSmem));
   // LA_FACTOR_CTAS_PER_SM caps the CTAs per SM (tuning override; default:
   // as many as fit).  Warps beyond what the widest levels use only poll.
   per_sm = std::max(per_sm, 1);
@@ -592,7 +767,8 @@ la_status plan_finish(la_factor_plan_s *P) {
     P->sleep_ns = std::max(0, std::atoi(e));
   if (const char *e = std::getenv("LA_FACTOR_CTAS_PER_SM"))
     per_sm = std::min(per_sm, std::max(1, std::atoi(e)));
-  const int need = (P->nchunks + kFactorThreads / 32 - 1) / (kFactorThreads / 32);
+  const int units = P->warp ? n : P->nchunks; // what a warp claims: a row or a chunk
+  const int need = (units + kFactorThreads / 32 - 1) / (kFactorThreads / 32);
   P->grid = std::max(1, std::min(per_sm * sm_count(), need));
   return LA_OK;
 }
@@ -825,6 +1001,7 @@ la_status plan_build_ic0_device(la_factor_plan_s *P, const int *ai, const int *a
   take(P->psrc, psrc);
   P->levels = lv;
   P->nchunks = nchunks;
+  P->npairs = npairs;
   LA_TRY(plan_finish(P));
   *ok = true;
   return LA_OK;
@@ -853,12 +1030,22 @@ la_status factor_numeric(la_factor_plan_s *P, const double *av, double omega, do
   const int init[4] = {0, 0, 0x7fffffff, 0};
   LA_CUDA_TRY(cudaMemcpyAsync(P->state.p, init, sizeof(init), cudaMemcpyHostToDevice, st));
   LA_CUDA_TRY(cudaMemsetAsync(P->done.p, 0, sizeof(int) * P->n, st));
-  auto launch = P->kind == kIC0 ? factor_kernel<kIC0> : factor_kernel<kILU0>;
-  launch<<<P->grid, kFactorThreads, kFactorSmem, st>>>(
-      P->nchunks, P->chunk_start.as<int>(), P->exec_row.as<int>(), P->rs.as<int>(),
-      P->diag.as<int>(), P->uptr.as<int>(), P->uk.as<int>(), P->us.as<int>(), P->upiv.as<int>(),
-      P->pptr.as<int>(), P->ptgt.as<int>(), P->psrc.as<int>(), P->vin.as<double>(), v,
-      1.0 + omega, P->done.as<int>(), P->state.as<int>(), P->sleep_ns);
+  if (P->warp) {
+    auto launch = P->kind == kIC0 ? factor_warp_kernel<kIC0> : factor_warp_kernel<kILU0>;
+    launch<<<P->grid, kFactorThreads, kWarpSmem, st>>>(
+        P->n, P->exec_row.as<int>(), P->rs.as<int>(), P->diag.as<int>(), P->uptr.as<int>(),
+        P->uk.as<int>(), P->us.as<int>(), P->upiv.as<int>(), P->pptr.as<int>(),
+        P->ptgt.as<int>(), P->psrc.as<int>(), P->vin.as<double>(), v, 1.0 + omega,
+        P->done.as<int>(), P->state.as<int>(), P->sleep_ns);
+  } else {
+    auto launch = P->kind == kIC0 ? factor_kernel<kIC0> : factor_kernel<kILU0>;
+    launch<<<P->grid, kFactorThreads, kFactorSmem, st>>>(
+        P->nchunks, P->chunk_start.as<int>(), P->exec_row.as<int>(), P->rs.as<int>(),
+        P->diag.as<int>(), P->uptr.as<int>(), P->uk.as<int>(), P->us.as<int>(),
+        P->upiv.as<int>(), P->pptr.as<int>(), P->ptgt.as<int>(), P->psrc.as<int>(),
+        P->vin.as<double>(), v, 1.0 + omega, P->done.as<int>(), P->state.as<int>(),
+        P->sleep_ns);
+  }
   LA_CUDA_TRY(cudaGetLastError());
   int state[4];
   LA_CUDA_TRY(cudaMemcpyAsync(state, P->state.p, sizeof(state), cudaMemcpyDeviceToHost, st));

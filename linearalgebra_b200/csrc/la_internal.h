@@ -213,6 +213,7 @@ struct la_trsv_plan_s {
   int nchunks = 0;
   int grid = 0;
   int kd = 0; // dependency slots of the kernel variant (0: grouped form)
+  int sleep_ns = 0; // level order: pause between polls of unpublished values
   // schedule: 0 = level order over the whole GPU with per-row readiness;
   // 1 = partitioned (one co-resident CTA per part, part values in shared
   // memory).  For schedule 1 the execution order is part-major, level-minor
@@ -255,6 +256,8 @@ struct la_factor_plan_s {
   int kind = 0; // 0: IC(0), 1: ILU(0)
   int n = 0, nnz = 0, base = 0, levels = 0, nchunks = 0, grid = 0;
   int sleep_ns = 0; // the numeric pass's pause between polls of unpublished rows
+  long long npairs = 0; // (target, source) pairs of all updates
+  bool warp = false;    // numeric pass: one warp per row (many pairs a row)
   // per row (original numbering): its value range [rs, re) and its diagonal
   la::DevBuf rs, diag;
   // rows in execution order, 32-row chunks that never cross a level

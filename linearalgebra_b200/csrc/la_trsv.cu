@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(kThreads)
                       const V *__restrict__ av, const V *__restrict__ diag,
                       const int *__restrict__ exec_row,
                       const X *__restrict__ b, X *x, const int base, int *err,
-                      int *ticket) {
+                      int *ticket, const int sleep_ns) {
   const int lane = threadIdx.x & 31;
   for (;;) {
     int c = 0;
@@ -279,6 +279,8 @@ __global__ void __launch_bounds__(kThreads)
           atomicExch(err, 1);
         return;
       }
+      if (sleep_ns > 0)
+        __nanosleep(sleep_ns);
     }
   }
 }
@@ -591,15 +593,15 @@ void launch_kernel(la_trsv_plan_t P, const X *b, X *x, cudaStream_t st) {
   switch (P->kd) {
   case 4:
     trsv_level_kernel<V, X, UNIT, 4><<<g, t, 0, st>>>(P->nchunks, cs, ai, aj, av, dg, er, b,
-                                                      x, P->base, err, tk);
+                                                      x, P->base, err, tk, P->sleep_ns);
     break;
   case 8:
     trsv_level_kernel<V, X, UNIT, 8><<<g, t, 0, st>>>(P->nchunks, cs, ai, aj, av, dg, er, b,
-                                                      x, P->base, err, tk);
+                                                      x, P->base, err, tk, P->sleep_ns);
     break;
   case 16:
     trsv_level_kernel<V, X, UNIT, 16><<<g, t, 0, st>>>(P->nchunks, cs, ai, aj, av, dg, er,
-                                                       b, x, P->base, err, tk);
+                                                       b, x, P->base, err, tk, P->sleep_ns);
     break;
   default:
     trsv_level_kernel_grouped<V, X, UNIT><<<g, t, 0, st>>>(P->nchunks, cs, ai, aj, av, dg,
@@ -1085,6 +1087,8 @@ la_status trsv_build(la_trsv_plan_t P, const int *ai, const int *aj,
     if (ok)
       return LA_OK;
   }
+  if (const char *e = std::getenv("LA_TRSV_SLEEP_NS")) // tuning override
+    P->sleep_ns = std::max(0, std::atoi(e));
   std::vector<int> eai(n + 1), erow(n), cstart;
   // filled below on the host's threads, every entry written: no initialisation
   std::unique_ptr<int[]> eaj(new int[std::max(P->nnz, 1)]);

@@ -176,6 +176,59 @@ def test_ic0_device_plan_large_patterns(lab):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("warp", ["0", "1"])
+def test_factor_both_forms_bit_identical(lab, monkeypatch, warp):
+    """The numeric pass in both forms -- a lane per row (LA_FACTOR_WARP=0)
+    and a warp per row (=1; chosen by itself when rows receive more than 8
+    pairs on average) -- on IC(0) of stencils (short and 27-point rows, in
+    natural and RCM order), an irregular pattern with rows over 128 entries
+    (their values worked on in global memory), ILU(0) with long rows, a
+    shift, a breakdown and base 1: always the host's factor bit for bit."""
+    from linearalgebra_b200 import gen
+    monkeypatch.setenv("LA_FACTOR_WARP", warp)
+    big = _random_spd(6000, 4)
+    # one row of 200 entries: longer than the warp's shared slice
+    n0, ai0, aj0, av0 = big
+    rows = [list(aj0[ai0[i]:ai0[i + 1]]) for i in range(n0)]
+    extra = np.random.default_rng(1).choice(np.arange(1, n0), 200, replace=False)
+    for c in extra:
+        if c not in rows[0]:
+            rows[0].append(int(c))
+            rows[int(c)].append(0)
+    ai = np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(np.int32)
+    aj = np.concatenate([sorted(r) for r in rows]).astype(np.int32)
+    r = np.repeat(np.arange(n0), np.diff(ai))
+    av = np.where(aj == r, 0.0, -0.3)
+    av[aj == r] = np.bincount(r, np.abs(av), minlength=n0) + 1.0
+    for name, mat, rcm in (("lap3d_24", gen.laplacian_3d(24), True),
+                           ("st27_16", gen.stencil27(16, seed=2), False),
+                           ("st27_16_rcm", gen.stencil27(16, seed=2), True),
+                           ("long_rows", (n0, ai, aj, av), False)):
+        n, ua, uj, uv = _ic_inputs(lab, mat, rcm)
+        want = lab.ICCLevelNumeric0(n, 0, ua, uj, uv)
+        plan = lab.FactorPlan("ic0", n, 0, ua, uj)
+        assert np.array_equal(plan.factor(uv), want), (name, warp)
+        want2 = lab.ICCLevelNumeric0(n, 0, ua, uj, uv, omega=0.25)
+        assert np.array_equal(plan.factor(uv, omega=0.25), want2), (name, warp)
+        got1 = lab.FactorPlan("ic0", n, 1, ua + 1, uj + 1).factor(uv)
+        assert np.array_equal(got1, want), (name, warp, "base 1")
+    # breakdown at the row where the sequential pass stops
+    n, ua, uj, uv = _ic_inputs(lab, gen.stencil27(12, seed=3), False)
+    j0 = n // 2
+    bad = uv.copy()
+    bad[ua[j0]] = 0.1
+    with pytest.raises(lab.LAError):
+        lab.ICCLevelNumeric0(n, 0, ua, uj, bad)
+    with pytest.raises(lab.LAError) as e:
+        lab.FactorPlan("ic0", n, 0, ua, uj).factor(bad)
+    assert e.value.name == "LA_ERR_BREAKDOWN" and e.value.bad_row == j0, warp
+    for n, ai, aj, av in (gen.laplacian_3d(16), _nonsym(2000, 6, long_every=5),
+                          _nonsym(2000, 8, long_every=1)):
+        want = lab.ILU0(n, 0, ai, aj, av)
+        assert np.array_equal(lab.FactorPlan("ilu0", n, 0, ai, aj).factor(av), want), (n, warp)
+
+
+@pytest.mark.gpu
 def test_ic0_device_base1_and_breakdown(lab):
     from linearalgebra_b200 import gen
     n, ua, uj, uv = _ic_inputs(lab, gen.laplacian_3d(16), True)
