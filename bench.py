@@ -293,11 +293,15 @@ def adjoint_case(la, torch, peak):
     nnz = int(ai[-1])
     t0 = time.perf_counter()
     ua, uj, uv = la.SplitTriangle("U", n, 0, ai, aj, av)
-    f = la.ICCLevelNumeric0(n, 0, ua, uj, uv)
+    f = la.FactorPlan("ic0", n, 0, ua, uj).factor(uv)  # IC(0) on the GPU
     A = la.CSR(n, n, 0, ai, aj, av)
     s = la.PCG(A, ua, uj, f)
     plan = la.SPMV(A)
     setup_s = time.perf_counter() - t0
+    t1 = time.perf_counter()
+    f_host = la.ICCLevelNumeric0(n, 0, ua, uj, uv)
+    icc0_host_s = time.perf_counter() - t1
+    icc0_identical = bool(np.array_equal(f, f_host))
     rng = np.random.default_rng(0)
     us = torch.as_tensor(rng.standard_normal(n)).cuda()
     b = torch.as_tensor(rng.standard_normal(n)).cuda()
@@ -328,7 +332,8 @@ def adjoint_case(la, torch, peak):
     t_ai, t_aj, t_av = la.Transpose(n, n, 0, s_ai, s_aj, s_av)
     ts = la.OptimizedTriangularSolve("L").analysis(n, 0, t_ai, t_aj, t_av, d)
     return {"config": "C4_stencil27_96_fp64", "n": n, "nnz": nnz, "rtol": 1e-10,
-            "setup_s": setup_s, "levels": ts.levels()[0],
+            "setup_s": setup_s, "icc0_host_s": icc0_host_s,
+            "icc0_device_bit_identical": icc0_identical, "levels": ts.levels()[0],
             "trsv_schedule": list(ts.schedule()),
             "forward_pcg": {"iterations": rf.iterations, "ms": fwd_ms,
                             "rel_residual": rf.rel_residual},
