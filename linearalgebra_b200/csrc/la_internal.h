@@ -213,7 +213,6 @@ struct la_trsv_plan_s {
   int nchunks = 0;
   int grid = 0;
   int kd = 0; // dependency slots of the kernel variant (0: grouped form)
-  int nosync = 0; // partitioned: no barrier per level (whole parts only)
   int sleep_ns = 0; // level order: pause between polls of unpublished values
   // schedule: 0 = level order over the whole GPU with per-row readiness;
   // 1 = partitioned (one co-resident CTA per part, part values in shared

@@ -353,17 +353,12 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
                      const V *__restrict__ av, const int *__restrict__ ej,
                      const V *__restrict__ ev, const V *__restrict__ diag,
                      const int *__restrict__ exec_row, const X *__restrict__ b, X *x,
-                     int *err, const int tail, const int rows_cap, const int ring_mask,
-                     const int nosync) {
+                     int *err, const int tail, const int rows_cap, const int ring_mask) {
   constexpr int T = part_threads<X, KD>();
   const bool ring = ring_mask != kNoRing;
   extern __shared__ __align__(16) unsigned char part_smem[];
   X *xs = reinterpret_cast<X *>(part_smem);
-  // nosync (whole parts only): no barrier per level; a row's x slot is
-  // marked final in a bit array and its readers wait (bounded) on that bit
-  const int nbw = nosync ? (rows_cap + 31) / 32 : 0;
-  unsigned *final_bits = reinterpret_cast<unsigned *>(xs + rows_cap);
-  int *ssb = reinterpret_cast<int *>(final_bits + nbw); // level boundaries
+  int *ssb = reinterpret_cast<int *>(xs + rows_cap); // level boundaries
   const int p = blockIdx.x, tid = threadIdx.x;
   const int P0 = __ldg(pstart + p), P1 = __ldg(pstart + p + 1);
   const int q0 = __ldg(psub + p), q1 = __ldg(psub + p + 1);
@@ -411,17 +406,6 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
     }
     return v;
   };
-  // a row of this part (nosync): wait (bounded) until its slot is final
-  auto await_local = [&](int d) {
-    const volatile unsigned *w = final_bits + (d >> 5);
-    for (unsigned pass = 1; !((*w >> (d & 31)) & 1u) && !aborted; pass++)
-      if ((pass & 63u) == 0u && (dev::ld_relaxed(err) != 0 || global_ns() - t0 > kWaitNs)) {
-        atomicExch(err, 1);
-        aborted = 1;
-      }
-    __threadfence_block();
-    return reinterpret_cast<const volatile X *>(xs)[d];
-  };
   // The slot reads are issued together (no branch between them), values of
   // other parts that were not yet published are waited for afterwards (the
   // rare case), and only then is the row summed in stored order -- an unused
@@ -442,8 +426,6 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
       const int c = R.j[s];
       if (c >= 0 && c != kEmptySlot && (!armed || Sentinel<X>::is(v[s])))
         v[s] = await(c, armed ? v[s] : dev::ld_relaxed(x + c));
-      else if (nosync && c < 0)
-        v[s] = await_local(-1 - c);
     }
     X sum = X(0);
 #pragma unroll
@@ -453,8 +435,7 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
       const int k1 = __ldg(ai + R.r + 1);
       for (int k = __ldg(ai + R.r) + KD; k < k1; k++) {
         const int c = __ldg(aj + k);
-        const X v = c < 0 ? (nosync ? await_local(-1 - c) : xs[-1 - c])
-                          : await(c, dev::ld_relaxed(x + c));
+        const X v = c < 0 ? xs[-1 - c] : await(c, dev::ld_relaxed(x + c));
         sum = add_rn(sum, mul_rn(X(__ldg(av + k)), v));
       }
     }
@@ -462,10 +443,6 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
     if (!UNIT)
       xi = div_rn(xi, R.dg);
     xs[slot] = xi;
-    if (nosync) { // the value first, then its bit
-      __threadfence_block();
-      atomicOr(final_bits + (slot >> 5), 1u << (slot & 31));
-    }
     dev::st_relaxed(x + R.i, Sentinel<X>::scrub(xi));
   };
   // W2: a thread's second row of level q (r = level start + T + tid)
@@ -511,8 +488,6 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
 
   for (int q = q0 + tid; q <= q1; q += T)
     ssb[q - q0] = __ldg(sb + q);
-  for (int w = tid; w < nbw; w += T)
-    final_bits[w] = 0u;
   __syncthreads();
   // Slices of the row arrays are pulled into L2 several levels ahead, four
   // levels per fire-and-forget bulk prefetch, one array per warp, so the
@@ -586,22 +561,22 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
     arm(R2);
     l2_ahead(q + 8, q + 12); // four levels per bulk prefetch
     prefetch(q + 3, R3);
-    if ((nosync ? aborted : __syncthreads_or(aborted)) || q + 1 >= q1)
+    if (__syncthreads_or(aborted) || q + 1 >= q1)
       break;
     run_level(q + 1, R1, S1, S0);
     arm(R3);
     prefetch(q + 4, R0);
-    if ((nosync ? aborted : __syncthreads_or(aborted)) || q + 2 >= q1)
+    if (__syncthreads_or(aborted) || q + 2 >= q1)
       break;
     run_level(q + 2, R2, S0, S1);
     arm(R0);
     prefetch(q + 5, R1);
-    if ((nosync ? aborted : __syncthreads_or(aborted)) || q + 3 >= q1)
+    if (__syncthreads_or(aborted) || q + 3 >= q1)
       break;
     run_level(q + 3, R3, S1, S0);
     arm(R1);
     prefetch(q + 6, R2);
-    if (nosync ? aborted : __syncthreads_or(aborted))
+    if (__syncthreads_or(aborted))
       break;
   }
   if (ring) // no copy may still be landing when the CTA leaves (an abort)
@@ -647,11 +622,11 @@ cudaError_t launch_parts_kd(la_trsv_plan_t P, const X *b, X *x, cudaStream_t st)
             *er = P->exec_row.as<int>();
   const V *av = P->av.as<V>(), *ev = P->ev.as<V>(), *dg = P->diag.as<V>();
   int *err = P->err.as<int>();
-  const int cap = P->part_rows, mask = P->ring_mask, nosync = P->nosync;
-  void *args[] = {(void *)&n,   (void *)&ps,   (void *)&pq,    (void *)&sb,  (void *)&ai,
-                  (void *)&aj,  (void *)&av,   (void *)&ej,    (void *)&ev,  (void *)&dg,
-                  (void *)&er,  (void *)&b,    (void *)&x,     (void *)&err, (void *)&tail,
-                  (void *)&cap, (void *)&mask, (void *)&nosync};
+  const int cap = P->part_rows, mask = P->ring_mask;
+  void *args[] = {(void *)&n,  (void *)&ps, (void *)&pq, (void *)&sb,  (void *)&ai,
+                  (void *)&aj, (void *)&av, (void *)&ej, (void *)&ev,  (void *)&dg,
+                  (void *)&er, (void *)&b,  (void *)&x,  (void *)&err, (void *)&tail,
+                  (void *)&cap, (void *)&mask};
   return cudaLaunchCooperativeKernel(part_fn<V, X, UNIT, KD, W2>(), dim3(P->nparts),
                                      dim3(part_threads<X, KD>()), args, P->part_smem, st);
 }
@@ -870,15 +845,7 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
       for (int g = psub[p]; g < psub[p + 1]; g++)
         if (end2(p, g) - sb[g] > ring)
           return LA_OK; // three consecutive levels must fit in the ring
-  // LA_TRSV_NOSYNC=1: no barrier per level (whole parts; testing / tuning override)
-  int nosync = 0;
-  if (const char *e = std::getenv("LA_TRSV_NOSYNC"))
-    nosync = !ring && std::atoi(e) != 0;
-  const size_t bits_need = sizeof(unsigned) * ((size_t)(rows_max + 31) / 32);
-  if (nosync && sizeof(X) * (size_t)rows_max + bits_need + sb_bytes + 1024 > (size_t)optin)
-    nosync = 0; // the bit array does not fit beside the part's rows
-  const size_t bits_bytes = nosync ? bits_need : 0;
-  const size_t smem = sizeof(X) * (size_t)(ring ? ring : rows_max) + bits_bytes + sb_bytes;
+  const size_t smem = sizeof(X) * (size_t)(ring ? ring : rows_max) + sb_bytes;
   const void *fns[2];
   int threads = 0;
   // second-row register sets when some level of a part is wider than the
@@ -1055,7 +1022,6 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
   P->ring_mask = ring ? ring - 1 : kNoRing;
   P->w2 = w2;
   P->part_smem = smem;
-  P->nosync = nosync;
   P->sched = 1;
   *ok = true;
   return LA_OK;

@@ -274,49 +274,6 @@ def test_trsv_schedules_bit_identical(lab, orc, monkeypatch, schedule):
             assert np.array_equal(x32, y32), (n, uplo, "fp32 schedules differ")
 
 
-@pytest.mark.gpu
-def test_trsv_parts_without_level_barriers_bit_identical(lab, orc, monkeypatch):
-    """The partitioned solve without a barrier per level (LA_TRSV_NOSYNC=1:
-    rows of the part wait on a shared-memory bit of each row they read):
-    the oracle's level solve bit for bit, FP64 and FP32, both triangles,
-    rows longer than the register slots, many parts and few, the
-    second-row (W2) variant."""
-    from linearalgebra_b200 import gen
-    P = orc.ptr
-    monkeypatch.setenv("LA_TRSV_SCHEDULE", "parts")
-    monkeypatch.setenv("LA_TRSV_NOSYNC", "1")
-    cases = []
-    for n, ai, aj, av in (gen.laplacian_3d(40), gen.stencil27(16), gen.aniso7(28, seed=3)):
-        _, lt, ut, d = _ic_factor_rcm(lab, n, ai, aj, av)
-        cases += [(n, "L", lt, d), (n, "U", ut, d)]
-    n = 30_000
-    cases.append((n, "L", _long_rows_lower(n, 1), np.random.default_rng(2).uniform(1, 2, n)))
-    for parts in (None, "3"):
-        if parts:
-            monkeypatch.setenv("LA_TRSV_PARTS", parts)
-        for n, uplo, (c_ai, c_aj, c_av), d in cases:
-            b = np.random.default_rng(n).uniform(-1, 1, n)
-            ts, x = solve(lab, uplo, n, c_ai, c_aj, c_av, d, b)
-            assert ts.schedule()[0] == "parts"
-            lv, ip, pf = ts.levels()
-            ref = np.zeros(n)
-            orc.port().oracle_level_solve(lv, P(ip), P(pf), 0, P(c_ai), P(c_aj), P(c_av),
-                                          P(d), P(b), P(ref))
-            assert np.array_equal(x, ref), (n, uplo, parts)
-            ts32, x32 = solve(lab, uplo, n, c_ai, c_aj, c_av, d, b, dtype=np.float32)
-            assert np.array_equal(x32, _oracle_f32(orc, lv, ip, pf, c_ai, c_aj, c_av, d, b))
-    # W2 (FP32 3-slot rows, part-levels wider than the CTA): two parts of the
-    # RCM-ordered 40^3 factor (32,000 rows each: values and bits fit)
-    monkeypatch.setenv("LA_TRSV_PARTS", "2")
-    n, ai, aj, av = gen.laplacian_3d(40)
-    _, lt, _, d = _ic_factor_rcm(lab, n, ai, aj, av)
-    b = np.random.default_rng(5).uniform(-1, 1, n)
-    ts32, x32 = solve(lab, "L", n, *lt, d, b, dtype=np.float32)
-    assert ts32.variant() == (3, True)
-    lv, ip, pf = ts32.levels()
-    assert np.array_equal(x32, _oracle_f32(orc, lv, ip, pf, *lt, d, b))
-
-
 def _oracle_f32(orc, lv, ip, pf, c_ai, c_aj, c_av, d, b):
     """The oracle's FP32 level solve (float storage, one float operation per
     step, the reference's row order), as float64 for comparison."""
