@@ -559,6 +559,14 @@ def run_case(case):
             t_ai, t_aj, _ = la.Transpose(n, n, 0, s_ai, s_aj, s_av)
             for _ in range(3):
                 la.TopologicalSort2("L", n, 0, t_ai, t_aj, device=True)
+    elif case == "factor-c4":
+        # IC(0) of the 96^3 27-point stencil (natural order) on the GPU: the
+        # warp-per-row numeric pass
+        n, ai, aj, av = gen.stencil27(96, seed=0)
+        ua, uj, uv = la.SplitTriangle("U", n, 0, ai, aj, av)
+        fp = la.FactorPlan("ic0", n, 0, ua, uj)
+        for _ in range(3):
+            fp.factor(uv)
     elif case == "rcm-c3":
         # reverse Cuthill-McKee of the 128^3 Laplacian ordered on the GPU
         n, ai, aj, av = gen.laplacian_3d(128)
@@ -643,7 +651,7 @@ def main():
     ap.add_argument("--case", default=None,
                     choices=["spmv-powerlaw", "spmv-lap3d", "trsv-lap3d", "trsv-c5-f32",
                              "pcg-lap3d", "adjoint-c4", "factor-c3", "levels-c3", "ingest",
-                             "noalloc-c3", "rcm-c3", "icplan-c3"],
+                             "noalloc-c3", "rcm-c3", "icplan-c3", "factor-c4"],
                     help="run one kernel workload a few times and exit (for ncu)")
     args = ap.parse_args()
     args.steps_given = args.steps is not None
