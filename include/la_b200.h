@@ -399,6 +399,12 @@ la_status la_trsv_analysis_transposed(la_uplo uplo, int n, int base, const int *
  * partition with nparts = one per SM when its cost model prefers it. */
 la_status la_trsv_partition(la_uplo uplo, int n, int base, const int *ai, const int *aj,
                             int nparts, int *part, int *coords);
+/* The same partition with its landmark stage on the GPU -- the undirected
+ * graph, the landmark searches and the candidate checks -- as the analysis
+ * computes it; part and *coords identical to la_trsv_partition's.  HOST
+ * arrays; needs a device (LA_ERR_NO_DEVICE otherwise). */
+la_status la_trsv_partition_device(la_uplo uplo, int n, int base, const int *ai,
+                                   const int *aj, int nparts, int *part, int *coords);
 /* x = T^-1 b (triangle_solve.tpp:115-155 operator()/BarrierOp): b, x device
  * arrays of the plan's dtype; b and x must not alias.  LA_ERR_TIMEOUT if a
  * dependency wait exceeded its bound (x is then undefined). */

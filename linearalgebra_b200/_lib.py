@@ -83,6 +83,7 @@ _SIGS = {
     "la_trsv_analysis_levels": [I, I, I, P, P, P, P, I, P, P, I, C.POINTER(P)],
     "la_trsv_analysis_transposed": [I, I, I, P, P, P, P, I, C.POINTER(P)],
     "la_trsv_partition": [I, I, I, P, P, I, P, P],
+    "la_trsv_partition_device": [I, I, I, P, P, I, P, P],
     "la_topological_sort": [I, I, I, P, P, P, P, P],
     "la_permute_vec": [I, I, P, P, P],
     "la_ilu0": [I, I, P, P, P, P],

@@ -440,13 +440,16 @@ class OptimizedTriangularSolve:
 
 
 # --------------------------------------------------------- host analysis
-def trsv_partition(uplo, n, base, ai, aj, nparts):
+def trsv_partition(uplo, n, base, ai, aj, nparts, device=False):
     """(part[n], coordinates used): the row partition the partitioned solve
-    schedule cuts for this strict triangle (host only)."""
+    schedule cuts for this strict triangle -- on the host, or with its
+    landmark stage on the GPU (``device=True``, as the analysis computes it;
+    the same partition)."""
     ai, aj = _i32(ai), _i32(aj)
     part = np.empty(max(n, 1), np.int32)
     c = C.c_int()
-    call("la_trsv_partition", LA_LOWER if uplo in ("L", 0, LA_LOWER) else LA_UPPER, int(n),
+    call("la_trsv_partition_device" if device else "la_trsv_partition",
+         LA_LOWER if uplo in ("L", 0, LA_LOWER) else LA_UPPER, int(n),
          int(base), _ptr(ai), _ptr(aj), int(nparts), _ptr(part), C.byref(c))
     return part[:n], c.value
 

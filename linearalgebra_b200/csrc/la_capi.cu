@@ -835,6 +835,29 @@ la_status la_trsv_partition(la_uplo uplo, int n, int base, const int *ai, const 
   return LA_OK;
 }
 
+la_status la_trsv_partition_device(la_uplo uplo, int n, int base, const int *ai,
+                                   const int *aj, int nparts, int *part, int *coords) {
+  LA_CHECK_ARG(ai && part && n >= 0 && nparts >= 1, "arguments");
+  LA_CHECK_ARG(uplo == LA_LOWER || uplo == LA_UPPER, "uplo");
+  LA_TRY(check_strict_triangle(uplo, n, base, ai, aj));
+  LA_TRY(require_device());
+  int used = 0;
+  if (n > 0) {
+    std::vector<int> iperm(n), prefix(n + 1), lvl(n);
+    const int levels = topological_sort2(uplo, n, base, ai, aj, iperm.data(), prefix.data());
+    for (int l = 0; l < levels; l++)
+      for (int p = prefix[l]; p < prefix[l + 1]; p++)
+        lvl[iperm[p] - base] = l;
+    la_status st = LA_OK;
+    used = monotone_partition_device(n, base, ai, aj, lvl.data(), nparts, part, &st);
+    if (used < 0)
+      return st;
+  }
+  if (coords)
+    *coords = used;
+  return LA_OK;
+}
+
 la_status la_trsv(la_trsv_plan_t plan, const void *b, void *x,
                   la_stream_t stream) {
   LA_CHECK_ARG(plan && ((b && x) || plan->n == 0), "arguments");

@@ -144,18 +144,26 @@ la_status rcm(int n, int base, const int *ai, const int *aj, int *iperm, int *pe
 // row j for every stored (i, j) of dep_ptr/dep_col, which carry `base`), so
 // the parts' dependency graph is acyclic.  xadj/adj: the 0-based undirected
 // graph; lvl: the rows' levels.  Returns the number of coordinates used.
-// device: the landmark searches run on the GPU (bfs_device_*; same
-// distances), else on the host's threads.
 int monotone_partition(int n, const int *xadj, const int *adj, const int *dep_ptr,
-                       const int *dep_col, int base, const int *lvl, int nparts, int *part,
-                       bool device = false);
-// Breadth-first distances on the GPU over one 0-based undirected graph, for
-// any number of sources (la_rcm.cu's cooperative search): d[v] = distance
-// from src, -1 where unreachable; *reached = vertices reached.
-struct BfsDevice;
-BfsDevice *bfs_device_create(int n, const int *xadj, const int *adj, la_status *st);
-la_status bfs_device_dist(BfsDevice *B, int src, int *d, int *reached);
-void bfs_device_destroy(BfsDevice *B);
+                       const int *dep_col, int base, const int *lvl, int nparts, int *part);
+// The same partition with its landmark stage on the GPU (graph, searches,
+// candidate checks; LandmarksDevice below): identical parts.  Returns the
+// coordinates used, or -1 with *st set when a device step failed.
+int monotone_partition_device(int n, int base, const int *ai, const int *aj, const int *lvl,
+                              int nparts, int *part, la_status *st);
+// A candidate cut coordinate: sign * (d_a - d_b) for landmarks a < b (a = -1:
+// the level), with its range over the vertices.
+struct PartitionCand {
+  int a, b, sign;
+  long long range;
+};
+struct LandmarksDevice;
+LandmarksDevice *landmarks_device_create(int n, int base, const int *ai, const int *aj,
+                                         la_status *st);
+la_status landmarks_device_candidates(LandmarksDevice *M, std::vector<PartitionCand> &cands);
+la_status landmarks_device_coordinate(LandmarksDevice *M, const PartitionCand &c, int *f);
+void landmarks_device_destroy(LandmarksDevice *M);
+
 // The triangle's pattern made undirected and 0-based (both directions of
 // every stored entry), the graph monotone_partition walks.
 void undirected_pattern(int n, int base, const int *ai, const int *aj, std::vector<int> &xadj,

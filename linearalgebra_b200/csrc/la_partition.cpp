@@ -106,111 +106,17 @@ void undirected_pattern(int n, int base, const int *ai, const int *aj, std::vect
   }
 }
 
-int monotone_partition(int n, const int *xadj, const int *adj, const int *dep_ptr,
-                       const int *dep_col, int base, const int *lvl, int nparts, int *part,
-                       bool device) {
-  if (n == 0)
-    return 0;
-  // the landmark searches: on the GPU when asked (one upload of the graph,
-  // a cooperative launch per search), else on the host's threads
-  BfsDevice *bdev = nullptr;
-  struct Owner {
-    BfsDevice *&b;
-    ~Owner() {
-      if (b)
-        bfs_device_destroy(b);
-    }
-  } own{bdev};
-  if (device) {
-    la_status st = LA_OK;
-    bdev = bfs_device_create(n, xadj, adj, &st);
-    if (!bdev)
-      cudaGetLastError(); // e.g. out of memory: the host's searches instead
-  }
-  auto search = [&](int src, std::vector<int> &d) {
-    if (bdev) {
-      d.resize(n);
-      int reached = 0;
-      if (bfs_device_dist(bdev, src, d.data(), &reached) == LA_OK)
-        return reached;
-      bfs_device_destroy(bdev); // a failed search: the host's from here on
-      bdev = nullptr;
-      cudaGetLastError();
-    }
-    return bfs_dist(n, xadj, adj, src, d);
-  };
-  std::vector<std::vector<int>> coords; // chosen coordinates
-  std::vector<std::vector<double>> basis;
-  // candidate: orientation-normalised values, ascending range order later
-  struct Cand {
-    int a, b, sign;
-    long long range;
-  };
-  std::vector<Cand> cands;
-  std::vector<std::vector<int>> dist;
+namespace {
+
+// The stage after the landmark candidates: the level coordinate joins them,
+// the narrowest independent ones are chosen, and the k-d cuts are made.
+// coordinate(c, f) writes candidate c's values (c.a >= 0) into f and
+// returns false if it could not.  Returns the coordinates used, -1 on such
+// a failure.
+int cut_parts(int n, const int *lvl, int nparts, int *part, std::vector<PartitionCand> cands,
+              const std::function<bool(const PartitionCand &, std::vector<int> &)> &coordinate) {
+  using Cand = PartitionCand;
   {
-    int dmin = INT_MAX;
-    for (int v = 0; v < n; v++)
-      dmin = std::min(dmin, xadj[v + 1] - xadj[v]);
-    std::vector<int> low;
-    for (int v = 0; v < n; v++)
-      if (xadj[v + 1] - xadj[v] == dmin)
-        low.push_back(v);
-    std::vector<int> d, mind;
-    bool connected = search(low[0], d) == n;
-    if (connected) {
-      dist.push_back(d);
-      mind = d;
-      while (dist.size() < 8) {
-        int best = -1;
-        for (int v : low)
-          if (best < 0 || mind[v] > mind[best])
-            best = v;
-        if (best < 0 || mind[best] == 0)
-          break;
-        search(best, d);
-        dist.push_back(d);
-#pragma omp parallel for schedule(static)
-        for (int v = 0; v < n; v++)
-          mind[v] = std::min(mind[v], d[v]);
-      }
-    }
-    // landmark pairs, checked on the host's threads (integer work: the same
-    // candidates, kept in pair order, whatever the threads)
-    const int L = (int)dist.size();
-    std::vector<std::pair<int, int>> pairs;
-    for (int a = 0; a < L; a++)
-      for (int b = a + 1; b < L; b++)
-        pairs.push_back({a, b});
-    const int np = (int)pairs.size();
-    std::vector<Cand> found(np);
-    std::vector<char> keep(np, 0);
-#pragma omp parallel for schedule(dynamic)
-    for (int q = 0; q < np; q++) {
-      const int a = pairs[q].first, b = pairs[q].second;
-      const std::vector<int> &da = dist[a], &db = dist[b];
-      long long pos = 0, neg = 0;
-      for (int i = 0; i < n && !(pos && neg); i++)
-        for (int k = dep_ptr[i] - base; k < dep_ptr[i + 1] - base; k++) {
-          const int j = dep_col[k] - base;
-          const int df = (da[i] - db[i]) - (da[j] - db[j]);
-          pos += df > 0;
-          neg += df < 0;
-        }
-      if ((pos == 0) == (neg == 0))
-        continue; // not monotone, or constant along every edge
-      int lo = INT_MAX, hi = INT_MIN;
-      for (int v = 0; v < n; v++) {
-        const int f = da[v] - db[v];
-        lo = std::min(lo, f);
-        hi = std::max(hi, f);
-      }
-      found[q] = {a, b, pos > 0 ? 1 : -1, (long long)hi - lo};
-      keep[q] = 1;
-    }
-    for (int q = 0; q < np; q++)
-      if (keep[q])
-        cands.push_back(found[q]);
     int lo = INT_MAX, hi = INT_MIN;
     for (int v = 0; v < n; v++) {
       lo = std::min(lo, lvl[v]);
@@ -220,6 +126,8 @@ int monotone_partition(int n, const int *xadj, const int *adj, const int *dep_pt
     std::stable_sort(cands.begin(), cands.end(),
                      [](const Cand &x, const Cand &y) { return x.range < y.range; });
   }
+  std::vector<std::vector<int>> coords; // chosen coordinates
+  std::vector<std::vector<double>> basis;
   // greedy selection: narrowest first, each with a Gram-Schmidt residual of
   // at least half its norm against those already chosen.  The sums run over
   // fixed 64K-vertex chunks on the host's threads and add the chunks' sums in
@@ -244,12 +152,14 @@ int monotone_partition(int n, const int *xadj, const int *adj, const int *dep_pt
     if (coords.size() == 3)
       break;
     std::vector<int> f(n);
+    if (c.a < 0)
+      std::copy(lvl, lvl + n, f.begin());
+    else if (!coordinate(c, f))
+      return -1;
     long long fsum = 0; // integer: exact in any order
 #pragma omp parallel for schedule(static) reduction(+ : fsum)
-    for (int v = 0; v < n; v++) {
-      f[v] = c.a < 0 ? lvl[v] : c.sign * (dist[c.a][v] - dist[c.b][v]);
+    for (int v = 0; v < n; v++)
       fsum += f[v];
-    }
     const double mean = (double)fsum / n;
     const double var =
         chunked_sum([&](int v) { return (f[v] - mean) * (f[v] - mean); }) / n;
@@ -275,7 +185,6 @@ int monotone_partition(int n, const int *xadj, const int *adj, const int *dep_pt
     basis.push_back(std::move(r));
     coords.push_back(std::move(f));
   }
-  dist.clear();
   basis.clear();
 
   // k-d tree of value-threshold cuts; the two halves of a node are cut as
@@ -358,6 +267,111 @@ int monotone_partition(int n, const int *xadj, const int *adj, const int *dep_pt
 #pragma omp single
   split(0, n, std::max(1, nparts), 0);
   return (int)coords.size();
+}
+
+} // namespace
+
+int monotone_partition(int n, const int *xadj, const int *adj, const int *dep_ptr,
+                       const int *dep_col, int base, const int *lvl, int nparts, int *part) {
+  if (n == 0)
+    return 0;
+  auto search = [&](int src, std::vector<int> &d) { return bfs_dist(n, xadj, adj, src, d); };
+  std::vector<PartitionCand> cands;
+  std::vector<std::vector<int>> dist;
+  {
+    int dmin = INT_MAX;
+    for (int v = 0; v < n; v++)
+      dmin = std::min(dmin, xadj[v + 1] - xadj[v]);
+    std::vector<int> low;
+    for (int v = 0; v < n; v++)
+      if (xadj[v + 1] - xadj[v] == dmin)
+        low.push_back(v);
+    std::vector<int> d, mind;
+    bool connected = search(low[0], d) == n;
+    if (connected) {
+      dist.push_back(d);
+      mind = d;
+      while (dist.size() < 8) {
+        int best = -1;
+        for (int v : low)
+          if (best < 0 || mind[v] > mind[best])
+            best = v;
+        if (best < 0 || mind[best] == 0)
+          break;
+        search(best, d);
+        dist.push_back(d);
+#pragma omp parallel for schedule(static)
+        for (int v = 0; v < n; v++)
+          mind[v] = std::min(mind[v], d[v]);
+      }
+    }
+    // landmark pairs, checked on the host's threads (integer work: the same
+    // candidates, kept in pair order, whatever the threads)
+    const int L = (int)dist.size();
+    std::vector<std::pair<int, int>> pairs;
+    for (int a = 0; a < L; a++)
+      for (int b = a + 1; b < L; b++)
+        pairs.push_back({a, b});
+    const int np = (int)pairs.size();
+    std::vector<PartitionCand> found(np);
+    std::vector<char> keep(np, 0);
+#pragma omp parallel for schedule(dynamic)
+    for (int q = 0; q < np; q++) {
+      const int a = pairs[q].first, b = pairs[q].second;
+      const std::vector<int> &da = dist[a], &db = dist[b];
+      long long pos = 0, neg = 0;
+      for (int i = 0; i < n && !(pos && neg); i++)
+        for (int k = dep_ptr[i] - base; k < dep_ptr[i + 1] - base; k++) {
+          const int j = dep_col[k] - base;
+          const int df = (da[i] - db[i]) - (da[j] - db[j]);
+          pos += df > 0;
+          neg += df < 0;
+        }
+      if ((pos == 0) == (neg == 0))
+        continue; // not monotone, or constant along every edge
+      int lo = INT_MAX, hi = INT_MIN;
+      for (int v = 0; v < n; v++) {
+        const int f = da[v] - db[v];
+        lo = std::min(lo, f);
+        hi = std::max(hi, f);
+      }
+      found[q] = {a, b, pos > 0 ? 1 : -1, (long long)hi - lo};
+      keep[q] = 1;
+    }
+    for (int q = 0; q < np; q++)
+      if (keep[q])
+        cands.push_back(found[q]);
+  }
+  return cut_parts(n, lvl, nparts, part, cands,
+                   [&](const PartitionCand &c, std::vector<int> &f) {
+#pragma omp parallel for schedule(static)
+                     for (int v = 0; v < n; v++)
+                       f[v] = c.sign * (dist[c.a][v] - dist[c.b][v]);
+                     return true;
+                   });
+}
+
+int monotone_partition_device(int n, int base, const int *ai, const int *aj, const int *lvl,
+                              int nparts, int *part, la_status *st) {
+  *st = LA_OK;
+  if (n == 0)
+    return 0;
+  LandmarksDevice *M = landmarks_device_create(n, base, ai, aj, st);
+  if (!M)
+    return -1;
+  struct Owner {
+    LandmarksDevice *m;
+    ~Owner() { landmarks_device_destroy(m); }
+  } own{M};
+  std::vector<PartitionCand> cands;
+  if ((*st = landmarks_device_candidates(M, cands)) != LA_OK)
+    return -1;
+  const int used = cut_parts(n, lvl, nparts, part, cands,
+                             [&](const PartitionCand &c, std::vector<int> &f) {
+                               *st = landmarks_device_coordinate(M, c, f.data());
+                               return *st == LA_OK;
+                             });
+  return used;
 }
 
 } // namespace la

@@ -356,8 +356,20 @@ struct RcmDevice {
     const int nnz = h_ai[n] - base;
     LA_TRY(ai.upload(h_ai, sizeof(int) * (n + 1)));
     LA_TRY(aj.upload(h_aj, sizeof(int) * std::max(nnz, 1)));
-    if (h_deg) // the searches alone (bfs_device_*) need no degrees
-      LA_TRY(deg.upload(h_deg, sizeof(int) * n));
+    LA_TRY(deg.upload(h_deg, sizeof(int) * n));
+    return init_work();
+  }
+  // a 0-based graph already on the device: its buffers are taken over
+  la_status init_device(int n_, DevBuf &d_ai, DevBuf &d_aj) {
+    n = n_;
+    base = 0;
+    std::swap(ai.p, d_ai.p);
+    std::swap(ai.bytes, d_ai.bytes);
+    std::swap(aj.p, d_aj.p);
+    std::swap(aj.bytes, d_aj.bytes);
+    return init_work();
+  }
+  la_status init_work() {
     for (DevBuf *b : {&level, &queue, &pos, &parent, &cm, &cnt})
       LA_TRY(b->alloc(sizeof(int) * n));
     LA_TRY(lstart.alloc(sizeof(int) * (n + 2)));
@@ -480,32 +492,303 @@ RcmDevice *rcm_device_create(int n, int base, const int *ai, const int *aj, cons
 
 void rcm_device_destroy(RcmDevice *D) { delete D; }
 
-struct BfsDevice {
-  RcmDevice D;
-  int reached = 0;
-};
 
-BfsDevice *bfs_device_create(int n, const int *xadj, const int *adj, la_status *st) {
-  auto *B = new BfsDevice();
-  *st = B->D.init(n, 0, xadj, adj, nullptr);
-  if (*st != LA_OK) {
-    delete B;
-    return nullptr;
+
+} // namespace la
+
+// ---- The partitioner's landmark stage on the device: the triangle's graph
+// made undirected, the breadth-first distances from up to eight landmarks
+// (the first vertex of minimum degree, then farthest-point sampling over the
+// vertices of minimum degree), and for every landmark pair the coordinate
+// d_a - d_b: monotone along every stored entry or not, and its range.  The
+// same landmarks, candidates and coordinates as la_partition.cpp's host
+// stage (integer work throughout).
+namespace la {
+namespace {
+
+__global__ void und_count_kernel(const int n, const int *__restrict__ ai,
+                                 const int *__restrict__ aj, int *cnt) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const int a = ai[v], e = ai[v + 1];
+    atomicAdd(cnt + v, e - a);
+    for (int k = a; k < e; k++)
+      atomicAdd(cnt + aj[k], 1);
   }
-  return B;
 }
 
-la_status bfs_device_dist(BfsDevice *B, int src, int *d, int *reached) {
+__global__ void und_fill_kernel(const int n, const int *__restrict__ ai,
+                                const int *__restrict__ aj, int *cursor, int *adj) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    for (int k = ai[v]; k < ai[v + 1]; k++) {
+      const int j = aj[k];
+      adj[atomicAdd(cursor + v, 1)] = j;
+      adj[atomicAdd(cursor + j, 1)] = v;
+    }
+}
+
+__global__ void rebase_copy_kernel(const long long m, const int *in, const int base, int *out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = in[i] - base;
+}
+
+// smallest (degree, vertex)
+__global__ void min_degree_kernel(const int n, const int *__restrict__ xadj,
+                                  unsigned long long *best) {
+  unsigned long long b = ~0ull;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    b = min(b, ((unsigned long long)(unsigned)(xadj[v + 1] - xadj[v]) << 32) | (unsigned)v);
+  for (int o = 16; o > 0; o >>= 1)
+    b = min(b, __shfl_down_sync(0xffffffffu, b, o));
+  if ((threadIdx.x & 31) == 0)
+    atomicMin(best, b);
+}
+
+// among the vertices of degree dmin: largest mind, the smallest vertex on ties
+__global__ void farthest_kernel(const int n, const int dmin, const int *__restrict__ xadj,
+                                const int *__restrict__ mind, unsigned long long *best) {
+  unsigned long long b = 0;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    if (xadj[v + 1] - xadj[v] == dmin)
+      b = max(b, ((unsigned long long)(unsigned)mind[v] << 32) | (0xffffffffu - (unsigned)v));
+  for (int o = 16; o > 0; o >>= 1)
+    b = max(b, __shfl_down_sync(0xffffffffu, b, o));
+  if ((threadIdx.x & 31) == 0)
+    atomicMax(best, b);
+}
+
+__global__ void min_update_kernel(const int n, const int *__restrict__ d, int *mind) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    mind[v] = min(mind[v], d[v]);
+}
+
+constexpr int kMaxLandmarks = 8; // 28 pairs: one bit each in a 32-bit mask
+
+// bit p of pos / neg: d_a - d_b rises / falls along some stored entry (i, j)
+// of the triangle, pair p = (a, b), a < b, in (0,1), (0,2), ... order
+__global__ void pair_sign_kernel(const int n, const int L, const int *__restrict__ ai,
+                                 const int *__restrict__ aj, const int *__restrict__ dist,
+                                 unsigned *masks) {
+  unsigned pos = 0, neg = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int di[kMaxLandmarks];
+    for (int l = 0; l < L; l++)
+      di[l] = __ldg(dist + (size_t)l * n + i);
+    for (int k = __ldg(ai + i); k < __ldg(ai + i + 1); k++) {
+      const int j = __ldg(aj + k);
+      int dj[kMaxLandmarks];
+      for (int l = 0; l < L; l++)
+        dj[l] = __ldg(dist + (size_t)l * n + j);
+      int p = 0;
+      for (int a = 0; a < L; a++)
+        for (int b = a + 1; b < L; b++, p++) {
+          const int df = (di[a] - di[b]) - (dj[a] - dj[b]);
+          pos |= (unsigned)(df > 0) << p;
+          neg |= (unsigned)(df < 0) << p;
+        }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    pos |= __shfl_down_sync(0xffffffffu, pos, o);
+    neg |= __shfl_down_sync(0xffffffffu, neg, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicOr(masks, pos);
+    atomicOr(masks + 1, neg);
+  }
+}
+
+// lo[p] / hi[p]: the range of d_a - d_b over the vertices
+__global__ void pair_range_kernel(const int n, const int L, const int *__restrict__ dist,
+                                  int *lo, int *hi) {
+  constexpr int kPairs = kMaxLandmarks * (kMaxLandmarks - 1) / 2;
+  int mn[kPairs], mx[kPairs];
+  for (int p = 0; p < kPairs; p++) {
+    mn[p] = INT_MAX;
+    mx[p] = INT_MIN;
+  }
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    int d[kMaxLandmarks];
+    for (int l = 0; l < L; l++)
+      d[l] = __ldg(dist + (size_t)l * n + v);
+    int p = 0;
+    for (int a = 0; a < L; a++)
+      for (int b = a + 1; b < L; b++, p++) {
+        mn[p] = min(mn[p], d[a] - d[b]);
+        mx[p] = max(mx[p], d[a] - d[b]);
+      }
+  }
+  const int np = L * (L - 1) / 2;
+  for (int p = 0; p < np; p++) {
+    int a = mn[p], b = mx[p];
+    for (int o = 16; o > 0; o >>= 1) {
+      a = min(a, __shfl_down_sync(0xffffffffu, a, o));
+      b = max(b, __shfl_down_sync(0xffffffffu, b, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicMin(lo + p, a);
+      atomicMax(hi + p, b);
+    }
+  }
+}
+
+__global__ void coordinate_kernel(const int n, const int *__restrict__ da,
+                                  const int *__restrict__ db, const int sign, int *f) {
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    f[v] = sign * (da[v] - db[v]);
+}
+
+int vgrid(long long m) { return (int)std::max(1LL, std::min((m + 255) / 256, 8LL * sm_count())); }
+
+} // namespace
+
+struct LandmarksDevice {
+  int n = 0, L = 0;
+  RcmDevice D;
+  DevBuf tai, taj; // the triangle, 0-based
+  DevBuf dist, mind, f, scratch;
+};
+
+LandmarksDevice *landmarks_device_create(int n, int base, const int *ai, const int *aj,
+                                         la_status *st) {
+  auto fail = [&](LandmarksDevice *M, la_status s) {
+    *st = s;
+    delete M;
+    return (LandmarksDevice *)nullptr;
+  };
+  auto *M = new LandmarksDevice();
+  M->n = n;
+  const long long nnz = (long long)ai[n] - base;
+  DevBuf raw, xadj, adj, cursor;
+  la_status s;
+  if ((s = raw.upload(ai, sizeof(int) * (n + 1))) != LA_OK ||
+      (s = M->tai.alloc(sizeof(int) * (n + 1))) != LA_OK)
+    return fail(M, s);
+  rebase_copy_kernel<<<vgrid(n + 1), 256>>>(n + 1, raw.as<int>(), base, M->tai.as<int>());
+  if ((s = raw.upload(aj, sizeof(int) * std::max(nnz, 1LL))) != LA_OK ||
+      (s = M->taj.alloc(sizeof(int) * std::max(nnz, 1LL))) != LA_OK)
+    return fail(M, s);
+  rebase_copy_kernel<<<vgrid(nnz), 256>>>(nnz, raw.as<int>(), base, M->taj.as<int>());
+  raw.release();
+  // the undirected graph: a row's own entries and its transpose's, any order
+  if ((s = xadj.alloc(sizeof(int) * (n + 1))) != LA_OK ||
+      (s = adj.alloc(sizeof(int) * std::max(2 * nnz, 1LL))) != LA_OK ||
+      (s = cursor.alloc(sizeof(int) * (n + 1))) != LA_OK)
+    return fail(M, s);
+  if (cudaMemset(xadj.p, 0, sizeof(int) * (n + 1)) != cudaSuccess)
+    return fail(M, LA_ERR_CUDA);
+  und_count_kernel<<<vgrid(n), 256>>>(n, M->tai.as<int>(), M->taj.as<int>(), xadj.as<int>());
+  if ((s = scan_exclusive(xadj.as<int>(), n + 1, nullptr)) != LA_OK)
+    return fail(M, s);
+  if (cudaMemcpy(cursor.p, xadj.p, sizeof(int) * (n + 1), cudaMemcpyDeviceToDevice) !=
+      cudaSuccess)
+    return fail(M, LA_ERR_CUDA);
+  und_fill_kernel<<<vgrid(n), 256>>>(n, M->tai.as<int>(), M->taj.as<int>(), cursor.as<int>(),
+                                     adj.as<int>());
+  if (cudaGetLastError() != cudaSuccess) {
+    set_error("partition landmarks: a kernel launch failed");
+    return fail(M, LA_ERR_CUDA);
+  }
+  if ((s = M->D.init_device(n, xadj, adj)) != LA_OK)
+    return fail(M, s);
+  *st = LA_OK;
+  return M;
+}
+
+void landmarks_device_destroy(LandmarksDevice *M) { delete M; }
+
+la_status landmarks_device_candidates(LandmarksDevice *M, std::vector<PartitionCand> &cands) {
+  const int n = M->n;
+  cands.clear();
+  M->L = 0;
+  LA_TRY(M->dist.alloc(sizeof(int) * (size_t)n * kMaxLandmarks));
+  LA_TRY(M->mind.alloc(sizeof(int) * n));
+  LA_TRY(M->scratch.alloc(sizeof(unsigned long long) * 2));
+  const int *xadj = M->D.ai.as<int>();
+  unsigned long long *best = M->scratch.as<unsigned long long>();
+  auto reduce = [&](bool farthest, int dmin, unsigned long long *out) -> la_status {
+    const unsigned long long init = farthest ? 0ull : ~0ull;
+    LA_CUDA_TRY(cudaMemcpy(best, &init, sizeof(init), cudaMemcpyHostToDevice));
+    if (farthest)
+      farthest_kernel<<<vgrid(n), 256>>>(n, dmin, xadj, M->mind.as<int>(), best);
+    else
+      min_degree_kernel<<<vgrid(n), 256>>>(n, xadj, best);
+    LA_CUDA_TRY(cudaGetLastError());
+    LA_CUDA_TRY(cudaMemcpy(out, best, sizeof(*out), cudaMemcpyDeviceToHost));
+    return LA_OK;
+  };
+  unsigned long long key = 0;
+  LA_TRY(reduce(false, 0, &key));
+  const int dmin = (int)(key >> 32), v0 = (int)(key & 0xffffffffu);
+  int reached = 0, height = 0;
   std::vector<int> ls;
-  int height = 0;
-  LA_TRY(B->D.bfs(src, B->reached, ls, &height));
-  // level[] holds the distances of this search's vertices, -1 elsewhere
-  LA_CUDA_TRY(cudaMemcpy(d, B->D.level.p, sizeof(int) * B->D.n, cudaMemcpyDeviceToHost));
-  *reached = B->reached;
+  auto search = [&](int src, int l) -> la_status {
+    LA_TRY(M->D.bfs(src, reached, ls, &height));
+    // level[] holds this search's distances (-1 where unreached)
+    LA_CUDA_TRY(cudaMemcpy(M->dist.as<int>() + (size_t)l * n, M->D.level.p, sizeof(int) * n,
+                           cudaMemcpyDeviceToDevice));
+    return LA_OK;
+  };
+  LA_TRY(search(v0, 0));
+  if (reached != n)
+    return LA_OK; // not connected: no landmark coordinates (as on the host)
+  M->L = 1;
+  LA_CUDA_TRY(cudaMemcpy(M->mind.p, M->dist.p, sizeof(int) * n, cudaMemcpyDeviceToDevice));
+  while (M->L < kMaxLandmarks) {
+    LA_TRY(reduce(true, dmin, &key));
+    if ((key >> 32) == 0)
+      break; // the farthest vertex of minimum degree is a landmark already
+    const int v = (int)(0xffffffffu - (unsigned)(key & 0xffffffffu));
+    LA_TRY(search(v, M->L));
+    min_update_kernel<<<vgrid(n), 256>>>(n, M->dist.as<int>() + (size_t)M->L * n,
+                                         M->mind.as<int>());
+    LA_CUDA_TRY(cudaGetLastError());
+    M->L++;
+  }
+  const int L = M->L, np = L * (L - 1) / 2;
+  if (np == 0)
+    return LA_OK;
+  DevBuf masks, lohi;
+  LA_TRY(masks.alloc(sizeof(unsigned) * 2));
+  LA_TRY(lohi.alloc(sizeof(int) * 2 * 28));
+  LA_CUDA_TRY(cudaMemset(masks.p, 0, sizeof(unsigned) * 2));
+  std::vector<int> init(56);
+  for (int p = 0; p < 28; p++) {
+    init[p] = INT_MAX;
+    init[28 + p] = INT_MIN;
+  }
+  LA_CUDA_TRY(cudaMemcpy(lohi.p, init.data(), sizeof(int) * 56, cudaMemcpyHostToDevice));
+  pair_sign_kernel<<<vgrid(n), 256>>>(n, L, M->tai.as<int>(), M->taj.as<int>(),
+                                      M->dist.as<int>(), masks.as<unsigned>());
+  pair_range_kernel<<<vgrid(n), 256>>>(n, L, M->dist.as<int>(), lohi.as<int>(),
+                                       lohi.as<int>() + 28);
+  LA_CUDA_TRY(cudaGetLastError());
+  unsigned mk[2];
+  int lh[56];
+  LA_CUDA_TRY(cudaMemcpy(mk, masks.p, sizeof(mk), cudaMemcpyDeviceToHost));
+  LA_CUDA_TRY(cudaMemcpy(lh, lohi.p, sizeof(lh), cudaMemcpyDeviceToHost));
+  int p = 0;
+  for (int a = 0; a < L; a++)
+    for (int b = a + 1; b < L; b++, p++) {
+      const bool pos = (mk[0] >> p) & 1u, neg = (mk[1] >> p) & 1u;
+      if (pos == neg)
+        continue; // not monotone, or constant along every entry
+      cands.push_back({a, b, pos ? 1 : -1, (long long)lh[28 + p] - lh[p]});
+    }
   return LA_OK;
 }
 
-void bfs_device_destroy(BfsDevice *B) { delete B; }
+la_status landmarks_device_coordinate(LandmarksDevice *M, const PartitionCand &c, int *f) {
+  const int n = M->n;
+  if (!M->f.p)
+    LA_TRY(M->f.alloc(sizeof(int) * n));
+  coordinate_kernel<<<vgrid(n), 256>>>(n, M->dist.as<int>() + (size_t)c.a * n,
+                                       M->dist.as<int>() + (size_t)c.b * n, c.sign,
+                                       M->f.as<int>());
+  LA_CUDA_TRY(cudaGetLastError());
+  LA_CUDA_TRY(cudaMemcpy(f, M->f.p, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  return LA_OK;
+}
 
 // One component (members ascending, more than two nodes): its Cuthill-McKee
 // order, node + base, into out[0, size).

@@ -751,11 +751,17 @@ void cached_partition(int n, const int *ai, const int *aj, int base,
         return;
       }
   }
-  std::vector<int> xadj, adj;
-  undirected_pattern(n, base, ai, aj, xadj, adj);
+  // the landmark stage on the GPU; should a device step fail (memory), the
+  // host's stage gives the same parts
   part.assign(n, 0);
-  monotone_partition(n, xadj.data(), adj.data(), ai, aj, base, lvl.data(), nparts, part.data(),
-                     true);
+  la_status st = LA_OK;
+  if (monotone_partition_device(n, base, ai, aj, lvl.data(), nparts, part.data(), &st) < 0) {
+    cudaGetLastError();
+    std::vector<int> xadj, adj;
+    undirected_pattern(n, base, ai, aj, xadj, adj);
+    monotone_partition(n, xadj.data(), adj.data(), ai, aj, base, lvl.data(), nparts,
+                       part.data());
+  }
   std::lock_guard<std::mutex> lock(g_part_mu);
   if (g_part_cache.size() == 4)
     g_part_cache.erase(g_part_cache.begin());

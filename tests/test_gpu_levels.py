@@ -58,3 +58,53 @@ def test_levels_device_rejects_non_strict(lab):
     with pytest.raises(lab.LAError) as e:
         lab.TopologicalSort2("L", 2, 0, ai, aj, device=True)
     assert e.value.name == "LA_ERR_INVALID_ARG"
+
+
+def test_partition_device_landmarks_equal_host(lab):
+    """The partitioned solve's row partition with its landmark stage on the
+    GPU (la_trsv_partition_device: the graph, the landmark searches and the
+    candidate checks on the device, as the analysis computes it) equals the
+    host's la_trsv_partition part for part -- grids in natural and RCM order,
+    both triangles, a 27-point stencil, an anisotropic grid at full C3 size,
+    a disconnected pattern (level coordinate only) and random triangles with
+    base 1."""
+    from linearalgebra_b200 import gen
+
+    def strict(n, ai, aj, lower):
+        r = np.repeat(np.arange(n), np.diff(ai))
+        keep = (aj < r) if lower else (aj > r)
+        t_ai = np.zeros(n + 1, np.int32)
+        np.cumsum(np.bincount(r[keep], minlength=n), out=t_ai[1:])
+        return t_ai, aj[keep].astype(np.int32)
+
+    cases = []
+    for name, (n, ai, aj, av), rcm in (("lap3d_20", gen.laplacian_3d(20), False),
+                                       ("lap3d_24_rcm", gen.laplacian_3d(24), True),
+                                       ("st27_12", gen.stencil27(12), False),
+                                       ("aniso_16", gen.aniso7(16, seed=2), True),
+                                       ("lap3d_128_rcm", gen.laplacian_3d(128), True)):
+        if rcm:
+            iperm, perm = lab.SerialCM(n, 0, ai, aj)
+            ai, aj, av = lab.Permute(n, 0, ai, aj, av, iperm, perm)
+        cases.append((name, n, np.asarray(ai, np.int32), np.asarray(aj, np.int32), 0))
+    # two disjoint grids: not connected
+    n1, a1, j1, _ = gen.laplacian_3d(10)
+    ai = np.concatenate([a1, a1[1:] + a1[-1]]).astype(np.int32)
+    aj = np.concatenate([j1, j1 + n1]).astype(np.int32)
+    cases.append(("two_grids", 2 * n1, ai, aj, 0))
+    rng = np.random.default_rng(3)
+    m = 4000
+    rows = [np.sort(rng.choice(m, 6, replace=False)) for _ in range(m)]
+    r_ai = np.concatenate([[0], np.cumsum([len(c) for c in rows])]).astype(np.int32)
+    r_aj = np.concatenate(rows).astype(np.int32)
+    cases.append(("random_base1", m, r_ai + 1, r_aj + 1, 1))
+    for name, n, ai, aj, base in cases:
+        for lower in (True, False):
+            t_ai, t_aj = strict(n, ai - base, aj - base, lower)
+            for nparts in (3, 148):
+                uplo = "L" if lower else "U"
+                want = lab.trsv_partition(uplo, n, base, t_ai + base, t_aj + base, nparts)
+                got = lab.trsv_partition(uplo, n, base, t_ai + base, t_aj + base, nparts,
+                                         device=True)
+                assert got[1] == want[1] and np.array_equal(got[0], want[0]), \
+                    (name, uplo, nparts, got[1], want[1])

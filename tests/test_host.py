@@ -253,6 +253,13 @@ def test_trsv_partition_never_reads_a_later_part(lab):
                 if nparts == 148 and want_coords == 3:
                     sizes = np.bincount(part, minlength=nparts)
                     assert sizes.min() > 0 and sizes.max() <= 2 * n / nparts, (name, sizes.max())
+    # the device form needs a GPU (without one: LA_ERR_NO_DEVICE, nothing computed)
+    from conftest import gpu_available
+    if not gpu_available():
+        with pytest.raises(lab.LAError) as e:
+            lab.trsv_partition("L", 1, 0, np.zeros(2, np.int32), np.zeros(0, np.int32), 4,
+                               device=True)
+        assert e.value.name == "LA_ERR_NO_DEVICE"
     # edge cases and argument checks
     assert lab.trsv_partition("L", 0, 0, np.zeros(1, np.int32), np.zeros(0, np.int32), 4)[0].size == 0
     part, _ = lab.trsv_partition("L", 1, 0, np.zeros(2, np.int32), np.zeros(0, np.int32), 4)
