@@ -780,7 +780,12 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
   int dev = 0, optin = 0;
   LA_CUDA_TRY(cudaGetDevice(&dev));
   LA_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  // a power of two: the k-d cuts then halve every node evenly (measured, 128
+  // against 148 parts: 128^3 factor 0.303 / 0.460 ms against 0.310 / 0.470
+  // FP32 / FP64, 192^3 FP32 0.796 against 0.814 ms; 136 or 144 in between)
   int nparts = std::min(sm_count(), std::max(1, (n + 2047) / 2048));
+  while (nparts & (nparts - 1))
+    nparts &= nparts - 1;
   if (const char *e = std::getenv("LA_TRSV_PARTS")) // tuning override
     nparts = std::max(1, std::min(sm_count(), std::atoi(e)));
   // rows' levels, then the partition (of the triangle's graph made undirected)
