@@ -72,6 +72,40 @@ def test_rcm_device_timing_c5_size(lab):
     print(f"RCM 192^3: host {t_host:.3f} s, with the device ordering {t_dev:.3f} s")
 
 
+def _random_connected(m, seed, max_extra=12):
+    """A connected irregular symmetric pattern: a ring plus random chords
+    (degrees 3 to ~40, many equal degrees, so the sweep's (degree, index)
+    ties matter), diagonal included."""
+    rng = np.random.default_rng(seed)
+    i = np.arange(m)
+    src = [i, (i + 1) % m]
+    k = rng.integers(0, max_extra, m)
+    a = np.repeat(i, k)
+    b = rng.integers(0, m, len(a))
+    keep = a != b
+    rows = np.concatenate([i, i, (i + 1) % m, a[keep], b[keep]])
+    cols = np.concatenate([i, (i + 1) % m, i, b[keep], a[keep]])
+    key = np.unique(rows.astype(np.int64) * m + cols)
+    r, c = key // m, (key % m).astype(np.int32)
+    ai = np.zeros(m + 1, np.int32)
+    np.cumsum(np.bincount(r, minlength=m), out=ai[1:])
+    return m, ai, c
+
+
+def test_rcm_device_irregular_graphs(lab):
+    """Irregular connected graphs above the device threshold (every row at
+    most 64 entries): the device ordering equals the host's, base 0 and 1."""
+    for seed in range(3):
+        n, ai, aj = _random_connected(70_000 + 5_000 * seed, seed)
+        assert np.diff(ai).max() <= 64
+        want = lab.SerialCM(n, 0, ai, aj)
+        got = lab.SerialCM(n, 0, ai, aj, device=True)
+        assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1]), seed
+        got1 = lab.SerialCM(n, 1, ai + 1, aj + 1, device=True)
+        want1 = lab.SerialCM(n, 1, ai + 1, aj + 1)
+        assert np.array_equal(got1[0], want1[0]) and np.array_equal(got1[1], want1[1]), seed
+
+
 def test_rcm_device_rejects_what_the_host_rejects(lab):
     """The pattern check runs on the device for la_rcm_device: an
     unsymmetric pattern and a symmetric one with an unsorted row are both
