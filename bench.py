@@ -261,6 +261,7 @@ def extras(la, torch, peak):
                 tb = time_device_spmv(la, torch, plan, xd, yd, 200, 5) / 200
                 b = spmv_bytes(n, nnz, vb, vb)
                 out["spmv"].append({"config": label, "form": kind, "dtype": dt, "n": n, "nnz": nnz,
+                                    "layout": plan.layout(),
                                     "bytes": b, "us": t * 1e6, "GB/s": b / t / 1e9,
                                     "frac_of_measured_hbm": b / t / 1e9 / peak,
                                     "frac_of_8TBs": b / t / 8e12,

@@ -147,6 +147,14 @@ la_status la_spmv(la_spmv_plan_t plan, double alpha, const void *x,
 la_status la_spmv_host(la_spmv_plan_t plan, double alpha, const double *x,
                        double beta, double *y);
 la_status la_spmv_plan_destroy(la_spmv_plan_t plan);
+/* The layout the plan's SpMV runs on (no reference counterpart):
+ * *row_slots = 0 for the nnz-balanced tile pass (1024-nonzero tiles, rows
+ * crossing a tile combined from partial sums in the reference's merge
+ * order), or k > 0 for the row-slot form the plan picks for matrices of at
+ * least 65,536 rows whose rows all hold at most 8 entries (k slots a row,
+ * padding at most a quarter): every row then summed by one thread in stored
+ * order, SerialSPMV's row sum formed as SegSum / ALBUS form it. */
+la_status la_spmv_layout(la_spmv_plan_t plan, int *row_slots);
 /* Measurement aid (no reference counterpart; not an SpMV): the bound a
  * matrix sets for the SpMV tile pass.  One launch streams the plan's FP64
  * matrix (columns and values, 16-byte loads, whole 1024-nonzero tiles) and,

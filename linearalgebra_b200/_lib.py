@@ -66,6 +66,7 @@ _SIGS = {
     "la_spmv": [P, D, P, D, P, I, P],
     "la_spmv_xparts": [P, D, P, P, I, D, P, I, P],
     "la_spmv_host": [P, D, P, D, P],
+    "la_spmv_layout": [P, P],
     "la_spmv_plan_destroy": [P],
     "la_spmv_noalloc": [I, I, I, I, P, P, P, D, P, D, P, P],
     "la_spmv_transpose": [P, D, P, D, P, P],

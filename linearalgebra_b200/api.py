@@ -157,6 +157,13 @@ class SPMV:
                  _ptr(x))
         return x
 
+    def layout(self):
+        """0 for the tile pass, k > 0 for the row-slot form with k slots a row
+        (la_spmv_layout)."""
+        k = C.c_int()
+        call("la_spmv_layout", self.h, C.byref(k))
+        return k.value
+
     def xparts(self, slices, starts, y, alpha=1.0, beta=0.0):
         """y = alpha*A*x + beta*y with x given as contiguous slices: slices[r]
         holds columns starts[r]..starts[r+1]-1; each entry is a CUDA tensor or a

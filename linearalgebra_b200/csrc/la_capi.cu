@@ -354,6 +354,12 @@ la_status la_spmv_host(la_spmv_plan_t plan, double alpha, const double *x,
   return spmv_host_chunked(plan, alpha, x, beta, y);
 }
 
+la_status la_spmv_layout(la_spmv_plan_t plan, int *row_slots) {
+  LA_CHECK_ARG(plan && row_slots, "arguments");
+  *row_slots = plan->ell_k;
+  return LA_OK;
+}
+
 la_status la_spmv_plan_destroy(la_spmv_plan_t plan) {
   if (plan) {
     delete plan->Atplan;

@@ -189,6 +189,11 @@ struct la_spmv_plan_s {
   la::DevBuf group_end; // int[ntiles]: end of the merge group a tile starts, else -1
   bool long_rows = true; // some row is longer than the per-thread row sum limit
   bool vec_tiles = false; // every row is short enough for the 16-byte load layout
+  // row-slot form (rows of at most 8 entries): ell_k slots per row, slot-major
+  // columns (-1 past a row's end) and values, FP64 and (if the matrix keeps
+  // them) FP32; ell_k == 0: not used
+  int ell_k = 0;
+  la::DevBuf ell_j, ell_v, ell_v32;
   // lazily built transpose for the adjoint
   la_csr_t At = nullptr;
   la_spmv_plan_t Atplan = nullptr;

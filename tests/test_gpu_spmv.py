@@ -283,6 +283,70 @@ def test_sddmm_rows_found_in_every_tile_shape(lab, orc):
         assert np.array_equal(dv.cpu().numpy(), ref), name
 
 
+def test_spmv_row_slot_form_bit_exact(lab, orc, monkeypatch):
+    """The row-slot form the plan picks for large matrices of short rows:
+    every row summed by one thread in stored order, so the result is the
+    reference's algorithm over a single chunk (no row split) bit for bit --
+    SegSum and ALBUS, several (alpha, beta), base 0 and 1, empty rows -- and
+    the tile pass is used otherwise."""
+    from linearalgebra_b200 import gen
+    P = orc.ptr
+    n0, ai0, aj0, av0 = gen.laplacian_3d(24)
+    # a pattern with empty rows and rows of 1 to 8 entries, 80,000 rows
+    rng = np.random.default_rng(9)
+    m = 80_000
+    lens = rng.integers(0, 9, m)
+    lens[rng.choice(m, 500, replace=False)] = 0
+    e_aj = np.concatenate([np.sort(rng.choice(m, k, replace=False)) for k in lens]).astype(np.int32)
+    e_ai = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    e_av = rng.standard_normal(len(e_aj))
+    # the ragged pattern pads by ~100% (mean row 4, longest 8): the plan keeps
+    # the tile pass for it unless LA_SPMV_ELL=1 forces the row-slot form
+    cases = [("lap3d_48", False, *gen.laplacian_3d(48)),
+             ("aniso_44", False, *gen.aniso7(44, seed=2)),
+             ("ragged_80k", True, m, e_ai, e_aj, e_av)]
+    for name, force, n, ai, aj, av in cases:
+        ai, aj = np.asarray(ai, np.int32), np.asarray(aj, np.int32)
+        nnz = int(ai[-1])
+        x = rng.uniform(-1, 1, n)
+        y0 = rng.uniform(-1, 1, n)
+        if force:
+            monkeypatch.delenv("LA_SPMV_ELL", raising=False)
+            assert lab.SPMV(lab.CSR(n, n, 0, ai, aj, av)).layout() == 0, name
+            monkeypatch.setenv("LA_SPMV_ELL", "1")
+        for base in (0, 1):
+            A = lab.CSR(n, n, base, ai + base, aj + base, av, keep_f32=True)
+            for kind, kname in ((lab.api.LA_SPMV_SEGSUM, "segsum"),
+                                (lab.api.LA_SPMV_ALBUS, "albus")):
+                plan = lab.SPMV(A, kind)
+                assert plan.layout() == int(np.diff(ai).max()), (name, plan.layout())
+                for alpha, beta in ((1.0, 0.0), (1.5, 0.5), (-0.75, 2.0)):
+                    y = torch_dev(y0)
+                    plan(torch_dev(x), y, alpha, beta)
+                    ref = y0.copy()
+                    getattr(orc.port(), f"oracle_{kname}_spmv_tiled")(
+                        max(nnz, 1), n, 0, P(ai), P(aj), P(av), P(x), P(ref), alpha, beta)
+                    got = y.cpu().numpy()
+                    # rows before the first stored entry: beta * y (the
+                    # reference's chunked algorithms skip them, a quirk)
+                    lead = int(np.argmax(np.diff(ai) > 0))
+                    want_lead = np.zeros(lead) if beta == 0 else 0.0 + beta * y0[:lead]
+                    assert np.array_equal(got[:lead], want_lead), (name, base, kname)
+                    assert np.array_equal(got[lead:], ref[lead:]), (name, base, kname, alpha)
+    # small matrices keep the tile pass
+    monkeypatch.delenv("LA_SPMV_ELL", raising=False)
+    A = lab.CSR(n0, n0, 0, ai0, aj0, av0)
+    assert lab.SPMV(A).layout() == 0
+    monkeypatch.setenv("LA_SPMV_ELL", "0")
+    n, ai, aj, av = gen.laplacian_3d(48)
+    assert lab.SPMV(lab.CSR(n, n, 0, ai, aj, av)).layout() == 0
+
+
+def torch_dev(a):
+    import torch
+    return torch.as_tensor(np.ascontiguousarray(a)).to("cuda")
+
+
 def test_spmv_xparts_emulated_ranks(lab):
     """The row-block SpMV of a sharded matrix reading x from its owners'
     slices (la_spmv_xparts), with the ranks emulated as separate device
