@@ -580,6 +580,20 @@ def run_case(case):
         fp = la.FactorPlan("ic0", n, 0, ua, uj)
         for _ in range(3):
             fp.factor(uv)
+    elif case == "pcg-mixed-c3":
+        # mixed-precision IC(0)-PCG on the RCM-ordered 128^3 Laplacian, 30
+        # iterations (FP32 copy of A, the solvers' analysis with its device
+        # partition stage, two reliable updates)
+        n, ai, aj, av = gen.laplacian_3d(128)
+        iperm, perm = la.SerialCM(n, 0, ai, aj)
+        b_ai, b_aj, b_av = la.Permute(n, 0, ai, aj, av, iperm, perm)
+        ua, uj, uv = gen.upper_with_diag(n, b_ai, b_aj, b_av)
+        f = la.ICCLevelNumeric0(n, 0, ua, uj, uv)
+        A = la.CSR(n, n, 0, b_ai, b_aj, b_av, keep_f32=True)
+        s = la.PCG(A, ua, uj, f, mixed=True)
+        b = torch.as_tensor(gen.uniform_vector(n, 0)).cuda()
+        x = torch.empty_like(b)
+        s.solve(b, x, rtol=1e-10, maxit=30, allow_not_converged=True)
     elif case == "rcm-c3":
         # reverse Cuthill-McKee of the 128^3 Laplacian ordered on the GPU
         n, ai, aj, av = gen.laplacian_3d(128)
@@ -664,7 +678,7 @@ def main():
     ap.add_argument("--case", default=None,
                     choices=["spmv-powerlaw", "spmv-lap3d", "trsv-lap3d", "trsv-c5-f32",
                              "pcg-lap3d", "adjoint-c4", "factor-c3", "levels-c3", "ingest",
-                             "noalloc-c3", "rcm-c3", "icplan-c3", "factor-c4"],
+                             "noalloc-c3", "rcm-c3", "icplan-c3", "factor-c4", "pcg-mixed-c3"],
                     help="run one kernel workload a few times and exit (for ncu)")
     args = ap.parse_args()
     args.steps_given = args.steps is not None

@@ -564,28 +564,40 @@ __global__ void min_update_kernel(const int n, const int *__restrict__ d, int *m
 
 constexpr int kMaxLandmarks = 8; // 28 pairs: one bit each in a 32-bit mask
 
+// Pair p = (a, b), a < b < L, numbered (0,1), (0,2), ... as the host reads
+// them.  The loops run over the compile-time maximum and test against L, so
+// the per-landmark distances and per-pair extrema stay in registers.
+__device__ __forceinline__ int pair_index(int L, int a, int b) {
+  return a * L - a * (a + 1) / 2 + (b - a - 1);
+}
+
 // bit p of pos / neg: d_a - d_b rises / falls along some stored entry (i, j)
-// of the triangle, pair p = (a, b), a < b, in (0,1), (0,2), ... order
+// of the triangle
 __global__ void pair_sign_kernel(const int n, const int L, const int *__restrict__ ai,
                                  const int *__restrict__ aj, const int *__restrict__ dist,
                                  unsigned *masks) {
   unsigned pos = 0, neg = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     int di[kMaxLandmarks];
-    for (int l = 0; l < L; l++)
-      di[l] = __ldg(dist + (size_t)l * n + i);
+#pragma unroll
+    for (int l = 0; l < kMaxLandmarks; l++)
+      di[l] = l < L ? __ldg(dist + (size_t)l * n + i) : 0;
     for (int k = __ldg(ai + i); k < __ldg(ai + i + 1); k++) {
       const int j = __ldg(aj + k);
       int dj[kMaxLandmarks];
-      for (int l = 0; l < L; l++)
-        dj[l] = __ldg(dist + (size_t)l * n + j);
-      int p = 0;
-      for (int a = 0; a < L; a++)
-        for (int b = a + 1; b < L; b++, p++) {
-          const int df = (di[a] - di[b]) - (dj[a] - dj[b]);
-          pos |= (unsigned)(df > 0) << p;
-          neg |= (unsigned)(df < 0) << p;
-        }
+#pragma unroll
+      for (int l = 0; l < kMaxLandmarks; l++)
+        dj[l] = l < L ? __ldg(dist + (size_t)l * n + j) : 0;
+#pragma unroll
+      for (int a = 0; a < kMaxLandmarks; a++)
+#pragma unroll
+        for (int b = a + 1; b < kMaxLandmarks; b++)
+          if (b < L) {
+            const int df = (di[a] - di[b]) - (dj[a] - dj[b]);
+            const int p = pair_index(L, a, b);
+            pos |= (unsigned)(df > 0) << p;
+            neg |= (unsigned)(df < 0) << p;
+          }
     }
   }
   for (int o = 16; o > 0; o >>= 1) {
@@ -598,36 +610,62 @@ __global__ void pair_sign_kernel(const int n, const int L, const int *__restrict
   }
 }
 
-// lo[p] / hi[p]: the range of d_a - d_b over the vertices
+// lo[p] / hi[p]: the smallest / largest d_a - d_b over all vertices
 __global__ void pair_range_kernel(const int n, const int L, const int *__restrict__ dist,
                                   int *lo, int *hi) {
   constexpr int kPairs = kMaxLandmarks * (kMaxLandmarks - 1) / 2;
   int mn[kPairs], mx[kPairs];
-  for (int p = 0; p < kPairs; p++) {
-    mn[p] = INT_MAX;
-    mx[p] = INT_MIN;
+#pragma unroll
+  for (int q = 0; q < kPairs; q++) {
+    mn[q] = INT_MAX;
+    mx[q] = INT_MIN;
   }
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
     int d[kMaxLandmarks];
-    for (int l = 0; l < L; l++)
-      d[l] = __ldg(dist + (size_t)l * n + v);
-    int p = 0;
-    for (int a = 0; a < L; a++)
-      for (int b = a + 1; b < L; b++, p++) {
-        mn[p] = min(mn[p], d[a] - d[b]);
-        mx[p] = max(mx[p], d[a] - d[b]);
+#pragma unroll
+    for (int l = 0; l < kMaxLandmarks; l++)
+      d[l] = l < L ? __ldg(dist + (size_t)l * n + v) : 0;
+    int q = 0; // register slot: pairs of the compile-time maximum
+#pragma unroll
+    for (int a = 0; a < kMaxLandmarks; a++)
+#pragma unroll
+      for (int b = a + 1; b < kMaxLandmarks; b++, q++) {
+        mn[q] = min(mn[q], d[a] - d[b]);
+        mx[q] = max(mx[q], d[a] - d[b]);
       }
   }
-  const int np = L * (L - 1) / 2;
-  for (int p = 0; p < np; p++) {
-    int a = mn[p], b = mx[p];
+  // warps, then the block's warps in shared memory, then one atomic per
+  // pair and block (atomics from every warp on the same 56 words serialise)
+  __shared__ int smn[32][kPairs], smx[32][kPairs];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < kPairs; q++) {
+    int x = mn[q], y = mx[q];
     for (int o = 16; o > 0; o >>= 1) {
-      a = min(a, __shfl_down_sync(0xffffffffu, a, o));
-      b = max(b, __shfl_down_sync(0xffffffffu, b, o));
+      x = min(x, __shfl_down_sync(0xffffffffu, x, o));
+      y = max(y, __shfl_down_sync(0xffffffffu, y, o));
     }
-    if ((threadIdx.x & 31) == 0) {
-      atomicMin(lo + p, a);
-      atomicMax(hi + p, b);
+    if (lane == 0) {
+      smn[warp][q] = x;
+      smx[warp][q] = y;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < kPairs) {
+    const int q = threadIdx.x;
+    int x = INT_MAX, y = INT_MIN;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+      x = min(x, smn[w][q]);
+      y = max(y, smx[w][q]);
+    }
+    int a = 0; // pair q of the compile-time maximum: pairs of a start at
+               // a (2K - a - 1) / 2
+    while (a + 1 < kMaxLandmarks && (a + 1) * (2 * kMaxLandmarks - a - 2) / 2 <= q)
+      a++;
+    const int b = a + 1 + q - a * (2 * kMaxLandmarks - a - 1) / 2;
+    if (b < L) {
+      atomicMin(lo + pair_index(L, a, b), x);
+      atomicMax(hi + pair_index(L, a, b), y);
     }
   }
 }
