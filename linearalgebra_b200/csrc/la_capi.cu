@@ -4,6 +4,7 @@
 #include <cstdarg>
 #include <cstring>
 #include <memory>
+#include <mutex>
 
 namespace la {
 
@@ -95,10 +96,71 @@ la_status DevBuf::alloc(size_t b) {
   bytes = b;
   return LA_OK;
 }
+// Large uploads (plans and matrices, built in pageable host memory) go
+// through two pinned halves of a staging area: the host's threads copy one
+// chunk into a half while the previous chunk crosses PCIe from the other.
+// Pageable cudaMemcpy measured ~6.6 GB/s on the B200 hosts.  One staging
+// area per process, behind a mutex; if it cannot be pinned, or the copy
+// fails part-way, the plain copy is used.
+namespace {
+constexpr size_t kStageChunk = size_t(16) << 20, kStageMin = size_t(8) << 20;
+std::mutex g_stage_mu;
+char *g_stage = nullptr; // 2 x kStageChunk, pinned
+cudaStream_t g_stage_stream = nullptr;
+cudaEvent_t g_stage_done[2] = {nullptr, nullptr};
+bool g_stage_failed = false;
+
+bool stage_ready() {
+  if (g_stage)
+    return true;
+  if (g_stage_failed)
+    return false;
+  if (cudaHostAlloc(&g_stage, 2 * kStageChunk, cudaHostAllocDefault) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&g_stage_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&g_stage_done[0], cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&g_stage_done[1], cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    g_stage = nullptr;
+    g_stage_failed = true;
+    return false;
+  }
+  return true;
+}
+
+bool staged_upload(void *dst, const void *src, size_t b) {
+  std::lock_guard<std::mutex> lock(g_stage_mu);
+  if (!stage_ready())
+    return false;
+  for (size_t off = 0, k = 0; off < b; off += kStageChunk, k++) {
+    const int h = (int)(k & 1);
+    const size_t len = std::min(kStageChunk, b - off);
+    char *stage = g_stage + h * kStageChunk;
+    if (k >= 2 && cudaEventSynchronize(g_stage_done[h]) != cudaSuccess)
+      return false;
+    constexpr size_t kPiece = size_t(1) << 20;
+    const long long pieces = (long long)((len + kPiece - 1) / kPiece);
+#pragma omp parallel for schedule(static)
+    for (long long q = 0; q < pieces; q++) {
+      const size_t o = (size_t)q * kPiece;
+      std::memcpy(stage + o, static_cast<const char *>(src) + off + o, std::min(kPiece, len - o));
+    }
+    if (cudaMemcpyAsync(static_cast<char *>(dst) + off, stage, len, cudaMemcpyHostToDevice,
+                        g_stage_stream) != cudaSuccess ||
+        cudaEventRecord(g_stage_done[h], g_stage_stream) != cudaSuccess)
+      return false;
+  }
+  return cudaStreamSynchronize(g_stage_stream) == cudaSuccess;
+}
+} // namespace
+
 la_status DevBuf::upload(const void *host, size_t b) {
   LA_TRY(alloc(b));
-  if (host && b)
-    LA_CUDA_TRY(cudaMemcpy(p, host, b, cudaMemcpyHostToDevice));
+  if (!host || !b)
+    return LA_OK;
+  if (b >= kStageMin && staged_upload(p, host, b))
+    return LA_OK;
+  cudaGetLastError();
+  LA_CUDA_TRY(cudaMemcpy(p, host, b, cudaMemcpyHostToDevice));
   return LA_OK;
 }
 void DevBuf::release() {

@@ -790,50 +790,88 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
     nparts = std::max(1, std::min(sm_count(), std::atoi(e)));
   // rows' levels, then the partition (of the triangle's graph made undirected)
   std::vector<int> lvl(n);
+#pragma omp parallel for schedule(dynamic, 16)
   for (int l = 0; l < P->levels; l++)
     for (int p = P->h_prefix[l]; p < P->h_prefix[l + 1]; p++)
       lvl[P->h_iperm[p] - base] = l;
   std::vector<int> part;
   cached_partition(n, ai, aj, base, lvl, nparts, part);
+  // The layout's host loops run over fixed chunks of the execution order on
+  // the host's threads; every array is the one a serial pass writes.
+  constexpr int kChunkRows = 1 << 16;
+  const int nchunk = (n + kChunkRows - 1) / kChunkRows;
+  // per chunk and part: rows of the part in the chunk (execution order)
+  std::vector<int> ccount((size_t)nchunk * nparts, 0);
+  int longest = 0; // register slots from the longest row (16 plus the CSR tail beyond)
+#pragma omp parallel for schedule(static) reduction(max : longest)
+  for (int c = 0; c < nchunk; c++) {
+    int *cc = ccount.data() + (size_t)c * nparts;
+    for (int q = c * kChunkRows; q < std::min(n, (c + 1) * kChunkRows); q++) {
+      const int i = P->h_iperm[q] - base;
+      cc[part[i]]++;
+      longest = std::max(longest, ai[i + 1] - ai[i]);
+    }
+  }
   std::vector<int> pstart(nparts + 1, 0);
-  for (int i = 0; i < n; i++)
-    pstart[part[i] + 1]++;
+  for (int c = 0; c < nchunk; c++)
+    for (int p = 0; p < nparts; p++)
+      pstart[p + 1] += ccount[(size_t)c * nparts + p];
   int rows_max = 0;
   for (int p = 0; p < nparts; p++)
     rows_max = std::max(rows_max, pstart[p + 1]);
   std::partial_sum(pstart.begin(), pstart.end(), pstart.begin());
-  // register slots from the longest row (16 plus the CSR tail beyond)
-  int longest = 0;
-  for (int i = 0; i < n; i++)
-    longest = std::max(longest, ai[i + 1] - ai[i]);
   // (3 slots for the 7-point stencils' IC(0) factors: a fourth would hold four
   // registers per prefetched row for nothing, and FP64 needs them)
   const int kd = longest <= 3 ? 3 : longest <= 4 ? 4 : longest <= 8 ? 8 : longest <= 16 ? 16 : 0;
   const int ks = kd ? kd : 16;
-  // execution order: part-major, level order inside a part; sb = the
-  // start position of every (part, level), psub = each part's first entry
-  std::vector<int> erow(n), pos(n);
+  // execution order: part-major, level order inside a part (a stable
+  // counting sort of the level order by part: chunk c's rows of part p start
+  // after those of the earlier chunks); sb = the start position of every
+  // (part, level), psub = each part's first entry
+  // (every entry written below: left uninitialised, no first-touch pass)
+  std::unique_ptr<int[]> erow(new int[std::max(n, 1)]), pos(new int[std::max(n, 1)]);
   {
-    std::vector<int> fill(pstart.begin(), pstart.end() - 1);
-    for (int q = 0; q < n; q++) {
-      const int i = P->h_iperm[q] - base, r = fill[part[i]]++;
-      erow[r] = i;
-      pos[i] = r;
+    for (int p = 0; p < nparts; p++) { // ccount becomes each chunk's first slot
+      int at = pstart[p];
+      for (int c = 0; c < nchunk; c++) {
+        const int k = ccount[(size_t)c * nparts + p];
+        ccount[(size_t)c * nparts + p] = at;
+        at += k;
+      }
+    }
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < nchunk; c++) {
+      int *fill = ccount.data() + (size_t)c * nparts;
+      for (int q = c * kChunkRows; q < std::min(n, (c + 1) * kChunkRows); q++) {
+        const int i = P->h_iperm[q] - base, r = fill[part[i]]++;
+        erow[r] = i;
+        pos[i] = r;
+      }
     }
   }
-  std::vector<int> sb, psub(nparts + 1), lvl_at(n);
+  std::vector<int> nsub(nparts, 0), psub(nparts + 1);
+  std::unique_ptr<int[]> lvl_at(new int[std::max(n, 1)]);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int p = 0; p < nparts; p++)
+    for (int r = pstart[p]; r < pstart[p + 1]; r++)
+      nsub[p] += r == pstart[p] || lvl[erow[r]] != lvl[erow[r - 1]];
   int subs_max = 0;
+  psub[0] = 0;
   for (int p = 0; p < nparts; p++) {
-    psub[p] = (int)sb.size();
+    psub[p + 1] = psub[p] + nsub[p];
+    subs_max = std::max(subs_max, nsub[p]);
+  }
+  std::vector<int> sb(psub[nparts] + 1);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int p = 0; p < nparts; p++) {
+    int g = psub[p] - 1;
     for (int r = pstart[p]; r < pstart[p + 1]; r++) {
       if (r == pstart[p] || lvl[erow[r]] != lvl[erow[r - 1]])
-        sb.push_back(r);
-      lvl_at[r] = (int)sb.size() - 1;
+        sb[++g] = r;
+      lvl_at[r] = g;
     }
-    subs_max = std::max(subs_max, (int)sb.size() - psub[p]);
   }
-  psub[nparts] = (int)sb.size();
-  sb.push_back(n);
+  sb[psub[nparts]] = n;
   // end of the level two after the one at sb index g (part p)
   auto end2 = [&](int p, int g) { return sb[std::min(g + 3, psub[p + 1])]; };
   // shared memory: every row of the largest part, else a ring (power of two)
@@ -916,17 +954,32 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
   // at most 0.8 of that.
   if (!force) {
     const double f = sizeof(X) == 8 ? 1.5 : 1.0;
-    std::vector<double> ready(n), last(nparts, 0.0), fin(nparts, 0.0);
+    std::vector<double> ready(n), last(nparts, 0.0), fin(nparts, 0.0), tin;
     std::vector<int> width(nparts, 0), touched;
+    // a row's input time: the latest of its dependencies' (levels of 4096
+    // rows or more on the host's threads; a max, so the same in any order)
+    auto input_time = [&](int q) {
+      const int i = P->h_iperm[q] - base, pi = part[i];
+      double t = 0;
+      for (int k = ai[i] - base; k < ai[i + 1] - base; k++) {
+        const int j = aj[k] - base;
+        t = std::max(t, ready[j] + (part[j] != pi ? 1.5 : 0.0));
+      }
+      return t;
+    };
     for (int l = 0; l < P->levels; l++) {
       touched.clear();
-      for (int q = P->h_prefix[l]; q < P->h_prefix[l + 1]; q++) {
+      const int q0l = P->h_prefix[l], q1l = P->h_prefix[l + 1];
+      const bool wide = q1l - q0l >= 4096;
+      if (wide) {
+        tin.resize(q1l - q0l);
+#pragma omp parallel for schedule(static)
+        for (int q = q0l; q < q1l; q++)
+          tin[q - q0l] = input_time(q);
+      }
+      for (int q = q0l; q < q1l; q++) {
         const int i = P->h_iperm[q] - base, pi = part[i];
-        double t = 0;
-        for (int k = ai[i] - base; k < ai[i + 1] - base; k++) {
-          const int j = aj[k] - base;
-          t = std::max(t, ready[j] + (part[j] != pi ? 1.5 : 0.0));
-        }
+        const double t = wide ? tin[q - q0l] : input_time(q);
         if (width[pi]++ == 0) {
           touched.push_back(pi);
           fin[pi] = last[pi];
@@ -1021,7 +1074,7 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
           break;
         }
   LA_TRY(P->ej.upload(ej.get(), sizeof(int) * cells));
-  LA_TRY(P->exec_row.upload(erow.data(), sizeof(int) * erow.size()));
+  LA_TRY(P->exec_row.upload(erow.get(), sizeof(int) * n));
   LA_TRY(P->pstart.upload(pstart.data(), sizeof(int) * pstart.size()));
   LA_TRY(P->psub.upload(psub.data(), sizeof(int) * psub.size()));
   LA_TRY(P->sb.upload(sb.data(), sizeof(int) * sb.size()));
@@ -1107,11 +1160,39 @@ la_status trsv_build(la_trsv_plan_t P, const int *ai, const int *aj,
   std::vector<double> ediag(n, 1.0);
   eaj[0] = 0; // the one placeholder entry of an empty triangle
   eav[0] = 0;
+  // row pointers in execution order: row lengths, then a chunked prefix sum
+  // (chunk totals added in order), on the host's threads
   eai[0] = base;
+  int longest = 0;
+#pragma omp parallel for schedule(static) reduction(max : longest)
   for (int p = 0; p < n; p++) {
     const int i = P->h_iperm[p] - base;
     erow[p] = i;
-    eai[p + 1] = eai[p] + (ai[i + 1] - ai[i]);
+    eai[p + 1] = ai[i + 1] - ai[i];
+    longest = std::max(longest, eai[p + 1]);
+  }
+  {
+    constexpr int kScanChunk = 1 << 16;
+    const int nc = (n + kScanChunk - 1) / kScanChunk;
+    std::vector<int> total(nc + 1, 0);
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < nc; c++) {
+      int acc = 0;
+      for (int p = c * kScanChunk; p < std::min(n, (c + 1) * kScanChunk); p++)
+        acc += eai[p + 1];
+      total[c + 1] = acc;
+    }
+    total[0] = base;
+    for (int c = 0; c < nc; c++)
+      total[c + 1] += total[c];
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < nc; c++) {
+      int acc = total[c];
+      for (int p = c * kScanChunk; p < std::min(n, (c + 1) * kScanChunk); p++) {
+        acc += eai[p + 1];
+        eai[p + 1] = acc;
+      }
+    }
   }
   // rows in execution order, copied on the host's threads
 #pragma omp parallel for schedule(dynamic, 4096)
@@ -1124,9 +1205,6 @@ la_status trsv_build(la_trsv_plan_t P, const int *ai, const int *aj,
       eav[w] = av[k];
     }
   }
-  int longest = 0;
-  for (int p = 0; p < n; p++)
-    longest = std::max(longest, eai[p + 1] - eai[p]);
   P->kd = longest <= 4 ? 4 : longest <= 8 ? 8 : longest <= 16 ? 16 : 0;
   for (int l = 0; l < P->levels; l++)
     for (int p = P->h_prefix[l]; p < P->h_prefix[l + 1]; p += kChunk)
