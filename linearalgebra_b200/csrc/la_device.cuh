@@ -52,6 +52,23 @@ __device__ __forceinline__ double ld_ahead(const double *p) {
   asm volatile("ld.global.nc.f64 %0, [%1];" : "=d"(v) : "l"(p));
   return v;
 }
+// 16-byte records (32 for FP64 values), same placement rule
+__device__ __forceinline__ int4 ld_ahead(const int4 *p) {
+  int4 v;
+  asm volatile("ld.global.nc.v4.s32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(p));
+  return v;
+}
+__device__ __forceinline__ void ld_ahead4(const float *p, float (&v)[4]) {
+  asm volatile("ld.global.nc.v4.f32 {%0,%1,%2,%3}, [%4];"
+               : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3])
+               : "l"(p));
+}
+__device__ __forceinline__ void ld_ahead4(const double *p, double (&v)[4]) {
+  asm volatile("ld.global.nc.v2.f64 {%0,%1}, [%2];" : "=d"(v[0]), "=d"(v[1]) : "l"(p));
+  asm volatile("ld.global.nc.v2.f64 {%0,%1}, [%2];" : "=d"(v[2]), "=d"(v[3]) : "l"(p + 2));
+}
 
 // Device-scope relaxed accesses (bypass the non-coherent L1) used for data
 // exchanged between CTAs of one kernel.

@@ -237,6 +237,9 @@ struct la_trsv_plan_s {
   bool w2 = false; // partitioned kernel with the second-row register sets
   la::DevBuf pstart, psub, sb;
   la::DevBuf ej, ev; // first slots of every row, slot-major (schedule 1)
+  // schedule 1 with 3-slot rows: per execution position {row, 3 columns}
+  // (int4) and {3 values, diagonal} in the solve's type, instead of ej / ev
+  la::DevBuf rmeta, rval;
   la::DevBuf hb, hx; // staging for the host form
 };
 

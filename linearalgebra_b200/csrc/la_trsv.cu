@@ -353,7 +353,8 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
                      const V *__restrict__ av, const int *__restrict__ ej,
                      const V *__restrict__ ev, const V *__restrict__ diag,
                      const int *__restrict__ exec_row, const X *__restrict__ b, X *x,
-                     int *err, const int tail, const int rows_cap, const int ring_mask) {
+                     int *err, const int tail, const int rows_cap, const int ring_mask,
+                     const int4 *__restrict__ rmeta, const V *__restrict__ rval) {
   constexpr int T = part_threads<X, KD>();
   const bool ring = ring_mask != kNoRing;
   extern __shared__ __align__(16) unsigned char part_smem[];
@@ -367,13 +368,24 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
 
   auto load_row = [&](int r, PartRow<X, KD> &R) {
     R.r = r;
-    R.i = dev::ld_ahead(exec_row + r);
+    if constexpr (KD == 3) { // two records: {row, 3 columns}, {3 values, diagonal}
+      const int4 m = dev::ld_ahead(rmeta + r);
+      V v[4];
+      dev::ld_ahead4(rval + 4 * (size_t)r, v);
+      R.i = m.x, R.j[0] = m.y, R.j[1] = m.z, R.j[2] = m.w;
 #pragma unroll
-    for (int s = 0; s < KD; s++) {
-      R.j[s] = dev::ld_ahead(ej + (size_t)s * n + r);
-      R.a[s] = X(dev::ld_ahead(ev + (size_t)s * n + r));
+      for (int s = 0; s < 3; s++)
+        R.a[s] = X(v[s]);
+      R.dg = UNIT ? X(1) : X(v[3]);
+    } else {
+      R.i = dev::ld_ahead(exec_row + r);
+#pragma unroll
+      for (int s = 0; s < KD; s++) {
+        R.j[s] = dev::ld_ahead(ej + (size_t)s * n + r);
+        R.a[s] = X(dev::ld_ahead(ev + (size_t)s * n + r));
+      }
+      R.dg = UNIT ? X(1) : X(dev::ld_ahead(diag + r));
     }
-    R.dg = UNIT ? X(1) : X(dev::ld_ahead(diag + r));
   };
   auto prefetch = [&](int q, PartRow<X, KD> &R) {
     R.r = -1;
@@ -500,7 +512,13 @@ __global__ void __launch_bounds__(part_threads<X, KD>(), 1)
     const int s = ssb[q - q0], e = ssb[qe - q0];
     const char *base_ptr;
     size_t es;
-    if (a == 0) {
+    if constexpr (KD == 3) { // the two record arrays
+      if (a >= 2)
+        return;
+      base_ptr = a == 0 ? reinterpret_cast<const char *>(rmeta)
+                        : reinterpret_cast<const char *>(rval);
+      es = a == 0 ? sizeof(int4) : 4 * sizeof(V);
+    } else if (a == 0) {
       base_ptr = reinterpret_cast<const char *>(exec_row);
       es = 4;
     } else if (a == 1) {
@@ -623,10 +641,12 @@ cudaError_t launch_parts_kd(la_trsv_plan_t P, const X *b, X *x, cudaStream_t st)
   const V *av = P->av.as<V>(), *ev = P->ev.as<V>(), *dg = P->diag.as<V>();
   int *err = P->err.as<int>();
   const int cap = P->part_rows, mask = P->ring_mask;
+  const int4 *rm = P->rmeta.as<int4>();
+  const V *rv = P->rval.as<V>();
   void *args[] = {(void *)&n,  (void *)&ps, (void *)&pq, (void *)&sb,  (void *)&ai,
                   (void *)&aj, (void *)&av, (void *)&ej, (void *)&ev,  (void *)&dg,
                   (void *)&er, (void *)&b,  (void *)&x,  (void *)&err, (void *)&tail,
-                  (void *)&cap, (void *)&mask};
+                  (void *)&cap, (void *)&mask, (void *)&rm, (void *)&rv};
   return cudaLaunchCooperativeKernel(part_fn<V, X, UNIT, KD, W2>(), dim3(P->nparts),
                                      dim3(part_threads<X, KD>()), args, P->part_smem, st);
 }
@@ -1073,12 +1093,36 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
           ej[r] = erow[r];
           break;
         }
-  LA_TRY(P->ej.upload(ej.get(), sizeof(int) * cells));
+  if (kd == 3) {
+    // 3-slot rows: one 16-byte record {row, columns} and one {values,
+    // diagonal} per position, read by two (FP64: three) vector loads instead
+    // of eight scalar ones -- fewer loads in flight per thread and level
+    const size_t m = 4 * (size_t)std::max(n, 1);
+    std::unique_ptr<int[]> meta(new int[m]);
+    std::unique_ptr<X[]> vals(new X[m]);
+#pragma omp parallel for schedule(static)
+    for (int r = 0; r < n; r++) {
+      meta[4 * (size_t)r] = erow[r];
+      for (int t = 0; t < 3; t++) {
+        meta[4 * (size_t)r + 1 + t] = ej[(size_t)t * n + r];
+        vals[4 * (size_t)r + t] = ev[(size_t)t * n + r];
+      }
+      vals[4 * (size_t)r + 3] = ediag[r];
+    }
+    LA_TRY(P->rmeta.upload(meta.get(), sizeof(int) * m));
+    LA_TRY(P->rval.upload(vals.get(), sizeof(X) * m));
+    P->ej.release();
+    P->ev.release();
+  } else {
+    LA_TRY(P->ej.upload(ej.get(), sizeof(int) * cells));
+    LA_TRY(P->ev.upload(ev.get(), sizeof(X) * cells));
+    P->rmeta.release();
+    P->rval.release();
+  }
   LA_TRY(P->exec_row.upload(erow.get(), sizeof(int) * n));
   LA_TRY(P->pstart.upload(pstart.data(), sizeof(int) * pstart.size()));
   LA_TRY(P->psub.upload(psub.data(), sizeof(int) * psub.size()));
   LA_TRY(P->sb.upload(sb.data(), sizeof(int) * sb.size()));
-  LA_TRY(P->ev.upload(ev.get(), sizeof(X) * cells));
   LA_TRY(P->diag.upload(ediag.get(), sizeof(X) * n));
   P->kd = kd;
   P->nparts = nparts;
