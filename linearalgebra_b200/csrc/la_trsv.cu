@@ -1197,11 +1197,13 @@ la_status trsv_build(la_trsv_plan_t P, const int *ai, const int *aj,
   }
   if (const char *e = std::getenv("LA_TRSV_SLEEP_NS")) // tuning override
     P->sleep_ns = std::max(0, std::atoi(e));
-  std::vector<int> eai(n + 1), erow(n), cstart;
+  std::vector<int> cstart;
   // filled below on the host's threads, every entry written: no initialisation
+  // (zeroed vectors would cost a serial first-touch pass over their pages)
+  std::unique_ptr<int[]> eai(new int[n + 1]), erow(new int[std::max(n, 1)]);
   std::unique_ptr<int[]> eaj(new int[std::max(P->nnz, 1)]);
   std::unique_ptr<double[]> eav(new double[std::max(P->nnz, 1)]);
-  std::vector<double> ediag(n, 1.0);
+  std::unique_ptr<double[]> ediag(new double[std::max(n, 1)]);
   eaj[0] = 0; // the one placeholder entry of an empty triangle
   eav[0] = 0;
   // row pointers in execution order: row lengths, then a chunked prefix sum
@@ -1242,8 +1244,7 @@ la_status trsv_build(la_trsv_plan_t P, const int *ai, const int *aj,
 #pragma omp parallel for schedule(dynamic, 4096)
   for (int p = 0; p < n; p++) {
     const int i = erow[p];
-    if (diag)
-      ediag[p] = diag[i];
+    ediag[p] = diag ? diag[i] : 1.0;
     for (int k = ai[i] - base, w = eai[p] - base; k < ai[i + 1] - base; k++, w++) {
       eaj[w] = aj[k];
       eav[w] = av[k];
@@ -1255,16 +1256,17 @@ la_status trsv_build(la_trsv_plan_t P, const int *ai, const int *aj,
       cstart.push_back(p);
   cstart.push_back(n);
   P->nchunks = (int)cstart.size() - 1;
-  LA_TRY(P->ai.upload(eai.data(), sizeof(int) * eai.size()));
+  LA_TRY(P->ai.upload(eai.get(), sizeof(int) * (n + 1)));
   LA_TRY(P->aj.upload(eaj.get(), sizeof(int) * std::max(P->nnz, 1)));
-  LA_TRY(P->exec_row.upload(erow.data(), sizeof(int) * erow.size()));
+  LA_TRY(P->exec_row.upload(erow.get(), sizeof(int) * n));
   LA_TRY(P->chunk_start.upload(cstart.data(), sizeof(int) * cstart.size()));
   if (P->dtype == LA_F64) {
     LA_TRY(P->av.upload(eav.get(), sizeof(double) * std::max(P->nnz, 1)));
-    LA_TRY(P->diag.upload(ediag.data(), sizeof(double) * n));
+    LA_TRY(P->diag.upload(ediag.get(), sizeof(double) * n));
     P->grid = grid_for<double, double>(P->nchunks, P->kd);
   } else {
-    std::vector<float> f(eav.get(), eav.get() + std::max(P->nnz, 1)), fd(ediag.begin(), ediag.end());
+    std::vector<float> f(eav.get(), eav.get() + std::max(P->nnz, 1)),
+        fd(ediag.get(), ediag.get() + n);
     LA_TRY(P->av.upload(f.data(), sizeof(float) * f.size()));
     LA_TRY(P->diag.upload(fd.data(), sizeof(float) * n));
     P->grid = grid_for<float, float>(P->nchunks, P->kd);

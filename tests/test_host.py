@@ -436,3 +436,47 @@ def test_ilu0_defining_property_and_restatement(lab):
         lab.ILU0(2, 0, np.array([0, 1, 2], np.int32), np.array([0, 0], np.int32),
                  np.array([1.0, 1.0]))
     assert e.value.name == "LA_ERR_INVALID_ARG"
+
+
+def test_trsv_partition_large_nodes_thread_invariant():
+    """A partition of over a million rows (the RCM-ordered 104^3 Laplacian's
+    lower triangle, 1,124,864 rows, 128 parts), whose landmark searches,
+    coordinate sums and k-d cuts run on the host's threads: the parts are the
+    same at 1 and 8 threads, no row reads a later part, and the parts are
+    balanced."""
+    import os
+    import subprocess
+    import sys
+    code = r'''
+import sys, numpy as np
+sys.path.insert(0, sys.argv[1])
+import linearalgebra_b200 as la
+from linearalgebra_b200 import gen
+n, ai, aj, av = gen.laplacian_3d(104)
+iperm, perm = la.SerialCM(n, 0, ai, aj)
+b_ai, b_aj, b_av = la.Permute(n, 0, ai, aj, av, iperm, perm)
+rows = np.repeat(np.arange(n), np.diff(b_ai))
+keep = b_aj < rows
+l_aj = b_aj[keep].astype(np.int32)
+l_ai = np.concatenate([[0], np.cumsum(np.bincount(rows[keep], minlength=n))]).astype(np.int32)
+part, coords = la.trsv_partition("L", n, 0, l_ai, l_aj, 128)
+np.savez(sys.argv[2], part=part, ai=l_ai, aj=l_aj, coords=coords)
+'''
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        got = []
+        for t in ("1", "8"):
+            out = os.path.join(d, f"p{t}.npz")
+            env = dict(os.environ, OMP_NUM_THREADS=t)
+            subprocess.run([sys.executable, "-c", code, root, out], check=True, env=env,
+                           timeout=600)
+            got.append(np.load(out))
+        p1, p8 = got[0]["part"], got[1]["part"]
+        assert np.array_equal(p1, p8)
+        ai, aj = got[0]["ai"], got[0]["aj"]
+        n = len(ai) - 1
+        r = np.repeat(np.arange(n), np.diff(ai))
+        assert not np.any(p1[aj] > p1[r])
+        sizes = np.bincount(p1, minlength=128)
+        assert int(got[0]["coords"]) == 3 and sizes.min() > 0 and sizes.max() <= 2 * n / 128
