@@ -100,8 +100,9 @@ la_status DevBuf::alloc(size_t b) {
 // through two pinned halves of a staging area: the host's threads copy one
 // chunk into a half while the previous chunk crosses PCIe from the other.
 // Pageable cudaMemcpy measured ~6.6 GB/s on the B200 hosts.  One staging
-// area per process, behind a mutex; if it cannot be pinned, or the copy
-// fails part-way, the plain copy is used.
+// area per process, behind a mutex, with its stream on the device current at
+// its first use; uploads while another device is current, or when it cannot
+// be pinned, or a copy that fails part-way, take the plain copy.
 namespace {
 constexpr size_t kStageChunk = size_t(16) << 20, kStageMin = size_t(8) << 20;
 std::mutex g_stage_mu;
@@ -109,12 +110,17 @@ char *g_stage = nullptr; // 2 x kStageChunk, pinned
 cudaStream_t g_stage_stream = nullptr;
 cudaEvent_t g_stage_done[2] = {nullptr, nullptr};
 bool g_stage_failed = false;
+int g_stage_dev = -1;
 
 bool stage_ready() {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess)
+    return false;
   if (g_stage)
-    return true;
+    return dev == g_stage_dev;
   if (g_stage_failed)
     return false;
+  g_stage_dev = dev;
   if (cudaHostAlloc(&g_stage, 2 * kStageChunk, cudaHostAllocDefault) != cudaSuccess ||
       cudaStreamCreateWithFlags(&g_stage_stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&g_stage_done[0], cudaEventDisableTiming) != cudaSuccess ||
