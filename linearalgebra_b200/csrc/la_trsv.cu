@@ -966,14 +966,17 @@ la_status build_parts(la_trsv_plan_t P, const int *ai, const int *aj, const doub
   // Modelled critical path (microseconds; B200 measurements): a part takes
   // ~0.35 us per level it holds plus ~1 us for every further round of rows
   // in a level wider than its CTA (~0.3 us for the second round when it is
-  // held in registers, W2), both 1.5x for FP64 (a part's level step
-  // measured 1.24 us FP64 against 0.80 us FP32 on the 128^3 IC(0) factor,
-  // while the level order costs about the same in both), and a value
+  // held in registers, W2), both 1.2x for FP64 3-slot rows and 1.5x for
+  // longer FP64 rows (a part's level step measured 0.96 / 1.24 us FP64 --
+  // with / without the 3-slot row records -- against 0.79 / 0.80 us FP32 on
+  // the 128^3 IC(0) factor, while the level order costs about the same in
+  // both; with the factor 1.2 the 192^3 FP64 factor's ring-mode parts,
+  // 1.107 ms, are taken over its level order, 1.201 ms), and a value
   // crossing parts arrives ~1.5 us after it is written; the level-order
   // schedule takes ~2 us per level.  The partition is used when it models
   // at most 0.8 of that.
   if (!force) {
-    const double f = sizeof(X) == 8 ? 1.5 : 1.0;
+    const double f = sizeof(X) == 8 ? (kd == 3 ? 1.2 : 1.5) : 1.0;
     std::vector<double> ready(n), last(nparts, 0.0), fin(nparts, 0.0), tin;
     std::vector<int> width(nparts, 0), touched;
     // a row's input time: the latest of its dependencies' (levels of 4096
