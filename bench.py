@@ -628,6 +628,22 @@ def run_case(case):
                                      C.c_void_p(ai_d.data_ptr()), C.c_void_p(aj_d.data_ptr()),
                                      C.c_void_p(av_d.data_ptr()), 1.0, C.c_void_p(x.data_ptr()),
                                      0.0, C.c_void_p(y.data_ptr()), st)
+    elif case == "trsv-c5":
+        # FP64 lower solve of the RCM-ordered 192^3 anisotropic IC(0) factor:
+        # the partitioned kernel with its x values in a shared-memory ring
+        n, ai, aj, av = gen.aniso7(192, seed=0)
+        iperm, perm = la.SerialCM(n, 0, ai, aj)
+        b_ai, b_aj, b_av = la.Permute(n, 0, ai, aj, av, iperm, perm)
+        ua, uj, uv = gen.upper_with_diag(n, b_ai, b_aj, b_av)
+        f = la.ICCLevelNumeric0(n, 0, ua, uj, uv)
+        _, d, (s_ai, s_aj, s_av) = la.SplitLDU(n, 0, ua, uj, f)
+        t_ai, t_aj, t_av = la.Transpose(n, n, 0, s_ai, s_aj, s_av)
+        ts = la.OptimizedTriangularSolve("L").analysis(n, 0, t_ai, t_aj, t_av, d)
+        b = torch.as_tensor(gen.uniform_vector(n, 0)).cuda()
+        x = torch.empty_like(b)
+        for _ in range(3):
+            ts(b, x)
+        print("schedule", ts.schedule())
     elif case == "trsv-c5-f32":
         # FP32 lower solve of the RCM-ordered 192^3 anisotropic IC(0) factor:
         # the partitioned kernel with second-row register sets
@@ -676,7 +692,7 @@ def main():
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-cpu-pcg", action="store_true")
     ap.add_argument("--case", default=None,
-                    choices=["spmv-powerlaw", "spmv-lap3d", "trsv-lap3d", "trsv-c5-f32",
+                    choices=["spmv-powerlaw", "spmv-lap3d", "trsv-lap3d", "trsv-c5", "trsv-c5-f32",
                              "pcg-lap3d", "adjoint-c4", "factor-c3", "levels-c3", "ingest",
                              "noalloc-c3", "rcm-c3", "icplan-c3", "factor-c4", "pcg-mixed-c3"],
                     help="run one kernel workload a few times and exit (for ncu)")
