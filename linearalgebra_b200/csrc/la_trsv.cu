@@ -321,10 +321,13 @@ template <typename X, int KD> struct PartRow {
 //  * the part's level boundaries and the b values of its rows are staged in
 //    shared memory at kernel start (row r's x slot holds b until row r
 //    overwrites it with x);
-//  * the first KD entries of every row are stored slot-major by execution
-//    position (ej[s*n + r], ev[s*n + r]; kEmptySlot marks an unused slot), so
-//    a thread's row is one coalesced load per slot; every thread fetches its
-//    first row of level q+3 while it solves level q (four register sets);
+//  * 3-slot rows are two records per execution position, {row, 3 columns}
+//    (int4) and {3 values, diagonal}; longer rows keep their first KD
+//    entries slot-major (ej[s*n + r], ev[s*n + r]); kEmptySlot marks an
+//    unused slot.  A warp's rows are coalesced loads either way -- two
+//    vector loads a row (three in FP64) against one per slot -- and every
+//    thread fetches its first row of level q+3 while it solves level q (four
+//    register sets);
 //  * at the end of level q it issues the loads of the other parts' values
 //    that its level-(q+2) row reads -- two levels after that row's columns
 //    were requested, so the addresses are there -- and only re-reads (waits
